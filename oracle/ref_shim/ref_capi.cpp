@@ -1,0 +1,127 @@
+// C entry points around the reference's OWN scan code, compiled from the
+// reference sources where they lie (see oracle/Makefile, target `ref`).
+// Oracle infrastructure only: the tests and the CPU-baseline leg of bench.py
+// load the resulting oracle/_ref/libtremor_ref.so; the product never does.
+//
+//   tmref_sss_knn / tmref_sss_threshold : SkipSequentialScan (SkipSequential.hpp:32-78)
+//       built from a waveform file, one object per call (the template counter is
+//       not reset between searches, SkipSequential.cpp:127-136).
+//   tmref_sss_stats                      : the per-window statistics that
+//       SkipSequentialScan::build computes (SkipSequential.cpp:157-190).
+//   tmref_l2_dist / tmref_znormalize / tmref_block_order / tmref_select_knn :
+//       the inline building blocks of ZnormSearch.hpp, for bit-level pinning.
+#include <cfloat>
+#include <cstdint>
+#include <cstring>
+#include <exception>
+#include <string>
+#include <vector>
+
+#define private public // read the statistics SkipSequentialScan::build keeps
+#include "tremor/algos/sss/SkipSequential.hpp"
+#undef private
+#include "tremor/distance_computers/ZnormSearch.hpp"
+#include "tremor/isax/iSAXPqueue.hpp"
+
+extern "C"
+{
+    int tmref_sss_knn(const char *waveform_file, uint64_t total_samples, int m, const float *queries, int query_count,
+                      int k, int merge_offset, int lower_bounds, int threads, int paa_segments, const char *out_csv)
+    {
+        try
+        {
+            SkipSequentialScan scan(threads, paa_segments, merge_offset, 0, lower_bounds != 0);
+            scan.build(waveform_file, total_samples, m);
+            scan.search_knn(queries, query_count, k, out_csv);
+            return 0;
+        }
+        catch (const std::exception &)
+        {
+            return -1;
+        }
+    }
+
+    int tmref_sss_threshold(const char *waveform_file, uint64_t total_samples, int m, const float *queries,
+                            int query_count, float correlation, int merge_offset, int lower_bounds, int threads,
+                            int paa_segments, const char *out_prefix)
+    {
+        try
+        {
+            SkipSequentialScan scan(threads, paa_segments, merge_offset, 0, lower_bounds != 0);
+            scan.build(waveform_file, total_samples, m);
+            scan.search_threshold(queries, query_count, correlation, out_prefix);
+            return 0;
+        }
+        catch (const std::exception &)
+        {
+            return -1;
+        }
+    }
+
+    int tmref_sss_stats(const char *waveform_file, uint64_t total_samples, int m, int threads, float *means,
+                        float *stds)
+    {
+        try
+        {
+            SkipSequentialScan scan(threads, 8, 0, 0, false);
+            scan.build(waveform_file, total_samples, m);
+            std::memcpy(means, scan.means.data(), scan.means.size() * sizeof(float));
+            std::memcpy(stds, scan.stds.data(), scan.stds.size() * sizeof(float));
+            return 0;
+        }
+        catch (const std::exception &)
+        {
+            return -1;
+        }
+    }
+
+    float tmref_l2_dist(const float *query_znorm, const float *raw, uint64_t start, int m, float mean, float stddev,
+                        float bound, const int *block_order, int *blocks_visited)
+    {
+        return l2_dist_znorm_subsequence(query_znorm, raw, start, m, mean, stddev, bound, block_order, blocks_visited);
+    }
+
+    void tmref_znormalize(float *values, int len) { znormalize_inplace(values, len); }
+
+    void tmref_block_order(const float *query_znorm, int m, int *order)
+    {
+        const std::vector<int> o = query_block_order(query_znorm, m);
+        std::memcpy(order, o.data(), o.size() * sizeof(int));
+    }
+
+    float tmref_cc_to_ed(float cc, int m) { return cc_to_ed(cc, m); }
+    float tmref_ed_to_cc(float ed, int m) { return ed_to_cc(ed, m); }
+
+    // Canonical exclusion selection (ZnormSearch.hpp:170-189); returns the number kept.
+    int tmref_select_knn(const uint64_t *positions, const float *distances, uint64_t count, int k, int merge_offset,
+                         uint64_t *out_positions, float *out_distances)
+    {
+        std::vector<KnnCandidate> c(count);
+        for (uint64_t i = 0; i < count; i++)
+            c[i] = {positions[i], distances[i]};
+        const std::vector<KnnCandidate> kept = select_knn_with_exclusion(c, k, merge_offset);
+        for (size_t i = 0; i < kept.size(); i++)
+        {
+            out_positions[i] = kept[i].first;
+            out_distances[i] = kept[i].second;
+        }
+        return static_cast<int>(kept.size());
+    }
+
+    // Exclusion-zone bound queue (iSAXPqueue.cpp:471-520): offers (distance, position)
+    // pairs in order and returns the final queue contents.
+    void tmref_pqueue_offset(const float *distances, const uint64_t *positions, uint64_t count, int size,
+                             int merge_offset, float *out_knn, int64_t *out_positions)
+    {
+        pqueue_bsf *q = pqueue_bsf_init(size);
+        for (uint64_t i = 0; i < count; i++)
+            if (distances[i] < q->knn[size - 1])
+                pqueue_bsf_insert_offset(q, distances[i], positions[i], nullptr, merge_offset);
+        for (int i = 0; i < size; i++)
+        {
+            out_knn[i] = q->knn[i];
+            out_positions[i] = q->position[i];
+        }
+        pqueue_bsf_destroy(q);
+    }
+}
