@@ -1,0 +1,162 @@
+/*
+ * tremor_b200 — C ABI of the B200 exact template-matching scan.
+ *
+ * One context holds one single-channel float32 waveform resident on one GPU,
+ * plus per-template-length window statistics. Every search returns exactly the
+ * answer sets of TREMOR's exact scan (the sequential / skip-sequential scan and
+ * the scan and FFT branches of the adaptive planner): the same kNN answers with
+ * the same exclusion-zone rule, the same threshold hits after the same merge,
+ * and bit-identical FP32 distances.
+ *
+ * Conventions
+ *   - every function returns int: TM_OK (0) or a negative TM_ERR_* code; nothing
+ *     exits or throws across this boundary; tm_last_error() describes the last
+ *     failure of a context;
+ *   - host buffers are caller-owned; device buffers are owned by the library;
+ *   - positions are window start indices into the whole waveform (uint64),
+ *     distances are squared z-normalised Euclidean distances (FP32),
+ *     ED^2 = 2 m (1 - correlation) (ZnormSearch.hpp:23-31);
+ *   - a context may be used by one host thread at a time.
+ *
+ * Reference interfaces replaced (paths inside the reference project):
+ *   tm_ctx_create + tm_prepare_length  <- SkipSequentialScan::build
+ *        (tremor/algos/sss/SkipSequential.hpp:42; stats SkipSequential.cpp:157-190)
+ *        and Tremor::buildIndexLongSequence (tremor/algos/htremor/Tremor.hpp:168-169;
+ *        stats tremor/algos/tremor/indexing.cpp:128-152)
+ *   tm_search_knn        <- SkipSequentialScan::search_knn (SkipSequential.hpp:48) and
+ *                           Tremor::searchIndex in kNN mode (Tremor.hpp:172)
+ *   tm_search_threshold  <- SkipSequentialScan::search_threshold (SkipSequential.hpp:45)
+ *                           and Tremor::searchIndex in threshold mode
+ *   tm_scan_batch        <- the per-template scan/FFT branches of the planner,
+ *                           refine_in_position_order / fft_in_position_order
+ *                           (tremor/algos/tremor/Tremor.cpp:1946, :2088), many
+ *                           templates (of any lengths and modes) per call
+ */
+#ifndef TREMOR_B200_H
+#define TREMOR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TM_OK 0
+#define TM_ERR_ARGUMENT (-1)  /* invalid argument (sizes, null pointers, m > n) */
+#define TM_ERR_CUDA (-2)      /* a CUDA call failed; see tm_last_error */
+#define TM_ERR_NO_MEMORY (-3) /* device or host allocation failed */
+#define TM_ERR_STATE (-4)     /* call not valid in the context's state */
+#define TM_ERR_CAPACITY (-5)  /* caller buffer too small; the needed size was written */
+#define TM_ERR_NO_DEVICE (-6) /* no usable sm_100 device */
+
+/* TREMOR_MISSING_VALUE (ZnormSearch.hpp:21): a missing sample counts as 0; a window
+ * whose first sample is missing is not searched. */
+#define TM_MISSING_VALUE (-100000.0f)
+
+/* query modes, as Tremor::setModeKNN / setModeThreshold (Tremor.hpp:152-153) */
+#define TM_MODE_THRESHOLD 0
+#define TM_MODE_KNN 1
+
+/* contraction kernels */
+#define TM_KERNEL_AUTO 0       /* split-BF16 tensor cores where available, else FP32 */
+#define TM_KERNEL_FP32 1       /* plain FP32 sliding dot product (CUDA cores) */
+#define TM_KERNEL_SPLIT_BF16 2 /* tcgen05 split-BF16 Hankel contraction */
+
+/* request flags */
+#define TM_FLAG_ZNORMALIZED 1u /* templ is already z-normalised (QaWorkerData::ts) */
+
+typedef struct tm_ctx tm_ctx;
+typedef struct tm_result tm_result;
+typedef struct tm_batch tm_batch;
+
+/* One template request (kNN or threshold). */
+typedef struct tm_request
+{
+    const float *templ;    /* m samples, host memory */
+    int32_t m;             /* template length (>= 1) */
+    int32_t mode;          /* TM_MODE_KNN or TM_MODE_THRESHOLD */
+    int32_t k;             /* kNN: answers wanted (>= 1) */
+    int32_t merge_offset;  /* exclusion zone / threshold merge offset (>= 0) */
+    float correlation;     /* threshold: minimum Pearson correlation */
+    uint32_t flags;        /* TM_FLAG_* */
+} tm_request;
+
+/* ---- context ------------------------------------------------------------------ */
+
+/* Copies the host waveform raw[0..n) to `device` and makes it resident. */
+int tm_ctx_create(const float *raw, uint64_t n, int device, tm_ctx **out);
+int tm_ctx_destroy(tm_ctx *ctx);
+/* Text of the last error of this context ("" if none). */
+const char *tm_last_error(const tm_ctx *ctx);
+/* TM_KERNEL_*; default TM_KERNEL_AUTO. */
+int tm_set_kernel(tm_ctx *ctx, int kernel);
+/* Restricts searches to windows [first, first + count) (a data partition as in
+ * SkipSequential.cpp:218-226); default: every window of every length. */
+int tm_set_window_range(tm_ctx *ctx, uint64_t first, uint64_t count);
+/* Computes (or reuses) the statistics of every window of length m. Optional: the
+ * searches prepare the lengths they need. */
+int tm_prepare_length(tm_ctx *ctx, int m);
+/* The statistics the reference keeps per window (SkipSequential.hpp:74): float mean and
+ * population std, (0, 0) for windows whose first sample is missing and std 0 for
+ * constant windows. Bit-identical to the reference's two-pass FP64 values. Writes
+ * count floats to each array, for windows [first, first + count). */
+int tm_window_stats(tm_ctx *ctx, int m, uint64_t first, uint64_t count, float *mean, float *stddev);
+
+/* ---- searches ------------------------------------------------------------------ */
+
+/* kNN for `count` raw templates of length m (row-major count x m): I, D are count x k,
+ * answers in order of (distance, position), unfilled slots (0, FLT_MAX) as the
+ * reference's writers and Tremor::searchIndex (Tremor.cpp:3699-3718). */
+int tm_search_knn(tm_ctx *ctx, const float *queries, int count, int m, int k, int merge_offset, uint64_t *I,
+                  float *D);
+
+/* Threshold search: every window with correlation >= `correlation`, merged by position
+ * with the merge offset (SkipSequential.cpp:358-370). Results in *out. */
+int tm_search_threshold(tm_ctx *ctx, const float *queries, int count, int m, float correlation, int merge_offset,
+                        tm_result **out);
+
+/* Any mix of kNN and threshold requests of any lengths in one call. */
+int tm_scan_batch(tm_ctx *ctx, const tm_request *requests, int count, tm_result **out);
+
+/* A batch prepared once (host z-normalisation, block orders, error-bound constants)
+ * whose templates stay resident on the device; run it any number of times. The
+ * serving loop and repeated searches of one template set use it; tm_scan_batch is
+ * create + run + destroy. A batch belongs to the context that created it. */
+int tm_batch_create(tm_ctx *ctx, const tm_request *requests, int count, tm_batch **out);
+int tm_batch_run(tm_ctx *ctx, tm_batch *batch, tm_result **out);
+int tm_batch_destroy(tm_batch *batch);
+/* Host-to-device bytes tm_batch_create copied (templates, orders, constants). */
+int tm_batch_h2d_bytes(const tm_batch *batch, uint64_t *bytes);
+
+/* Results: per request, its answers (kNN: exactly k, padded; threshold: the merged hits). */
+int tm_result_count(const tm_result *res, int request, uint64_t *count);
+int tm_result_get(const tm_result *res, int request, uint64_t *positions, float *distances, uint64_t capacity);
+void tm_result_free(tm_result *res);
+
+/* ---- conversions (ZnormSearch.hpp:23-31, bit-identical) -------------------------- */
+float tm_cc_to_ed(float correlation, int m);
+float tm_ed_to_cc(float distance, int m);
+
+/* ---- instrumentation -------------------------------------------------------------- */
+
+/* When enabled, the dominant contraction kernel is bracketed by CUDA events on the
+ * library's stream and its launches and device time are accumulated. */
+int tm_profile_enable(tm_ctx *ctx, int enable);
+/* Name of the dominant kernel, its launch count, total device milliseconds, the
+ * algorithmic flops it performed (2 m per template-window pair) and the number of
+ * kernel launches of this library since the last reset. Resets the counters. */
+int tm_profile_read(tm_ctx *ctx, char *name, size_t name_capacity, int64_t *launches, double *milliseconds,
+                    double *flops, int64_t *all_launches);
+/* Device-to-host bytes the searches of this context copied since the last call (resets). */
+int tm_d2h_bytes(tm_ctx *ctx, uint64_t *bytes);
+/* The context's CUDA stream (a cudaStream_t), for callers that order or time work on it. */
+int tm_ctx_stream(tm_ctx *ctx, void **stream);
+/* Candidates re-scored exactly in the last search (diagnostic). */
+int tm_last_candidates(const tm_ctx *ctx, uint64_t *count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

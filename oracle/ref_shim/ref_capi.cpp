@@ -11,6 +11,7 @@
 //   tmref_l2_dist / tmref_znormalize / tmref_block_order / tmref_select_knn :
 //       the inline building blocks of ZnormSearch.hpp, for bit-level pinning.
 #include <cfloat>
+#include <chrono>
 #include <cstdint>
 #include <cstring>
 #include <exception>
@@ -74,6 +75,47 @@ extern "C"
             return -1;
         }
     }
+
+    // A scan built once (SkipSequentialScan::build) and searched many times, with the
+    // template counter rewound between searches; the searches are timed alone.
+    void *tmref_sss_create(const char *waveform_file, uint64_t total_samples, int m, int k_unused, int merge_offset,
+                           int lower_bounds, int threads, int paa_segments)
+    {
+        (void)k_unused;
+        try
+        {
+            auto *scan = new SkipSequentialScan(threads, paa_segments, merge_offset, 0, lower_bounds != 0);
+            scan->build(waveform_file, total_samples, m);
+            return scan;
+        }
+        catch (const std::exception &)
+        {
+            return nullptr;
+        }
+    }
+
+    // Seconds of SkipSequentialScan::search_knn / search_threshold (negative on failure).
+    double tmref_sss_search(void *handle, const float *queries, int query_count, int knn, int k, float correlation,
+                            const char *out)
+    {
+        auto *scan = static_cast<SkipSequentialScan *>(handle);
+        try
+        {
+            *scan->counter = 0;
+            const auto t0 = std::chrono::steady_clock::now();
+            if (knn)
+                scan->search_knn(queries, query_count, k, out);
+            else
+                scan->search_threshold(queries, query_count, correlation, out);
+            return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        }
+        catch (const std::exception &)
+        {
+            return -1.0;
+        }
+    }
+
+    void tmref_sss_destroy(void *handle) { delete static_cast<SkipSequentialScan *>(handle); }
 
     float tmref_l2_dist(const float *query_znorm, const float *raw, uint64_t start, int m, float mean, float stddev,
                         float bound, const int *block_order, int *blocks_visited)

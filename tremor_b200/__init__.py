@@ -1,0 +1,291 @@
+"""tremor_b200 — TREMOR's exact template-matching scan on one B200.
+
+Python binding of the C ABI in include/tremor_b200.h (libtremor_b200.so, built by
+``python -m tremor_b200.build``). The search calls mirror the reference's
+``SkipSequentialScan`` (tremor/algos/sss/SkipSequential.hpp:32-78):
+
+    ctx = Context(waveform)                       # ~ SkipSequentialScan::build
+    I, D = ctx.search_knn(queries, k, merge)      # ~ search_knn (Tremor::searchIndex I/D)
+    hits = ctx.search_threshold(queries, 0.8, 0)  # ~ search_threshold
+    rows = knn_rows(I, D, m)                      # the reference's CSV rows
+
+There is no CPU fallback: without the native library or a CUDA device every call
+raises.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+from typing import List, Sequence, Tuple
+
+import numpy as np
+
+__all__ = ['Context', 'Batch', 'TremorError', 'Request', 'knn_rows', 'threshold_rows', 'load_library',
+           'MODE_KNN', 'MODE_THRESHOLD', 'KERNEL_AUTO', 'KERNEL_FP32', 'KERNEL_SPLIT_BF16', 'MISSING_VALUE']
+
+MODE_THRESHOLD = 0
+MODE_KNN = 1
+KERNEL_AUTO, KERNEL_FP32, KERNEL_SPLIT_BF16 = 0, 1, 2
+FLAG_ZNORMALIZED = 1
+MISSING_VALUE = np.float32(-100000.0)
+FLT_MAX = float(np.finfo(np.float32).max)
+
+_ERRORS = {-1: 'invalid argument', -2: 'CUDA error', -3: 'out of memory', -4: 'invalid state',
+           -5: 'buffer too small', -6: 'no usable sm_100 device'}
+
+LIB_PATH = Path(__file__).resolve().parent / 'libtremor_b200.so'
+_lib = None
+_vp = ctypes.c_void_p
+
+
+class TremorError(RuntimeError):
+    def __init__(self, code: int, detail: str = ''):
+        super().__init__(f'{_ERRORS.get(code, "error")} ({code}){": " + detail if detail else ""}')
+        self.code = code
+
+
+class _Request(ctypes.Structure):
+    _fields_ = [('templ', _vp), ('m', ctypes.c_int32), ('mode', ctypes.c_int32), ('k', ctypes.c_int32),
+                ('merge_offset', ctypes.c_int32), ('correlation', ctypes.c_float), ('flags', ctypes.c_uint32)]
+
+
+def load_library():
+    """Loads libtremor_b200.so; raises ImportError when it was not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(f'{LIB_PATH} is missing: build it with `python -m tremor_b200.build`')
+    lib = ctypes.CDLL(str(LIB_PATH))
+    i, u64, f, pp = ctypes.c_int, ctypes.c_uint64, ctypes.c_float, ctypes.POINTER(_vp)
+    sig = {
+        'tm_ctx_create': (i, [_vp, u64, i, pp]),
+        'tm_ctx_destroy': (i, [_vp]),
+        'tm_last_error': (ctypes.c_char_p, [_vp]),
+        'tm_set_kernel': (i, [_vp, i]),
+        'tm_set_window_range': (i, [_vp, u64, u64]),
+        'tm_prepare_length': (i, [_vp, i]),
+        'tm_window_stats': (i, [_vp, i, u64, u64, _vp, _vp]),
+        'tm_search_knn': (i, [_vp, _vp, i, i, i, i, _vp, _vp]),
+        'tm_search_threshold': (i, [_vp, _vp, i, i, f, i, pp]),
+        'tm_scan_batch': (i, [_vp, _vp, i, pp]),
+        'tm_result_count': (i, [_vp, i, ctypes.POINTER(u64)]),
+        'tm_result_get': (i, [_vp, i, _vp, _vp, u64]),
+        'tm_result_free': (None, [_vp]),
+        'tm_cc_to_ed': (f, [f, i]),
+        'tm_ed_to_cc': (f, [f, i]),
+        'tm_profile_enable': (i, [_vp, i]),
+        'tm_profile_read': (i, [_vp, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_int64),
+                                ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                ctypes.POINTER(ctypes.c_int64)]),
+        'tm_last_candidates': (i, [_vp, ctypes.POINTER(u64)]),
+        'tm_batch_create': (i, [_vp, _vp, i, pp]),
+        'tm_batch_run': (i, [_vp, _vp, pp]),
+        'tm_batch_destroy': (i, [_vp]),
+        'tm_batch_h2d_bytes': (i, [_vp, ctypes.POINTER(u64)]),
+        'tm_d2h_bytes': (i, [_vp, ctypes.POINTER(u64)]),
+        'tm_ctx_stream': (i, [_vp, pp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_vp)
+
+
+class Request:
+    """One template request (kNN or threshold), as tm_request."""
+
+    def __init__(self, template, mode=MODE_KNN, k=1, merge_offset=0, correlation=0.0, znormalized=False):
+        self.template = np.ascontiguousarray(template, dtype=np.float32)
+        self.mode, self.k, self.merge_offset = int(mode), int(k), int(merge_offset)
+        self.correlation = float(correlation)
+        self.flags = FLAG_ZNORMALIZED if znormalized else 0
+
+
+class Context:
+    """A waveform resident on one GPU (tm_ctx)."""
+
+    def __init__(self, waveform: np.ndarray, device: int = 0):
+        self._lib = load_library()
+        self.waveform = np.ascontiguousarray(waveform, dtype=np.float32)
+        self.n = len(self.waveform)
+        h = _vp()
+        rc = self._lib.tm_ctx_create(_ptr(self.waveform), self.n, device, ctypes.byref(h))
+        if rc != 0:
+            raise TremorError(rc, 'tm_ctx_create')
+        self._h = h
+
+    def close(self):
+        if getattr(self, '_h', None):
+            self._lib.tm_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc):
+        if rc != 0:
+            raise TremorError(rc, self._lib.tm_last_error(self._h).decode())
+
+    def set_kernel(self, kernel: int):
+        self._check(self._lib.tm_set_kernel(self._h, kernel))
+
+    def set_window_range(self, first: int, count: int):
+        self._check(self._lib.tm_set_window_range(self._h, first, count))
+
+    def prepare_length(self, m: int):
+        self._check(self._lib.tm_prepare_length(self._h, m))
+
+    def window_stats(self, m: int, first: int = 0, count: int | None = None):
+        """The reference's per-window (mean, std) floats (SkipSequential.cpp:157-190)."""
+        if count is None:
+            count = self.n - m + 1 - first
+        mean = np.zeros(count, np.float32)
+        std = np.zeros(count, np.float32)
+        self._check(self._lib.tm_window_stats(self._h, m, first, count, _ptr(mean), _ptr(std)))
+        return mean, std
+
+    def search_knn(self, queries: np.ndarray, k: int, merge_offset: int = 0) -> Tuple[np.ndarray, np.ndarray]:
+        q = np.ascontiguousarray(np.atleast_2d(queries), dtype=np.float32)
+        I = np.zeros((q.shape[0], k), np.uint64)
+        D = np.zeros((q.shape[0], k), np.float32)
+        self._check(self._lib.tm_search_knn(self._h, _ptr(q), q.shape[0], q.shape[1], k, merge_offset,
+                                            _ptr(I), _ptr(D)))
+        return I, D
+
+    def search_threshold(self, queries: np.ndarray, correlation: float, merge_offset: int = 0):
+        q = np.ascontiguousarray(np.atleast_2d(queries), dtype=np.float32)
+        res = _vp()
+        self._check(self._lib.tm_search_threshold(self._h, _ptr(q), q.shape[0], q.shape[1], correlation,
+                                                  merge_offset, ctypes.byref(res)))
+        return self._take(res, q.shape[0])
+
+    @staticmethod
+    def _requests(requests: Sequence[Request]):
+        arr = (_Request * len(requests))()
+        for i, r in enumerate(requests):
+            arr[i] = _Request(_ptr(r.template), len(r.template), r.mode, r.k, r.merge_offset, r.correlation,
+                              r.flags)
+        return arr
+
+    def scan_batch(self, requests: Sequence[Request]):
+        """Answers (positions, distances) per request, any mix of modes and lengths."""
+        arr = self._requests(requests)
+        res = _vp()
+        self._check(self._lib.tm_scan_batch(self._h, arr, len(requests), ctypes.byref(res)))
+        return self._take(res, len(requests))
+
+    def batch(self, requests: Sequence[Request]) -> 'Batch':
+        """A prepared batch whose templates stay resident on the device (tm_batch)."""
+        return Batch(self, requests)
+
+    def stream(self) -> int:
+        """The context's cudaStream_t as an integer handle."""
+        s = _vp()
+        self._check(self._lib.tm_ctx_stream(self._h, ctypes.byref(s)))
+        return s.value or 0
+
+    def d2h_bytes(self) -> int:
+        n = ctypes.c_uint64(0)
+        self._check(self._lib.tm_d2h_bytes(self._h, ctypes.byref(n)))
+        return n.value
+
+    def _take(self, res, count) -> List[Tuple[np.ndarray, np.ndarray]]:
+        out = []
+        try:
+            for i in range(count):
+                n = ctypes.c_uint64(0)
+                self._check(self._lib.tm_result_count(res, i, ctypes.byref(n)))
+                pos = np.zeros(n.value, np.uint64)
+                dist = np.zeros(n.value, np.float32)
+                self._check(self._lib.tm_result_get(res, i, _ptr(pos), _ptr(dist), n.value))
+                out.append((pos, dist))
+        finally:
+            self._lib.tm_result_free(res)
+        return out
+
+    def profile_enable(self, on: bool = True):
+        self._check(self._lib.tm_profile_enable(self._h, 1 if on else 0))
+
+    def profile_read(self):
+        """(kernel name, launches, device ms, algorithmic flops, all library launches); resets."""
+        name = ctypes.create_string_buffer(64)
+        launches, allk = ctypes.c_int64(0), ctypes.c_int64(0)
+        ms, flops = ctypes.c_double(0), ctypes.c_double(0)
+        self._check(self._lib.tm_profile_read(self._h, name, 64, ctypes.byref(launches), ctypes.byref(ms),
+                                              ctypes.byref(flops), ctypes.byref(allk)))
+        return name.value.decode(), launches.value, ms.value, flops.value, allk.value
+
+    def last_candidates(self) -> int:
+        n = ctypes.c_uint64(0)
+        self._check(self._lib.tm_last_candidates(self._h, ctypes.byref(n)))
+        return n.value
+
+
+class Batch:
+    """Requests prepared once and resident on the device; run() any number of times."""
+
+    def __init__(self, ctx: Context, requests: Sequence[Request]):
+        self.ctx, self.count = ctx, len(requests)
+        self._keep = list(requests)
+        arr = ctx._requests(requests)
+        h = _vp()
+        ctx._check(ctx._lib.tm_batch_create(ctx._h, arr, len(requests), ctypes.byref(h)))
+        self._h = h
+
+    def run(self):
+        res = _vp()
+        self.ctx._check(self.ctx._lib.tm_batch_run(self.ctx._h, self._h, ctypes.byref(res)))
+        return self.ctx._take(res, self.count)
+
+    def h2d_bytes(self) -> int:
+        n = ctypes.c_uint64(0)
+        self.ctx._check(self.ctx._lib.tm_batch_h2d_bytes(self._h, ctypes.byref(n)))
+        return n.value
+
+    def close(self):
+        if getattr(self, '_h', None):
+            self.ctx._lib.tm_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def ed_to_cc(ed: float, m: int) -> float:
+    return load_library().tm_ed_to_cc(float(ed), m)
+
+
+def knn_rows(I: np.ndarray, D: np.ndarray, m: int):
+    """kNN answers as the reference's writer prints them: tID, k, pos, corr (SkipSequential.cpp:461-470)."""
+    lib = load_library()
+    return [[str(q), str(j + 1), str(int(I[q, j])), '%f' % lib.tm_ed_to_cc(float(D[q, j]), m)]
+            for q in range(I.shape[0]) for j in range(I.shape[1])]
+
+
+def threshold_rows(hits, m: int):
+    """Threshold hits as the reference's writer prints them: Query, Counter, Position, Cross Correlation."""
+    lib = load_library()
+    rows = []
+    for q, (pos, dist) in enumerate(hits):
+        for c, (p, d) in enumerate(zip(pos, dist)):
+            rows.append([str(q), str(c), str(int(p)), '%f' % lib.tm_ed_to_cc(float(d), m)])
+    return rows

@@ -1,0 +1,943 @@
+// C ABI of tremor_b200 (include/tremor_b200.h): context, window statistics, batched
+// searches, results. One search of a group of same-length templates runs:
+//
+//   1. host: z-normalise each template (bit-identical to the reference), block order,
+//      epilogue constants;                                        (tm_host.cpp)
+//   2. device: contraction kernel with fused epilogue: threshold candidates and
+//      per-bucket minima for kNN;                (tm_scan_fp32.cu / tm_scan_umma.cu)
+//   3. device, kNN only: bound from bucket minima, list of buckets within it, FP32
+//      re-pass of those buckets emitting the kNN candidates;        (tm_select.cu)
+//   4. device: every candidate re-scored with the reference's exact arithmetic;
+//   5. host: canonical exclusion selection / threshold merge on the exact distances.
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/tremor_b200.h"
+#include "tm_epilogue.cuh"
+#include "tm_host.h"
+#include "tm_internal.cuh"
+
+namespace tmb {
+cudaError_t launch_clean(const float *raw, float *clean, uint64_t n, uint64_t n_total, cudaStream_t s);
+cudaError_t launch_window_stats(const float *clean, const float *raw, uint64_t n, int m, uint64_t w0, uint64_t W,
+                                double2 *suf, float *mean, float *inv, uint8_t *flags, cudaStream_t s);
+cudaError_t launch_reference_stats(const float *raw, int m, uint64_t w0, uint64_t count, float *mean, float *stddev,
+                                   cudaStream_t s);
+cudaError_t launch_scan_fp32(const ScanArgs &a, cudaStream_t s);
+cudaError_t launch_scan_umma(const ScanArgs &a, cudaStream_t s, bool *supported);
+cudaError_t launch_bucket_select(const uint32_t *bmin_u, uint32_t nb, const TemplParam *tp, const int *knn_slots,
+                                 int nk, uint32_t *tkey, cudaStream_t s);
+cudaError_t launch_list_buckets(const uint32_t *bmin_l, uint32_t nb, const int *knn_slots, int nk,
+                                const uint32_t *tkey, uint2 *list, uint32_t *list_count, uint32_t cap, cudaStream_t s);
+cudaError_t launch_passb(const uint2 *list, uint32_t items, const float *x, const float *q, const TemplParam *tp,
+                         const float *mean, const float *inv, const uint32_t *tkey, uint64_t w0, uint32_t W,
+                         Candidate *cand, uint32_t *cand_count, uint32_t cand_cap, cudaStream_t s);
+cudaError_t launch_rescore(const Candidate *cand, uint32_t count, const TemplParam *tp, const float *q,
+                           const int *order, const float *raw, uint64_t w0, float *dist, cudaStream_t s);
+} // namespace tmb
+
+using tmb::Candidate;
+using tmb::TemplParam;
+using tm_host::Hit;
+
+namespace {
+
+struct Failure
+{
+    int code;
+    std::string what;
+};
+
+#define TM_CUDA(call)                                                                                             \
+    do                                                                                                            \
+    {                                                                                                             \
+        cudaError_t e_ = (call);                                                                                  \
+        if (e_ != cudaSuccess)                                                                                    \
+            throw Failure{e_ == cudaErrorMemoryAllocation ? TM_ERR_NO_MEMORY : TM_ERR_CUDA,                      \
+                          std::string(#call) + ": " + cudaGetErrorString(e_)};                                    \
+    } while (0)
+
+// Grow-only device buffer.
+struct DevBuf
+{
+    void *p = nullptr;
+    size_t bytes = 0;
+    void reserve(size_t need)
+    {
+        if (need <= bytes)
+            return;
+        if (p)
+            cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        size_t b = std::max<size_t>(need, 256);
+        TM_CUDA(cudaMalloc(&p, b));
+        bytes = b;
+    }
+    template <class T> T *as() const { return static_cast<T *>(p); }
+    void release()
+    {
+        if (p)
+            cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+};
+
+// Grow-only pinned host buffer.
+struct HostBuf
+{
+    void *p = nullptr;
+    size_t bytes = 0;
+    void reserve(size_t need)
+    {
+        if (need <= bytes)
+            return;
+        if (p)
+            cudaFreeHost(p);
+        p = nullptr;
+        bytes = 0;
+        TM_CUDA(cudaMallocHost(&p, std::max<size_t>(need, 256)));
+        bytes = std::max<size_t>(need, 256);
+    }
+    template <class T> T *as() const { return static_cast<T *>(p); }
+    void release()
+    {
+        if (p)
+            cudaFreeHost(p);
+        p = nullptr;
+        bytes = 0;
+    }
+};
+
+struct LengthStats
+{
+    int m = 0;
+    uint64_t w0 = 0, W = 0;
+    DevBuf mean, inv, flags;
+    uint64_t last_use = 0;
+    size_t bytes() const { return mean.bytes + inv.bytes + flags.bytes; }
+};
+
+constexpr double kU = 5.9604644775390625e-08;   // 2^-24
+constexpr double kE64 = 1.1102230246251565e-16; // 2^-53
+
+} // namespace
+
+struct tm_result
+{
+    std::vector<std::vector<Hit>> answers;
+};
+
+struct tm_ctx
+{
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    uint64_t n = 0;
+    DevBuf raw, clean;
+    uint64_t range_first = 0, range_count = UINT64_MAX;
+    int kernel = TM_KERNEL_AUTO;
+    std::map<int, std::unique_ptr<LengthStats>> lengths;
+    uint64_t use_clock = 0;
+    // scratch
+    DevBuf suf, tkey, bmin_u, bmin_l, list, counters, cand, dist;
+    HostBuf h_q, h_order, h_slots, h_cand, h_dist, h_counters, h_tkey;
+    uint32_t cand_cap = 1u << 22, list_cap = 1u << 20;
+    std::string err;
+    // instrumentation
+    bool profile = false;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string kname;
+    int64_t prof_launches = 0, all_launches = 0;
+    double prof_ms = 0.0, prof_flops = 0.0;
+    uint64_t last_candidates = 0;
+    uint64_t d2h_bytes = 0;
+};
+
+namespace {
+
+int fail(tm_ctx *ctx, const Failure &f)
+{
+    if (ctx)
+        ctx->err = f.what;
+    return f.code;
+}
+
+template <class F> int guarded(tm_ctx *ctx, F body)
+{
+    try
+    {
+        body();
+        if (ctx)
+            ctx->err.clear();
+        return TM_OK;
+    }
+    catch (const Failure &f)
+    {
+        return fail(ctx, f);
+    }
+    catch (const std::bad_alloc &)
+    {
+        return fail(ctx, Failure{TM_ERR_NO_MEMORY, "host allocation failed"});
+    }
+}
+
+void count_launch(tm_ctx *ctx, int k = 1) { ctx->all_launches += k; }
+
+LengthStats &ensure_length(tm_ctx *ctx, int m)
+{
+    auto it = ctx->lengths.find(m);
+    if (it != ctx->lengths.end())
+    {
+        it->second->last_use = ++ctx->use_clock;
+        return *it->second;
+    }
+    const uint64_t total = ctx->n - static_cast<uint64_t>(m) + 1; // windows of the whole waveform
+    const uint64_t w0 = std::min(ctx->range_first, total);
+    const uint64_t W = std::min(ctx->range_count, total - w0);
+    // keep the resident statistics under half of the free memory: evict least recently used
+    size_t free_b = 0, total_b = 0;
+    TM_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t need = W * 9 + 4096;
+    while (!ctx->lengths.empty() && need * 2 > free_b)
+    {
+        auto victim = ctx->lengths.begin();
+        for (auto jt = ctx->lengths.begin(); jt != ctx->lengths.end(); ++jt)
+            if (jt->second->last_use < victim->second->last_use)
+                victim = jt;
+        free_b += victim->second->bytes();
+        victim->second->mean.release();
+        victim->second->inv.release();
+        victim->second->flags.release();
+        ctx->lengths.erase(victim);
+    }
+    auto ls = std::make_unique<LengthStats>();
+    ls->m = m;
+    ls->w0 = w0;
+    ls->W = W;
+    if (W > 0)
+    {
+        ls->mean.reserve(W * sizeof(float) + 64);
+        ls->inv.reserve(W * sizeof(float) + 64);
+        ls->flags.reserve(W + 64);
+        const uint64_t a_count = (w0 + W - 1) / m - w0 / m + 1;
+        ctx->suf.reserve(a_count * static_cast<uint64_t>(m) * sizeof(double2));
+        TM_CUDA(tmb::launch_window_stats(ctx->clean.as<float>(), ctx->raw.as<float>(), ctx->n, m, w0, W,
+                                        ctx->suf.as<double2>(), ls->mean.as<float>(), ls->inv.as<float>(),
+                                        ls->flags.as<uint8_t>(), ctx->stream));
+        count_launch(ctx, 3);
+    }
+    ls->last_use = ++ctx->use_clock;
+    LengthStats &ref = *ls;
+    ctx->lengths[m] = std::move(ls);
+    return ref;
+}
+
+// Epilogue constants of one template (error-bound terms of fast_distance).
+void fill_param(TemplParam &p, int m, double q2, double s1, double gamma_main, double gamma_fp32)
+{
+    const double qn = std::sqrt(q2), qs = qn * std::sqrt(static_cast<double>(m));
+    const double md = static_cast<double>(m);
+    const double safety = 1.25;
+    p.s1 = static_cast<float>(s1);
+    p.c_lin = static_cast<float>(q2 + md);
+    p.a1_main = static_cast<float>(safety * 2.0 * (gamma_main + 6.0 * kU) * qs);
+    p.a1_fp32 = static_cast<float>(safety * 2.0 * (gamma_fp32 + 6.0 * kU) * qs);
+    p.a2 = static_cast<float>(safety * (4.02 * kU * qs + 10.11 * kU * md + 4.0 * kU * (q2 + md)) + 1e-6 * md);
+    p.a3 = static_cast<float>(safety * (md / 16.0 + 40.0) * kU);
+    p.a4 = static_cast<float>(safety * 8.0 * md * md * kE64);
+    p.a5 = static_cast<float>(safety * md * kU * kU);
+    p.a6 = static_cast<float>(safety * 8.0 * kU * std::fabs(s1));
+    p.m = m;
+}
+
+// FP32 chain: one FMA per sample and accumulator; split BF16: three products per
+// sample plus the tensor-core accumulation (truncating adds, 2^-22 per MMA step).
+double gamma_fp32(int m) { return 1.01 * static_cast<double>((m + 63) & ~63) * kU; }
+double gamma_bf16(int m) { return 1.2e-5 + (3.0 * ((m + 63) & ~63) / 16.0 + 16.0) * 2.384185791015625e-07; }
+
+// One group of same-length requests of a batch, prepared on the host and resident on
+// the device (templates, block orders, epilogue constants).
+struct GroupPlan
+{
+    int m = 0, T = 0, T_pad = 0, m_pad = 0, nblk = 0, nk = 0;
+    bool umma_constants = false;
+    std::vector<int> index; // request index of each slot
+    std::vector<int> mode, k, merge;
+    std::vector<float> thr; // threshold distance per slot
+    std::vector<TemplParam> htp;
+    DevBuf q, order, tp, slots;
+    void release()
+    {
+        q.release();
+        order.release();
+        tp.release();
+        slots.release();
+    }
+};
+
+} // namespace
+
+struct tm_batch
+{
+    int count = 0;
+    std::vector<GroupPlan> groups;
+    uint64_t h2d_bytes = 0;
+    ~tm_batch()
+    {
+        for (GroupPlan &g : groups)
+            g.release();
+    }
+};
+
+namespace {
+
+// Host preparation of one group (bit-identical template z-normalisation and block
+// order, epilogue constants) and its upload.
+void prepare_group(tm_ctx *ctx, int m, const std::vector<int> &idx, const tm_request *reqs, GroupPlan &g,
+                   uint64_t &h2d)
+{
+    g.m = m;
+    g.T = static_cast<int>(idx.size());
+    g.T_pad = (g.T + 63) & ~63;
+    g.m_pad = (m + 63) & ~63;
+    g.nblk = std::max(1, m / tm_host::kZnormBlock);
+    g.umma_constants = ctx->kernel != TM_KERNEL_FP32;
+    g.index = idx;
+    const int T = g.T, T_pad = g.T_pad, m_pad = g.m_pad, nblk = g.nblk;
+    ctx->h_q.reserve(sizeof(float) * static_cast<size_t>(T_pad) * m_pad);
+    ctx->h_order.reserve(sizeof(int) * static_cast<size_t>(T) * nblk);
+    ctx->h_slots.reserve(sizeof(int) * T);
+    float *hq = ctx->h_q.as<float>();
+    int *ho = ctx->h_order.as<int>();
+    int *hslots = ctx->h_slots.as<int>();
+    std::memset(hq, 0, sizeof(float) * static_cast<size_t>(T_pad) * m_pad);
+    std::memset(ho, 0, sizeof(int) * static_cast<size_t>(T) * nblk);
+    g.htp.assign(T_pad, TemplParam{});
+    g.mode.assign(T, 0);
+    g.k.assign(T, 0);
+    g.merge.assign(T, 0);
+    g.thr.assign(T, 0.0f);
+    g.nk = 0;
+    for (int t = 0; t < T; t++)
+    {
+        const tm_request *r = &reqs[idx[t]];
+        float *q = hq + static_cast<size_t>(t) * m_pad;
+        std::memcpy(q, r->templ, sizeof(float) * m);
+        if (!(r->flags & TM_FLAG_ZNORMALIZED))
+            tm_host::znormalize(q, m);
+        tm_host::block_order(q, m, ho + static_cast<size_t>(t) * nblk);
+        double q2 = 0.0, s1 = 0.0;
+        for (int i = 0; i < m; i++)
+        {
+            q2 += static_cast<double>(q[i]) * q[i];
+            s1 += q[i];
+        }
+        TemplParam &p = g.htp[t];
+        fill_param(p, m, q2, s1, g.umma_constants ? gamma_bf16(m) : gamma_fp32(m), gamma_fp32(m));
+        p.mode = g.mode[t] = r->mode;
+        p.k = g.k[t] = r->k;
+        p.merge = g.merge[t] = r->merge_offset;
+        p.q_offset = static_cast<int64_t>(t) * m_pad;
+        p.order_offset = static_cast<int64_t>(t) * nblk;
+        if (r->mode == TM_MODE_KNN)
+            hslots[g.nk++] = t;
+        else
+            p.thr_ed = g.thr[t] = tm_host::cc_to_ed(r->correlation, m);
+    }
+    for (int t = T; t < T_pad; t++)
+    {
+        g.htp[t].mode = TM_MODE_THRESHOLD;
+        g.htp[t].thr_ed = -FLT_MAX;
+        g.htp[t].m = m;
+    }
+    cudaStream_t s = ctx->stream;
+    g.q.reserve(sizeof(float) * static_cast<size_t>(T_pad) * m_pad);
+    g.order.reserve(sizeof(int) * static_cast<size_t>(T) * nblk);
+    g.tp.reserve(sizeof(TemplParam) * T_pad);
+    g.slots.reserve(sizeof(int) * std::max(g.nk, 1));
+    TM_CUDA(cudaMemcpyAsync(g.q.p, hq, sizeof(float) * static_cast<size_t>(T_pad) * m_pad, cudaMemcpyHostToDevice, s));
+    TM_CUDA(cudaMemcpyAsync(g.order.p, ho, sizeof(int) * static_cast<size_t>(T) * nblk, cudaMemcpyHostToDevice, s));
+    TM_CUDA(cudaMemcpyAsync(g.tp.p, g.htp.data(), sizeof(TemplParam) * T_pad, cudaMemcpyHostToDevice, s));
+    if (g.nk > 0)
+        TM_CUDA(cudaMemcpyAsync(g.slots.p, hslots, sizeof(int) * g.nk, cudaMemcpyHostToDevice, s));
+    // the staging buffers are reused by the next group: finish the copies first
+    TM_CUDA(cudaStreamSynchronize(s));
+    h2d += sizeof(float) * static_cast<uint64_t>(T) * m + sizeof(int) * static_cast<uint64_t>(T) * nblk +
+           sizeof(TemplParam) * T_pad;
+}
+
+// Device pipeline and selection for one prepared group; writes answers[index].
+void execute_group(tm_ctx *ctx, GroupPlan &g, std::vector<std::vector<Hit>> &answers)
+{
+    const int m = g.m;
+    LengthStats &ls = ensure_length(ctx, m);
+    const int T = g.T, T_pad = g.T_pad, m_pad = g.m_pad, nk = g.nk;
+    const uint64_t w0 = ls.w0, W = ls.W;
+    if (W == 0)
+    {
+        for (int t = 0; t < T; t++)
+            answers[g.index[t]] = g.mode[t] == TM_MODE_KNN
+                                      ? std::vector<Hit>(static_cast<size_t>(g.k[t]), Hit{0, FLT_MAX})
+                                      : std::vector<Hit>();
+        return;
+    }
+    if (W >= (1ull << 32))
+        throw Failure{TM_ERR_ARGUMENT, "more than 2^32 - 1 windows in one range; split the range"};
+    cudaStream_t s = ctx->stream;
+    bool use_umma = ctx->kernel != TM_KERNEL_FP32;
+    if (use_umma != g.umma_constants) // kernel changed since preparation: refresh the bound constants
+    {
+        for (int t = 0; t < T; t++)
+            g.htp[t].a1_main = use_umma ? g.htp[t].a1_main : g.htp[t].a1_fp32;
+        if (use_umma)
+            throw Failure{TM_ERR_STATE, "batch prepared for the FP32 kernel; prepare it again"};
+        TM_CUDA(cudaMemcpyAsync(g.tp.p, g.htp.data(), sizeof(TemplParam) * T_pad, cudaMemcpyHostToDevice, s));
+        g.umma_constants = false;
+    }
+    ctx->tkey.reserve(sizeof(uint32_t) * T);
+
+    const uint32_t nb = static_cast<uint32_t>((W + tmb::kBucket - 1) / tmb::kBucket);
+    if (nk > 0)
+    {
+        ctx->bmin_u.reserve(sizeof(uint32_t) * static_cast<size_t>(T) * nb);
+        ctx->bmin_l.reserve(sizeof(uint32_t) * static_cast<size_t>(T) * nb);
+    }
+    ctx->counters.reserve(4 * sizeof(uint32_t));
+    ctx->h_counters.reserve(4 * sizeof(uint32_t));
+    uint32_t *hc = ctx->h_counters.as<uint32_t>();
+
+    uint32_t ncand = 0;
+    for (int attempt = 0; attempt < 3; attempt++)
+    {
+        ctx->cand.reserve(sizeof(Candidate) * static_cast<size_t>(ctx->cand_cap));
+        if (nk > 0)
+        {
+            TM_CUDA(cudaMemsetAsync(ctx->bmin_u.p, 0xff, sizeof(uint32_t) * static_cast<size_t>(T) * nb, s));
+            TM_CUDA(cudaMemsetAsync(ctx->bmin_l.p, 0xff, sizeof(uint32_t) * static_cast<size_t>(T) * nb, s));
+        }
+        TM_CUDA(cudaMemsetAsync(ctx->counters.p, 0, 4 * sizeof(uint32_t), s));
+        uint32_t *d_cand_count = ctx->counters.as<uint32_t>();
+        uint32_t *d_list_count = d_cand_count + 1;
+
+        tmb::ScanArgs a{};
+        a.x = ctx->clean.as<float>();
+        a.q = g.q.as<float>();
+        a.tp = g.tp.as<TemplParam>();
+        a.mean = ls.mean.as<float>();
+        a.inv = ls.inv.as<float>();
+        a.w0 = w0;
+        a.W = static_cast<uint32_t>(W);
+        a.m_pad = m_pad;
+        a.T = T;
+        a.bmin_u = ctx->bmin_u.as<uint32_t>();
+        a.bmin_l = ctx->bmin_l.as<uint32_t>();
+        a.nb = nb;
+        a.cand = ctx->cand.as<Candidate>();
+        a.cand_count = d_cand_count;
+        a.cand_cap = ctx->cand_cap;
+
+        // 2. contraction with fused epilogue
+        if (ctx->profile)
+            TM_CUDA(cudaEventRecord(ctx->ev0, s));
+        bool ran_umma = false;
+        if (use_umma)
+        {
+            bool supported = false;
+            TM_CUDA(tmb::launch_scan_umma(a, s, &supported));
+            ran_umma = supported;
+            if (!supported && ctx->kernel == TM_KERNEL_SPLIT_BF16)
+                throw Failure{TM_ERR_STATE, "split-BF16 kernel does not support this length"};
+        }
+        if (!ran_umma)
+        {
+            if (g.umma_constants) // constants were computed for the tensor-core kernel: use FP32's
+            {
+                for (int t = 0; t < T; t++)
+                    g.htp[t].a1_main = g.htp[t].a1_fp32;
+                TM_CUDA(cudaMemcpyAsync(g.tp.p, g.htp.data(), sizeof(TemplParam) * T_pad, cudaMemcpyHostToDevice, s));
+                g.umma_constants = false;
+            }
+            TM_CUDA(tmb::launch_scan_fp32(a, s));
+        }
+        count_launch(ctx);
+        if (ctx->profile)
+        {
+            TM_CUDA(cudaEventRecord(ctx->ev1, s));
+            TM_CUDA(cudaEventSynchronize(ctx->ev1));
+            float ms = 0.0f;
+            TM_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+            ctx->kname = ran_umma ? "k_scan_umma" : "k_scan_fp32";
+            ctx->prof_launches++;
+            ctx->prof_ms += ms;
+            ctx->prof_flops += 2.0 * m * static_cast<double>(W) * T;
+        }
+
+        // 3. kNN bound, bucket list, FP32 re-pass
+        if (nk > 0)
+        {
+            TM_CUDA(tmb::launch_bucket_select(ctx->bmin_u.as<uint32_t>(), nb, g.tp.as<TemplParam>(),
+                                              g.slots.as<int>(), nk, ctx->tkey.as<uint32_t>(), s));
+            for (int la = 0; la < 3; la++)
+            {
+                ctx->list.reserve(sizeof(uint2) * static_cast<size_t>(ctx->list_cap));
+                TM_CUDA(cudaMemsetAsync(d_list_count, 0, sizeof(uint32_t), s));
+                TM_CUDA(tmb::launch_list_buckets(ctx->bmin_l.as<uint32_t>(), nb, g.slots.as<int>(), nk,
+                                                 ctx->tkey.as<uint32_t>(), ctx->list.as<uint2>(), d_list_count,
+                                                 ctx->list_cap, s));
+                TM_CUDA(cudaMemcpyAsync(hc + 1, d_list_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+                TM_CUDA(cudaStreamSynchronize(s));
+                count_launch(ctx, 2);
+                if (hc[1] <= ctx->list_cap)
+                    break;
+                ctx->list_cap = hc[1] + hc[1] / 2;
+            }
+            if (hc[1] > ctx->list_cap)
+                throw Failure{TM_ERR_NO_MEMORY, "bucket list overflow"};
+            TM_CUDA(tmb::launch_passb(ctx->list.as<uint2>(), hc[1], ctx->clean.as<float>(), g.q.as<float>(),
+                                      g.tp.as<TemplParam>(), ls.mean.as<float>(), ls.inv.as<float>(),
+                                      ctx->tkey.as<uint32_t>(), w0, static_cast<uint32_t>(W),
+                                      ctx->cand.as<Candidate>(), d_cand_count, ctx->cand_cap, s));
+            if (hc[1] > 0)
+                count_launch(ctx);
+        }
+        TM_CUDA(cudaMemcpyAsync(hc, d_cand_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        TM_CUDA(cudaStreamSynchronize(s));
+        ncand = hc[0];
+        if (ncand <= ctx->cand_cap)
+            break;
+        ctx->cand_cap = ncand + ncand / 2;
+        if (attempt == 2)
+            throw Failure{TM_ERR_NO_MEMORY, "candidate buffer overflow"};
+    }
+
+    // 4. exact re-scoring
+    ctx->dist.reserve(sizeof(float) * std::max<uint32_t>(ncand, 1));
+    TM_CUDA(tmb::launch_rescore(ctx->cand.as<Candidate>(), ncand, g.tp.as<TemplParam>(), g.q.as<float>(),
+                                g.order.as<int>(), ctx->raw.as<float>(), w0, ctx->dist.as<float>(), s));
+    if (ncand > 0)
+        count_launch(ctx);
+    ctx->h_cand.reserve(sizeof(Candidate) * std::max<uint32_t>(ncand, 1));
+    ctx->h_dist.reserve(sizeof(float) * std::max<uint32_t>(ncand, 1));
+    ctx->h_tkey.reserve(sizeof(uint32_t) * std::max(T, 1));
+    if (ncand > 0)
+    {
+        TM_CUDA(cudaMemcpyAsync(ctx->h_cand.p, ctx->cand.p, sizeof(Candidate) * ncand, cudaMemcpyDeviceToHost, s));
+        TM_CUDA(cudaMemcpyAsync(ctx->h_dist.p, ctx->dist.p, sizeof(float) * ncand, cudaMemcpyDeviceToHost, s));
+    }
+    if (nk > 0)
+        TM_CUDA(cudaMemcpyAsync(ctx->h_tkey.p, ctx->tkey.p, sizeof(uint32_t) * T, cudaMemcpyDeviceToHost, s));
+    TM_CUDA(cudaStreamSynchronize(s));
+    ctx->last_candidates += ncand;
+    ctx->d2h_bytes += (sizeof(Candidate) + sizeof(float)) * static_cast<uint64_t>(ncand) + 8 +
+                      (nk > 0 ? sizeof(uint32_t) * T : 0);
+
+    // 5. answers
+    std::vector<std::vector<Hit>> per(T);
+    const Candidate *hcand = ctx->h_cand.as<Candidate>();
+    const float *hdist = ctx->h_dist.as<float>();
+    for (uint32_t i = 0; i < ncand; i++)
+        per[hcand[i].templ].push_back(Hit{w0 + hcand[i].window, hdist[i]});
+    std::vector<uint8_t> flags; // fetched only when some kNN bound is unbounded
+    for (int t = 0; t < T; t++)
+    {
+        std::vector<Hit> &out = answers[g.index[t]];
+        out.clear();
+        if (g.mode[t] == TM_MODE_KNN)
+        {
+            tm_host::select_knn(per[t], g.k[t], g.merge[t], out);
+            const bool unbounded = ctx->h_tkey.as<uint32_t>()[t] == tmb::kEmptyKey;
+            if (static_cast<int>(out.size()) < g.k[t] && unbounded)
+            {
+                // Too few separated windows for a finite bound: the reference's queue never
+                // fills, so its constant windows (distance FLT_MAX) are candidates too.
+                if (flags.empty())
+                {
+                    flags.resize(W);
+                    TM_CUDA(cudaMemcpy(flags.data(), ls.flags.p, W, cudaMemcpyDeviceToHost));
+                }
+                std::vector<Hit> degenerate;
+                for (uint64_t j = 0; j < W; j++)
+                    if ((flags[j] & tmb::kFlagDegenerate) && !(flags[j] & tmb::kFlagMissingStart))
+                        degenerate.push_back(Hit{w0 + j, FLT_MAX});
+                tm_host::extend_knn(degenerate, g.k[t], g.merge[t], out);
+            }
+            while (static_cast<int>(out.size()) < g.k[t])
+                out.push_back(Hit{0, FLT_MAX});
+        }
+        else
+        {
+            std::vector<Hit> hits;
+            hits.reserve(per[t].size());
+            for (const Hit &h : per[t])
+                if (h.dist <= g.thr[t])
+                    hits.push_back(h);
+            tm_host::threshold_merge(hits, g.merge[t], out);
+        }
+    }
+}
+
+void create_batch(tm_ctx *ctx, const tm_request *requests, int count, tm_batch &b)
+{
+    b.count = count;
+    std::map<int, std::vector<int>> by_m;
+    for (int i = 0; i < count; i++)
+        by_m[requests[i].m].push_back(i);
+    b.groups.resize(by_m.size());
+    size_t gi = 0;
+    for (auto &kv : by_m)
+        prepare_group(ctx, kv.first, kv.second, requests, b.groups[gi++], b.h2d_bytes);
+}
+
+void run_batch(tm_ctx *ctx, tm_batch &b, tm_result &res)
+{
+    res.answers.assign(static_cast<size_t>(b.count), std::vector<Hit>());
+    ctx->last_candidates = 0;
+    for (GroupPlan &g : b.groups)
+        execute_group(ctx, g, res.answers);
+}
+
+int validate_requests(const tm_ctx *ctx, const tm_request *reqs, int count)
+{
+    if (count < 0 || (count > 0 && reqs == nullptr))
+        return TM_ERR_ARGUMENT;
+    for (int i = 0; i < count; i++)
+    {
+        const tm_request &r = reqs[i];
+        if (r.templ == nullptr || r.m < 1 || static_cast<uint64_t>(r.m) > ctx->n || r.merge_offset < 0)
+            return TM_ERR_ARGUMENT;
+        if (r.mode == TM_MODE_KNN)
+        {
+            if (r.k < 1)
+                return TM_ERR_ARGUMENT;
+        }
+        else if (r.mode != TM_MODE_THRESHOLD)
+            return TM_ERR_ARGUMENT;
+    }
+    return TM_OK;
+}
+
+} // namespace
+
+// ---------------------------------------------------------------------------------
+extern "C" {
+
+int tm_ctx_create(const float *raw, uint64_t n, int device, tm_ctx **out)
+{
+    if (out == nullptr || raw == nullptr || n == 0)
+        return TM_ERR_ARGUMENT;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+        return TM_ERR_NO_DEVICE;
+    cudaDeviceProp prop{};
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major < 10)
+        return TM_ERR_NO_DEVICE;
+    auto ctx = std::make_unique<tm_ctx>();
+    ctx->device = device;
+    ctx->n = n;
+    const int rc = guarded(ctx.get(), [&] {
+        TM_CUDA(cudaSetDevice(device));
+        TM_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+        TM_CUDA(cudaEventCreate(&ctx->ev0));
+        TM_CUDA(cudaEventCreate(&ctx->ev1));
+        const uint64_t total = n + tmb::kStagePad;
+        ctx->raw.reserve(sizeof(float) * total);
+        ctx->clean.reserve(sizeof(float) * total);
+        TM_CUDA(cudaMemsetAsync(ctx->raw.p, 0, sizeof(float) * total, ctx->stream));
+        TM_CUDA(cudaMemcpyAsync(ctx->raw.p, raw, sizeof(float) * n, cudaMemcpyHostToDevice, ctx->stream));
+        TM_CUDA(tmb::launch_clean(ctx->raw.as<float>(), ctx->clean.as<float>(), n, total, ctx->stream));
+        TM_CUDA(cudaStreamSynchronize(ctx->stream));
+    });
+    if (rc != TM_OK)
+    {
+        tm_ctx_destroy(ctx.release());
+        return rc;
+    }
+    *out = ctx.release();
+    return TM_OK;
+}
+
+int tm_ctx_destroy(tm_ctx *ctx)
+{
+    if (ctx == nullptr)
+        return TM_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream)
+        cudaStreamSynchronize(ctx->stream);
+    for (auto &kv : ctx->lengths)
+    {
+        kv.second->mean.release();
+        kv.second->inv.release();
+        kv.second->flags.release();
+    }
+    for (DevBuf *b : {&ctx->raw, &ctx->clean, &ctx->suf, &ctx->tkey, &ctx->bmin_u, &ctx->bmin_l, &ctx->list, &ctx->counters, &ctx->cand, &ctx->dist})
+        b->release();
+    for (HostBuf *b : {&ctx->h_q, &ctx->h_order, &ctx->h_slots, &ctx->h_cand, &ctx->h_dist,
+                       &ctx->h_counters, &ctx->h_tkey})
+        b->release();
+    if (ctx->ev0)
+        cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1)
+        cudaEventDestroy(ctx->ev1);
+    if (ctx->stream)
+        cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return TM_OK;
+}
+
+const char *tm_last_error(const tm_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int tm_set_kernel(tm_ctx *ctx, int kernel)
+{
+    if (ctx == nullptr || kernel < TM_KERNEL_AUTO || kernel > TM_KERNEL_SPLIT_BF16)
+        return TM_ERR_ARGUMENT;
+    ctx->kernel = kernel;
+    return TM_OK;
+}
+
+int tm_set_window_range(tm_ctx *ctx, uint64_t first, uint64_t count)
+{
+    if (ctx == nullptr || count == 0)
+        return TM_ERR_ARGUMENT;
+    return guarded(ctx, [&] {
+        TM_CUDA(cudaSetDevice(ctx->device));
+        TM_CUDA(cudaStreamSynchronize(ctx->stream));
+        for (auto &kv : ctx->lengths)
+        {
+            kv.second->mean.release();
+            kv.second->inv.release();
+            kv.second->flags.release();
+        }
+        ctx->lengths.clear();
+        ctx->range_first = first;
+        ctx->range_count = count;
+    });
+}
+
+int tm_prepare_length(tm_ctx *ctx, int m)
+{
+    if (ctx == nullptr || m < 1 || static_cast<uint64_t>(m) > ctx->n)
+        return TM_ERR_ARGUMENT;
+    return guarded(ctx, [&] {
+        TM_CUDA(cudaSetDevice(ctx->device));
+        ensure_length(ctx, m);
+        TM_CUDA(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+int tm_window_stats(tm_ctx *ctx, int m, uint64_t first, uint64_t count, float *mean, float *stddev)
+{
+    if (ctx == nullptr || m < 1 || static_cast<uint64_t>(m) > ctx->n || mean == nullptr || stddev == nullptr)
+        return TM_ERR_ARGUMENT;
+    const uint64_t total = ctx->n - static_cast<uint64_t>(m) + 1;
+    if (first > total || count > total - first)
+        return TM_ERR_ARGUMENT;
+    if (count == 0)
+        return TM_OK;
+    return guarded(ctx, [&] {
+        TM_CUDA(cudaSetDevice(ctx->device));
+        DevBuf dm, ds;
+        dm.reserve(count * sizeof(float));
+        ds.reserve(count * sizeof(float));
+        TM_CUDA(tmb::launch_reference_stats(ctx->raw.as<float>(), m, first, count, dm.as<float>(), ds.as<float>(),
+                                           ctx->stream));
+        count_launch(ctx);
+        TM_CUDA(cudaMemcpyAsync(mean, dm.p, count * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+        TM_CUDA(cudaMemcpyAsync(stddev, ds.p, count * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+        TM_CUDA(cudaStreamSynchronize(ctx->stream));
+        dm.release();
+        ds.release();
+    });
+}
+
+int tm_batch_create(tm_ctx *ctx, const tm_request *requests, int count, tm_batch **out)
+{
+    if (ctx == nullptr || out == nullptr)
+        return TM_ERR_ARGUMENT;
+    *out = nullptr;
+    const int v = validate_requests(ctx, requests, count);
+    if (v != TM_OK)
+    {
+        ctx->err = "invalid request";
+        return v;
+    }
+    auto b = std::make_unique<tm_batch>();
+    const int rc = guarded(ctx, [&] {
+        TM_CUDA(cudaSetDevice(ctx->device));
+        create_batch(ctx, requests, count, *b);
+    });
+    if (rc == TM_OK)
+        *out = b.release();
+    return rc;
+}
+
+int tm_batch_run(tm_ctx *ctx, tm_batch *batch, tm_result **out)
+{
+    if (ctx == nullptr || batch == nullptr || out == nullptr)
+        return TM_ERR_ARGUMENT;
+    *out = nullptr;
+    auto res = std::make_unique<tm_result>();
+    const int rc = guarded(ctx, [&] {
+        TM_CUDA(cudaSetDevice(ctx->device));
+        run_batch(ctx, *batch, *res);
+    });
+    if (rc == TM_OK)
+        *out = res.release();
+    return rc;
+}
+
+int tm_batch_destroy(tm_batch *batch)
+{
+    delete batch;
+    return TM_OK;
+}
+
+int tm_batch_h2d_bytes(const tm_batch *batch, uint64_t *bytes)
+{
+    if (batch == nullptr || bytes == nullptr)
+        return TM_ERR_ARGUMENT;
+    *bytes = batch->h2d_bytes;
+    return TM_OK;
+}
+
+int tm_scan_batch(tm_ctx *ctx, const tm_request *requests, int count, tm_result **out)
+{
+    tm_batch *b = nullptr;
+    int rc = tm_batch_create(ctx, requests, count, &b);
+    if (rc != TM_OK)
+        return rc;
+    rc = tm_batch_run(ctx, b, out);
+    tm_batch_destroy(b);
+    return rc;
+}
+
+int tm_search_knn(tm_ctx *ctx, const float *queries, int count, int m, int k, int merge_offset, uint64_t *I, float *D)
+{
+    if (ctx == nullptr || queries == nullptr || I == nullptr || D == nullptr || count < 0 || k < 1)
+        return TM_ERR_ARGUMENT;
+    std::vector<tm_request> reqs(static_cast<size_t>(count));
+    for (int i = 0; i < count; i++)
+        reqs[i] = tm_request{queries + static_cast<size_t>(i) * m, m, TM_MODE_KNN, k, merge_offset, 0.0f, 0u};
+    tm_result *res = nullptr;
+    const int rc = tm_scan_batch(ctx, reqs.data(), count, &res);
+    if (rc != TM_OK)
+        return rc;
+    for (int i = 0; i < count; i++)
+        for (int j = 0; j < k; j++)
+        {
+            I[static_cast<size_t>(i) * k + j] = res->answers[i][j].pos;
+            D[static_cast<size_t>(i) * k + j] = res->answers[i][j].dist;
+        }
+    tm_result_free(res);
+    return TM_OK;
+}
+
+int tm_search_threshold(tm_ctx *ctx, const float *queries, int count, int m, float correlation, int merge_offset,
+                        tm_result **out)
+{
+    if (ctx == nullptr || queries == nullptr || out == nullptr || count < 0)
+        return TM_ERR_ARGUMENT;
+    std::vector<tm_request> reqs(static_cast<size_t>(count));
+    for (int i = 0; i < count; i++)
+        reqs[i] = tm_request{queries + static_cast<size_t>(i) * m, m, TM_MODE_THRESHOLD, 1, merge_offset, correlation,
+                             0u};
+    return tm_scan_batch(ctx, reqs.data(), count, out);
+}
+
+int tm_result_count(const tm_result *res, int request, uint64_t *count)
+{
+    if (res == nullptr || count == nullptr || request < 0 || request >= static_cast<int>(res->answers.size()))
+        return TM_ERR_ARGUMENT;
+    *count = res->answers[request].size();
+    return TM_OK;
+}
+
+int tm_result_get(const tm_result *res, int request, uint64_t *positions, float *distances, uint64_t capacity)
+{
+    if (res == nullptr || request < 0 || request >= static_cast<int>(res->answers.size()))
+        return TM_ERR_ARGUMENT;
+    const std::vector<Hit> &a = res->answers[request];
+    if (capacity < a.size())
+        return TM_ERR_CAPACITY;
+    for (size_t i = 0; i < a.size(); i++)
+    {
+        if (positions)
+            positions[i] = a[i].pos;
+        if (distances)
+            distances[i] = a[i].dist;
+    }
+    return TM_OK;
+}
+
+void tm_result_free(tm_result *res) { delete res; }
+
+float tm_cc_to_ed(float correlation, int m) { return tm_host::cc_to_ed(correlation, m); }
+float tm_ed_to_cc(float distance, int m) { return tm_host::ed_to_cc(distance, m); }
+
+int tm_profile_enable(tm_ctx *ctx, int enable)
+{
+    if (ctx == nullptr)
+        return TM_ERR_ARGUMENT;
+    ctx->profile = enable != 0;
+    return TM_OK;
+}
+
+int tm_profile_read(tm_ctx *ctx, char *name, size_t name_capacity, int64_t *launches, double *milliseconds,
+                    double *flops, int64_t *all_launches)
+{
+    if (ctx == nullptr)
+        return TM_ERR_ARGUMENT;
+    if (name && name_capacity > 0)
+    {
+        std::snprintf(name, name_capacity, "%s", ctx->kname.c_str());
+    }
+    if (launches)
+        *launches = ctx->prof_launches;
+    if (milliseconds)
+        *milliseconds = ctx->prof_ms;
+    if (flops)
+        *flops = ctx->prof_flops;
+    if (all_launches)
+        *all_launches = ctx->all_launches;
+    ctx->prof_launches = 0;
+    ctx->prof_ms = 0.0;
+    ctx->prof_flops = 0.0;
+    ctx->all_launches = 0;
+    return TM_OK;
+}
+
+int tm_d2h_bytes(tm_ctx *ctx, uint64_t *bytes)
+{
+    if (ctx == nullptr || bytes == nullptr)
+        return TM_ERR_ARGUMENT;
+    *bytes = ctx->d2h_bytes;
+    ctx->d2h_bytes = 0;
+    return TM_OK;
+}
+
+int tm_ctx_stream(tm_ctx *ctx, void **stream)
+{
+    if (ctx == nullptr || stream == nullptr)
+        return TM_ERR_ARGUMENT;
+    *stream = static_cast<void *>(ctx->stream);
+    return TM_OK;
+}
+
+int tm_last_candidates(const tm_ctx *ctx, uint64_t *count)
+{
+    if (ctx == nullptr || count == nullptr)
+        return TM_ERR_ARGUMENT;
+    *count = ctx->last_candidates;
+    return TM_OK;
+}
+
+} // extern "C"
