@@ -1,0 +1,393 @@
+"""Benchmark of the exact template-matching scan on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload precision|plain_knn|threshold] [--kernel auto|fp32|bf16]
+
+Workload (default "precision"): a seeded synthetic waveform of 2^28 float32 samples
+(AR(2) noise x slow envelope, 2000 injected chirp events), 1024 chirp templates of
+4096 samples, kNN k=100 with merge offset 0. One step = one batch of 128 templates
+against every window of the waveform (2^28 - 4095 windows); the metric is
+template-subsequence pairs per second (G pairs/s), whole job over all GPUs.
+
+`value`: templates already resident in HBM (a prepared batch), each step the full
+device pipeline plus the exact answers copied back. `e2e`: the same steps through
+the public call with host templates (host z-normalisation, host->device copy,
+device pipeline, device->host answers). The waveform (1 GiB) is larger than L2, so
+no flush is needed between steps. With N GPUs every rank runs its own replica (the
+path needs no exchange); time is the max over ranks.
+
+--impl reference: the reference's own CPU scan (SkipSequentialScan, sequential mode,
+built from the reference sources into oracle/_ref) on a bounded sample of the same
+workload (the first 2^24 samples, a few templates per step), all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = 'G template-subseq pairs/s vs plain FP32 kernel, exact answers; p50/p99 latency'
+UNIT = 'G pairs/s'
+
+WORKLOADS = {
+    # precision = config 3, plain_knn = config 1, threshold = config 2
+    'precision': dict(n=1 << 28, q=1024, m=4096, events=2000, mode='knn', k=100, merge=0, corr=0.0,
+                      per_step=128, seed=2028),
+    'plain_knn': dict(n=1 << 22, q=16, m=1024, events=50, mode='knn', k=10, merge=512, corr=0.0,
+                      per_step=16, seed=2026),
+    # the precision workload's kernel on 2^25 samples (> L2) and 64 templates: ncu captures
+    'precision_small': dict(n=1 << 25, q=64, m=4096, events=250, mode='knn', k=100, merge=0, corr=0.0,
+                            per_step=64, seed=2028),
+    'threshold': dict(n=1 << 26, q=256, m=2048, events=500, mode='threshold', k=1, merge=0, corr=0.8,
+                      per_step=64, seed=2027),
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def make_workload(w):
+    from tremor_b200 import synth
+    t0 = time.time()
+    x, q, _ = synth.workload(w['n'], w['q'], w['m'], w['events'], seed=w['seed'])
+    log(f'[bench] workload generated in {time.time() - t0:.1f} s')
+    return x, q
+
+
+def requests_for(w, q):
+    import tremor_b200 as tb
+    if w['mode'] == 'knn':
+        return [tb.Request(t, tb.MODE_KNN, k=w['k'], merge_offset=w['merge']) for t in q]
+    return [tb.Request(t, tb.MODE_THRESHOLD, correlation=w['corr'], merge_offset=w['merge']) for t in q]
+
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) during the timed region."""
+
+    FIELDS = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+              'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+              'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, device):
+        self.device, self.proc, self.lines = device, None, []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.device), f'--query-gpu={self.FIELDS}',
+                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['nvidia-smi unavailable']}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, power, reasons = [], None, [], set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(',')]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith('active'):
+                    reasons.add(name)
+        loaded = [s for s, p in zip(sm, power) if p > 300] or sm
+        return {'sm_mhz': statistics.median(loaded) if loaded else None, 'sm_max_mhz': smax,
+                'reasons': sorted(reasons), 'samples': len(sm), 'power_w_max': max(power) if power else None}
+
+
+def peaks():
+    path = ROOT / 'MEASURED_PEAKS.json'
+    if path.exists():
+        d = json.loads(path.read_text())
+        return d.get('bf16_tflops', 1590.0), d.get('hbm_gbs', 6650.0), 'measured'
+    return 1590.0, 6650.0, 'fallback'
+
+
+def traffic_for(kernel, workload):
+    """Per-launch DRAM bytes of the kernel from the committed ncu summary, or None."""
+    path = ROOT / 'profiles' / 'traffic.txt'
+    if not path.exists():
+        return None
+    for line in path.read_text().splitlines():
+        parts = line.split()
+        if len(parts) >= 3 and parts[0] == kernel and parts[1] == workload:
+            return float(parts[2])
+    return None
+
+
+class RefScan:
+    """The reference's own SkipSequentialScan (sequential mode, no lower bounds) built once on
+    the first 2^24 samples of the waveform (its build is the reference's index step, not
+    timed); search() times SkipSequentialScan::search_knn / search_threshold alone."""
+
+    def __init__(self, w, x, threads=None):
+        import ctypes
+        from tests import oracle_bindings as ob
+        self.w, self.ct, self.h = w, ctypes, None
+        self.ref = ob.reference()
+        if self.ref is None:
+            self.error = 'oracle/_ref not built'
+            return
+        ref = self.ref
+        ref.tmref_sss_create.restype = ctypes.c_void_p
+        ref.tmref_sss_create.argtypes = [ctypes.c_char_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        ref.tmref_sss_search.restype = ctypes.c_double
+        ref.tmref_sss_search.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_float, ctypes.c_char_p]
+        ref.tmref_sss_destroy.argtypes = [ctypes.c_void_p]
+        self.threads = threads or os.cpu_count() or 1
+        n_s = min(len(x), 1 << 24)
+        self.windows = n_s - w['m'] + 1
+        self.tmp = tempfile.TemporaryDirectory()
+        wf = os.path.join(self.tmp.name, 'w.bin')
+        x[:n_s].tofile(wf)
+        t0 = time.time()
+        self.h = ref.tmref_sss_create(wf.encode(), n_s, w['m'], w['k'], w['merge'], 0, self.threads,
+                                      16 if w['m'] % 16 == 0 else 8)
+        log(f'[bench] reference scan built in {time.time() - t0:.1f} s ({self.threads} threads)')
+        self.error = None if self.h else 'reference build failed'
+
+    def search(self, template) -> float:
+        qi = np.ascontiguousarray(np.asarray(template, np.float32)[None, :])
+        out = os.path.join(self.tmp.name, 'out.csv')
+        s = self.ref.tmref_sss_search(self.h, qi.ctypes.data_as(self.ct.c_void_p), 1,
+                                      1 if self.w['mode'] == 'knn' else 0, self.w['k'], self.w['corr'], out.encode())
+        if s < 0:
+            raise RuntimeError('reference search failed')
+        return s
+
+    def close(self):
+        if self.h:
+            self.ref.tmref_sss_destroy(self.h)
+            self.h = None
+
+
+def cpu_reference(w, x, q, budget_s=15.0, max_templates=32):
+    """(pairs/s, info) of the reference's CPU scan over a bounded sample: as many templates as
+    fit in about `budget_s` seconds of search, at least one."""
+    scan = RefScan(w, x)
+    if scan.error:
+        return None, {'error': scan.error}
+    try:
+        done, secs = 0, 0.0
+        while done < min(max_templates, len(q)) and (secs < budget_s or done == 0):
+            secs += scan.search(q[done])
+            done += 1
+    finally:
+        scan.close()
+    return done * scan.windows / secs / 1e9, {
+        'cores': scan.threads, 'kind': 'reference',
+        'sample': f'{done} templates x {scan.windows} windows (first 2^24 samples of the waveform), '
+                  f'SkipSequentialScan sequential mode, {secs:.1f} s of search'}
+
+
+def dist_setup(gpus):
+    if gpus <= 1 or 'RANK' not in os.environ:
+        return 0, 1, int(os.environ.get('LOCAL_RANK', 0)), None
+    import datetime
+    import torch.distributed as dist
+    dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=600))
+    return dist.get_rank(), dist.get_world_size(), int(os.environ.get('LOCAL_RANK', 0)), dist
+
+
+def run_reference(args, w):
+    rank, world, local, dist = dist_setup(args.gpus)
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    x, q = make_workload(w)  # the sample is the first 2^24 samples of the full waveform
+    scan = RefScan(w, x)
+    if scan.error:
+        print(json.dumps({'impl': 'reference', 'unavailable': scan.error}), flush=True)
+        return
+    per_step = max(1, int(os.environ.get('TM_REF_TEMPLATES_PER_STEP', 2)))
+    for s in range(args.warmup):
+        scan.search(q[s % len(q)])
+    secs = 0.0
+    for s in range(args.steps):
+        for t in range(per_step):
+            secs += scan.search(q[(s * per_step + t) % len(q)])
+    scan.close()
+    value = args.steps * per_step * scan.windows / secs / 1e9
+    info = {'cores': scan.threads, 'kind': 'reference',
+            'sample': f'{per_step} templates x {scan.windows} windows per step (first 2^24 samples), '
+                      'SkipSequentialScan sequential mode'}
+    line = {'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': args.gpus, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': 1000.0 * secs / args.steps, 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic', 'impl': 'reference',
+            'config': {'workload': args.workload, **{k: w[k] for k in ('n', 'q', 'm', 'k', 'merge', 'corr')},
+                       'sample': 'first 2^24 samples'},
+            'cpu_baseline': {'value': value, 'unit': UNIT, **info},
+            'e2e': {'value': value, 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def run_ours(args, w):
+    import torch
+    import tremor_b200 as tb
+    rank, world, local, dist = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    x, q = make_workload(w)
+    kernel = {'auto': tb.KERNEL_AUTO, 'fp32': tb.KERNEL_FP32, 'bf16': tb.KERNEL_SPLIT_BF16}[args.kernel]
+    ctx = tb.Context(x, device=local)
+    ctx.set_kernel(kernel)
+    t0 = time.time()
+    ctx.prepare_length(w['m'])
+    log(f'[bench] window statistics in {time.time() - t0:.2f} s')
+    reqs = requests_for(w, q)
+    per = w['per_step']
+    nbatch = (len(reqs) + per - 1) // per
+    batches = [ctx.batch(reqs[i * per:(i + 1) * per]) for i in range(nbatch)]
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=local)
+    windows = w['n'] - w['m'] + 1
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+
+    for s in range(args.warmup):
+        batches[s % nbatch].run()
+    ctx.profile_enable(True)
+    ctx.profile_read()
+    ctx.d2h_bytes()
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    pairs = 0
+    for s in range(args.steps):
+        b = batches[(args.warmup + s) % nbatch]
+        b.run()
+        pairs += b.count * windows
+    ev1.record(stream)
+    barrier()
+    clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1)
+    kname, launches, kms, kflops, all_launches = ctx.profile_read()
+    ctx.profile_enable(False)
+    d2h_value = ctx.d2h_bytes()
+
+    # e2e: host templates through the public call, copies inside the timed region
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    h2d = 0
+    e0.record(stream)
+    for s in range(args.steps):
+        chunk = reqs[((args.warmup + s) % nbatch) * per:((args.warmup + s) % nbatch + 1) * per]
+        b = ctx.batch(chunk)
+        h2d += b.h2d_bytes()
+        b.run()
+        b.close()
+    e1.record(stream)
+    barrier()
+    e_ms = e0.elapsed_time(e1)
+    d2h = ctx.d2h_bytes()
+
+    t = torch.tensor([ms, e_ms, kms / max(launches, 1)], dtype=torch.float64, device=f'cuda:{local}')
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms, e_ms, k_avg_ms = t.tolist()
+    total_pairs = pairs * world
+    value = total_pairs / (ms / 1e3) / 1e9
+    e2e_value = total_pairs / (e_ms / 1e3) / 1e9
+
+    if rank == 0:
+        bf16_peak, _, peak_kind = peaks()
+        flops_per_launch = kflops / max(launches, 1)
+        achieved = flops_per_launch / (k_avg_ms / 1e3) / 1e12
+        if kname == 'k_scan_umma':
+            roof = {'bound': 'tensor', 'achieved': achieved, 'peak': bf16_peak / 3.0, 'unit': 'TFLOP/s',
+                    'peak_note': f'{peak_kind} bf16 dense / 3 (three BF16 products per FP32 multiply-add)'}
+        else:
+            nominal = 148 * 128 * 2 * 1.965e9 / 1e12
+            roof = {'bound': 'fp32', 'achieved': achieved, 'peak': nominal, 'unit': 'TFLOP/s',
+                    'peak_note': 'nominal FP32 FMA peak (148 SMs x 128 lanes x 2 x 1.965 GHz); no measured FP32 figure'}
+        roof['frac'] = achieved / roof['peak']
+        tb_bytes = traffic_for(kname, args.workload)
+        roof['traffic'] = tb_bytes
+        roof['kernel'] = kname
+        roof['algorithmic_flops_per_launch'] = flops_per_launch
+        roof['kernel_ms_per_launch'] = k_avg_ms
+        cpu_v, cpu_info = (None, {'error': 'skipped'}) if args.no_cpu else cpu_reference(w, x, q)
+        line = {'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
+                'warmup': args.warmup, 'ms_per_step': ms / args.steps, 'higher_is_better': True, 'scaling': 'weak',
+                'vs_baseline': None, 'dtype': 'bf16x3+f32' if kname == 'k_scan_umma' else 'f32',
+                'data': 'synthetic',
+                'config': {'workload': args.workload, 'n': w['n'], 'templates': w['q'], 'templates_per_step': per,
+                           'm': w['m'], 'mode': w['mode'], 'k': w['k'], 'merge': w['merge'], 'corr': w['corr'],
+                           'events': w['events'], 'seed': w['seed'], 'kernel': args.kernel,
+                           'l2': 'inputs larger than L2 (waveform 4n bytes)', 'parallelism': f'replicas x{world}'},
+                'roofline': roof,
+                'cpu_baseline': {'value': cpu_v, 'unit': UNIT, **cpu_info},
+                'e2e': {'value': e2e_value, 'unit': UNIT, 'h2d_bytes_per_step': h2d // args.steps,
+                        'd2h_bytes_per_step': d2h // args.steps},
+                'gpu_launches': all_launches, 'clocks': clocks,
+                'd2h_bytes_per_step_value': d2h_value // args.steps,
+                'candidates_last_step': ctx.last_candidates()}
+        print(json.dumps(line), flush=True)
+    for b in batches:
+        b.close()
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    p = argparse.ArgumentParser()
+    p.add_argument('--gpus', type=int, default=1)
+    p.add_argument('--steps', type=int, default=5)
+    p.add_argument('--warmup', type=int, default=3)
+    p.add_argument('--impl', choices=['ours', 'reference'], default='ours')
+    p.add_argument('--workload', choices=sorted(WORKLOADS), default='precision')
+    p.add_argument('--kernel', choices=['auto', 'fp32', 'bf16'], default='auto')
+    p.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline leg')
+    args = p.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    w = WORKLOADS[args.workload]
+    if args.impl == 'reference':
+        run_reference(args, w)
+    else:
+        run_ours(args, w)
+
+
+if __name__ == '__main__':
+    main()
