@@ -154,3 +154,22 @@ def test_config1_shape_self_match_and_oracle(kernel):
         assert int(I[i, 0]) == int(planted[i])
         assert D[i, 0] < 1e-2
     _assert_knn_equal(x, q[:2], 1024, 10, 512, I[:2], D[:2])
+
+
+def test_prepared_batch_reruns_and_kernel_switch():
+    """A prepared batch (templates resident) gives the same answers on every run, under
+    either contraction kernel."""
+    x = _waveform(1 << 16, 31)
+    m = 256
+    q = _templates(x, m, np.random.default_rng(32), 4)
+    reqs = [tb.Request(q[0], tb.MODE_KNN, k=8, merge_offset=128), tb.Request(q[1], tb.MODE_THRESHOLD, correlation=0.5),
+            tb.Request(q[2], tb.MODE_KNN, k=3), tb.Request(q[3], tb.MODE_THRESHOLD, correlation=0.7, merge_offset=30)]
+    with tb.Context(x) as ctx:
+        b = ctx.batch(reqs)
+        first = b.run()
+        for kernel in [tb.KERNEL_FP32, tb.KERNEL_AUTO, tb.KERNEL_FP32]:
+            ctx.set_kernel(kernel)
+            again = b.run()
+            for (p0, d0), (p1, d1) in zip(first, again):
+                assert np.array_equal(p0, p1) and np.array_equal(d0.view(np.uint32), d1.view(np.uint32))
+        b.close()

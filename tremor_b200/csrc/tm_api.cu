@@ -32,7 +32,8 @@ cudaError_t launch_window_stats(const float *clean, const float *raw, uint64_t n
 cudaError_t launch_reference_stats(const float *raw, int m, uint64_t w0, uint64_t count, float *mean, float *stddev,
                                    cudaStream_t s);
 cudaError_t launch_scan_fp32(const ScanArgs &a, cudaStream_t s);
-cudaError_t launch_scan_umma(const ScanArgs &a, cudaStream_t s, bool *supported);
+cudaError_t launch_scan_umma(const ScanArgs &a, cudaStream_t s);
+bool umma_supported(int m, int T, uint64_t W);
 cudaError_t launch_bucket_select(const uint32_t *bmin_u, uint32_t nb, const TemplParam *tp, const int *knn_slots,
                                  int nk, uint32_t *tkey, cudaStream_t s);
 cudaError_t launch_list_buckets(const uint32_t *bmin_l, uint32_t nb, const int *knn_slots, int nk,
@@ -269,7 +270,8 @@ double gamma_bf16(int m) { return 1.2e-5 + (3.0 * ((m + 63) & ~63) / 16.0 + 16.0
 struct GroupPlan
 {
     int m = 0, T = 0, T_pad = 0, m_pad = 0, nblk = 0, nk = 0;
-    bool umma_constants = false;
+    bool umma_constants = false; // a1_main of the device constants is the tensor-core one
+    std::vector<float> a1_umma;  // a1 of the tensor-core kernel per slot
     std::vector<int> index; // request index of each slot
     std::vector<int> mode, k, merge;
     std::vector<float> thr; // threshold distance per slot
@@ -310,7 +312,7 @@ void prepare_group(tm_ctx *ctx, int m, const std::vector<int> &idx, const tm_req
     g.T_pad = (g.T + 63) & ~63;
     g.m_pad = (m + 63) & ~63;
     g.nblk = std::max(1, m / tm_host::kZnormBlock);
-    g.umma_constants = ctx->kernel != TM_KERNEL_FP32;
+    g.umma_constants = false;
     g.index = idx;
     const int T = g.T, T_pad = g.T_pad, m_pad = g.m_pad, nblk = g.nblk;
     ctx->h_q.reserve(sizeof(float) * static_cast<size_t>(T_pad) * m_pad);
@@ -326,6 +328,7 @@ void prepare_group(tm_ctx *ctx, int m, const std::vector<int> &idx, const tm_req
     g.k.assign(T, 0);
     g.merge.assign(T, 0);
     g.thr.assign(T, 0.0f);
+    g.a1_umma.assign(T, 0.0f);
     g.nk = 0;
     for (int t = 0; t < T; t++)
     {
@@ -342,7 +345,9 @@ void prepare_group(tm_ctx *ctx, int m, const std::vector<int> &idx, const tm_req
             s1 += q[i];
         }
         TemplParam &p = g.htp[t];
-        fill_param(p, m, q2, s1, g.umma_constants ? gamma_bf16(m) : gamma_fp32(m), gamma_fp32(m));
+        fill_param(p, m, q2, s1, gamma_bf16(m), gamma_fp32(m));
+        g.a1_umma[t] = p.a1_main;
+        p.a1_main = p.a1_fp32;
         p.mode = g.mode[t] = r->mode;
         p.k = g.k[t] = r->k;
         p.merge = g.merge[t] = r->merge_offset;
@@ -393,15 +398,15 @@ void execute_group(tm_ctx *ctx, GroupPlan &g, std::vector<std::vector<Hit>> &ans
     if (W >= (1ull << 32))
         throw Failure{TM_ERR_ARGUMENT, "more than 2^32 - 1 windows in one range; split the range"};
     cudaStream_t s = ctx->stream;
-    bool use_umma = ctx->kernel != TM_KERNEL_FP32;
-    if (use_umma != g.umma_constants) // kernel changed since preparation: refresh the bound constants
+    const bool use_umma = ctx->kernel != TM_KERNEL_FP32 && tmb::umma_supported(m, T, W);
+    if (ctx->kernel == TM_KERNEL_SPLIT_BF16 && !use_umma)
+        throw Failure{TM_ERR_STATE, "split-BF16 kernel not available for this request group"};
+    if (use_umma != g.umma_constants) // error-bound constants of the kernel that will run
     {
         for (int t = 0; t < T; t++)
-            g.htp[t].a1_main = use_umma ? g.htp[t].a1_main : g.htp[t].a1_fp32;
-        if (use_umma)
-            throw Failure{TM_ERR_STATE, "batch prepared for the FP32 kernel; prepare it again"};
+            g.htp[t].a1_main = use_umma ? g.a1_umma[t] : g.htp[t].a1_fp32;
         TM_CUDA(cudaMemcpyAsync(g.tp.p, g.htp.data(), sizeof(TemplParam) * T_pad, cudaMemcpyHostToDevice, s));
-        g.umma_constants = false;
+        g.umma_constants = use_umma;
     }
     ctx->tkey.reserve(sizeof(uint32_t) * T);
 
@@ -448,26 +453,10 @@ void execute_group(tm_ctx *ctx, GroupPlan &g, std::vector<std::vector<Hit>> &ans
         // 2. contraction with fused epilogue
         if (ctx->profile)
             TM_CUDA(cudaEventRecord(ctx->ev0, s));
-        bool ran_umma = false;
         if (use_umma)
-        {
-            bool supported = false;
-            TM_CUDA(tmb::launch_scan_umma(a, s, &supported));
-            ran_umma = supported;
-            if (!supported && ctx->kernel == TM_KERNEL_SPLIT_BF16)
-                throw Failure{TM_ERR_STATE, "split-BF16 kernel does not support this length"};
-        }
-        if (!ran_umma)
-        {
-            if (g.umma_constants) // constants were computed for the tensor-core kernel: use FP32's
-            {
-                for (int t = 0; t < T; t++)
-                    g.htp[t].a1_main = g.htp[t].a1_fp32;
-                TM_CUDA(cudaMemcpyAsync(g.tp.p, g.htp.data(), sizeof(TemplParam) * T_pad, cudaMemcpyHostToDevice, s));
-                g.umma_constants = false;
-            }
+            TM_CUDA(tmb::launch_scan_umma(a, s));
+        else
             TM_CUDA(tmb::launch_scan_fp32(a, s));
-        }
         count_launch(ctx);
         if (ctx->profile)
         {
@@ -475,7 +464,7 @@ void execute_group(tm_ctx *ctx, GroupPlan &g, std::vector<std::vector<Hit>> &ans
             TM_CUDA(cudaEventSynchronize(ctx->ev1));
             float ms = 0.0f;
             TM_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-            ctx->kname = ran_umma ? "k_scan_umma" : "k_scan_fp32";
+            ctx->kname = use_umma ? "k_scan_umma" : "k_scan_fp32";
             ctx->prof_launches++;
             ctx->prof_ms += ms;
             ctx->prof_flops += 2.0 * m * static_cast<double>(W) * T;

@@ -4,10 +4,8 @@
 
 namespace tmb {
 
-cudaError_t launch_scan_umma(const ScanArgs &, cudaStream_t, bool *supported)
-{
-    *supported = false;
-    return cudaSuccess;
-}
+bool umma_supported(int, int, uint64_t) { return false; }
+
+cudaError_t launch_scan_umma(const ScanArgs &, cudaStream_t) { return cudaErrorNotSupported; }
 
 } // namespace tmb
