@@ -49,6 +49,7 @@ extern "C" {
 #define TM_ERR_STATE (-4)     /* call not valid in the context's state */
 #define TM_ERR_CAPACITY (-5)  /* caller buffer too small; the needed size was written */
 #define TM_ERR_NO_DEVICE (-6) /* no usable sm_100 device */
+#define TM_ERR_TIMEOUT (-7)   /* a kernel gave up waiting (bounded wait); the context stays usable */
 
 /* TREMOR_MISSING_VALUE (ZnormSearch.hpp:21): a missing sample counts as 0; a window
  * whose first sample is missing is not searched. */
@@ -148,6 +149,12 @@ int tm_profile_enable(tm_ctx *ctx, int enable);
  * kernel launches of this library since the last reset. Resets the counters. */
 int tm_profile_read(tm_ctx *ctx, char *name, size_t name_capacity, int64_t *launches, double *milliseconds,
                     double *flops, int64_t *all_launches);
+/* Diagnostic: for `count` raw templates of length m, the contraction kernel's distance d
+ * and error bound e of every (template, window) pair, and (if `exact` is not null) the
+ * reference's exact FP32 distance of every pair; count x windows floats each, for the
+ * context's window range. The bound holds when |d - exact| <= e (windows that are not
+ * searched stay NaN in d and e). Small cases only: windows x count <= 2^31. */
+int tm_bound_diagnostics(tm_ctx *ctx, const float *queries, int count, int m, float *d, float *e, float *exact);
 /* Device-to-host bytes the searches of this context copied since the last call (resets). */
 int tm_d2h_bytes(tm_ctx *ctx, uint64_t *bytes);
 /* The context's CUDA stream (a cudaStream_t), for callers that order or time work on it. */

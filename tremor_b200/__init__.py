@@ -31,7 +31,7 @@ MISSING_VALUE = np.float32(-100000.0)
 FLT_MAX = float(np.finfo(np.float32).max)
 
 _ERRORS = {-1: 'invalid argument', -2: 'CUDA error', -3: 'out of memory', -4: 'invalid state',
-           -5: 'buffer too small', -6: 'no usable sm_100 device'}
+           -5: 'buffer too small', -6: 'no usable sm_100 device', -7: 'kernel wait timed out'}
 
 LIB_PATH = Path(__file__).resolve().parent / 'libtremor_b200.so'
 _lib = None
@@ -85,6 +85,7 @@ def load_library():
         'tm_batch_h2d_bytes': (i, [_vp, ctypes.POINTER(u64)]),
         'tm_d2h_bytes': (i, [_vp, ctypes.POINTER(u64)]),
         'tm_ctx_stream': (i, [_vp, pp]),
+        'tm_bound_diagnostics': (i, [_vp, _vp, i, i, _vp, _vp, _vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -230,6 +231,19 @@ class Context:
         self._check(self._lib.tm_profile_read(self._h, name, 64, ctypes.byref(launches), ctypes.byref(ms),
                                               ctypes.byref(flops), ctypes.byref(allk)))
         return name.value.decode(), launches.value, ms.value, flops.value, allk.value
+
+    def bound_diagnostics(self, queries: np.ndarray, exact: bool = True):
+        """(d, e, exact) arrays [templates, windows]: the contraction kernel's distance, its
+        error bound, and the reference's exact distance of every pair (tm_bound_diagnostics)."""
+        q = np.ascontiguousarray(np.atleast_2d(queries), dtype=np.float32)
+        m = q.shape[1]
+        W = self.n - m + 1
+        d = np.zeros((q.shape[0], W), np.float32)
+        e = np.zeros((q.shape[0], W), np.float32)
+        x = np.zeros((q.shape[0], W), np.float32) if exact else None
+        self._check(self._lib.tm_bound_diagnostics(self._h, _ptr(q), q.shape[0], m, _ptr(d), _ptr(e),
+                                                   _ptr(x) if exact else None))
+        return d, e, x
 
     def last_candidates(self) -> int:
         n = ctypes.c_uint64(0)

@@ -128,6 +128,22 @@ struct LengthStats
     size_t bytes() const { return mean.bytes + inv.bytes + flags.bytes; }
 };
 
+// BF16 bits of a float, round to nearest even (finite inputs).
+inline uint16_t bf16_bits(float f)
+{
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    return static_cast<uint16_t>(u >> 16);
+}
+inline float bf16_value(uint16_t h)
+{
+    const uint32_t u = static_cast<uint32_t>(h) << 16;
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+
 constexpr double kU = 5.9604644775390625e-08;   // 2^-24
 constexpr double kE64 = 1.1102230246251565e-16; // 2^-53
 
@@ -150,7 +166,7 @@ struct tm_ctx
     uint64_t use_clock = 0;
     // scratch
     DevBuf suf, tkey, bmin_u, bmin_l, list, counters, cand, dist;
-    HostBuf h_q, h_order, h_slots, h_cand, h_dist, h_counters, h_tkey;
+    HostBuf h_split, h_q, h_order, h_slots, h_cand, h_dist, h_counters, h_tkey;
     uint32_t cand_cap = 1u << 22, list_cap = 1u << 20;
     std::string err;
     // instrumentation
@@ -276,9 +292,12 @@ struct GroupPlan
     std::vector<int> mode, k, merge;
     std::vector<float> thr; // threshold distance per slot
     std::vector<TemplParam> htp;
-    DevBuf q, order, tp, slots;
+    DevBuf q, order, tp, slots, q_hi, q_lo;
+    int t_rows = 0;
     void release()
     {
+        q_hi.release();
+        q_lo.release();
         q.release();
         order.release();
         tp.release();
@@ -374,6 +393,28 @@ void prepare_group(tm_ctx *ctx, int m, const std::vector<int> &idx, const tm_req
     TM_CUDA(cudaMemcpyAsync(g.tp.p, g.htp.data(), sizeof(TemplParam) * T_pad, cudaMemcpyHostToDevice, s));
     if (g.nk > 0)
         TM_CUDA(cudaMemcpyAsync(g.slots.p, hslots, sizeof(int) * g.nk, cudaMemcpyHostToDevice, s));
+    if (ctx->kernel != TM_KERNEL_FP32)
+    {
+        // BF16 halves for the tensor-core kernel: q = hi + lo (round to nearest even)
+        g.t_rows = (T + 127) & ~127;
+        const size_t elems = static_cast<size_t>(g.t_rows) * m_pad;
+        ctx->h_split.reserve(2 * sizeof(uint16_t) * elems);
+        uint16_t *hh = ctx->h_split.as<uint16_t>(), *hl = hh + elems;
+        std::memset(hh, 0, 2 * sizeof(uint16_t) * elems);
+        for (int t = 0; t < T; t++)
+            for (int i = 0; i < m; i++)
+            {
+                const size_t at = static_cast<size_t>(t) * m_pad + i;
+                const float v = hq[at];
+                hh[at] = bf16_bits(v);
+                hl[at] = bf16_bits(v - bf16_value(hh[at]));
+            }
+        g.q_hi.reserve(sizeof(uint16_t) * elems);
+        g.q_lo.reserve(sizeof(uint16_t) * elems);
+        TM_CUDA(cudaMemcpyAsync(g.q_hi.p, hh, sizeof(uint16_t) * elems, cudaMemcpyHostToDevice, s));
+        TM_CUDA(cudaMemcpyAsync(g.q_lo.p, hl, sizeof(uint16_t) * elems, cudaMemcpyHostToDevice, s));
+        h2d += 2 * sizeof(uint16_t) * static_cast<uint64_t>(T) * m;
+    }
     // the staging buffers are reused by the next group: finish the copies first
     TM_CUDA(cudaStreamSynchronize(s));
     h2d += sizeof(float) * static_cast<uint64_t>(T) * m + sizeof(int) * static_cast<uint64_t>(T) * nblk +
@@ -398,7 +439,7 @@ void execute_group(tm_ctx *ctx, GroupPlan &g, std::vector<std::vector<Hit>> &ans
     if (W >= (1ull << 32))
         throw Failure{TM_ERR_ARGUMENT, "more than 2^32 - 1 windows in one range; split the range"};
     cudaStream_t s = ctx->stream;
-    const bool use_umma = ctx->kernel != TM_KERNEL_FP32 && tmb::umma_supported(m, T, W);
+    const bool use_umma = ctx->kernel != TM_KERNEL_FP32 && g.t_rows > 0 && tmb::umma_supported(m, T, W);
     if (ctx->kernel == TM_KERNEL_SPLIT_BF16 && !use_umma)
         throw Failure{TM_ERR_STATE, "split-BF16 kernel not available for this request group"};
     if (use_umma != g.umma_constants) // error-bound constants of the kernel that will run
@@ -449,6 +490,10 @@ void execute_group(tm_ctx *ctx, GroupPlan &g, std::vector<std::vector<Hit>> &ans
         a.cand = ctx->cand.as<Candidate>();
         a.cand_count = d_cand_count;
         a.cand_cap = ctx->cand_cap;
+        a.q_hi = g.q_hi.p;
+        a.q_lo = g.q_lo.p;
+        a.t_rows = g.t_rows;
+        a.err = reinterpret_cast<int *>(d_cand_count + 2);
 
         // 2. contraction with fused epilogue
         if (ctx->profile)
@@ -499,7 +544,10 @@ void execute_group(tm_ctx *ctx, GroupPlan &g, std::vector<std::vector<Hit>> &ans
                 count_launch(ctx);
         }
         TM_CUDA(cudaMemcpyAsync(hc, d_cand_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        TM_CUDA(cudaMemcpyAsync(hc + 2, d_cand_count + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
         TM_CUDA(cudaStreamSynchronize(s));
+        if (hc[2] != 0)
+            throw Failure{TM_ERR_TIMEOUT, "contraction kernel gave up waiting (code " + std::to_string(hc[2]) + ")"};
         ncand = hc[0];
         if (ncand <= ctx->cand_cap)
             break;
@@ -670,7 +718,7 @@ int tm_ctx_destroy(tm_ctx *ctx)
     }
     for (DevBuf *b : {&ctx->raw, &ctx->clean, &ctx->suf, &ctx->tkey, &ctx->bmin_u, &ctx->bmin_l, &ctx->list, &ctx->counters, &ctx->cand, &ctx->dist})
         b->release();
-    for (HostBuf *b : {&ctx->h_q, &ctx->h_order, &ctx->h_slots, &ctx->h_cand, &ctx->h_dist,
+    for (HostBuf *b : {&ctx->h_split, &ctx->h_q, &ctx->h_order, &ctx->h_slots, &ctx->h_cand, &ctx->h_dist,
                        &ctx->h_counters, &ctx->h_tkey})
         b->release();
     if (ctx->ev0)
@@ -902,6 +950,99 @@ int tm_profile_read(tm_ctx *ctx, char *name, size_t name_capacity, int64_t *laun
     ctx->prof_flops = 0.0;
     ctx->all_launches = 0;
     return TM_OK;
+}
+
+int tm_bound_diagnostics(tm_ctx *ctx, const float *queries, int count, int m, float *d, float *e, float *exact)
+{
+    if (ctx == nullptr || queries == nullptr || d == nullptr || e == nullptr || count < 1 || m < 1 ||
+        static_cast<uint64_t>(m) > ctx->n)
+        return TM_ERR_ARGUMENT;
+    return guarded(ctx, [&] {
+        TM_CUDA(cudaSetDevice(ctx->device));
+        std::vector<tm_request> reqs(static_cast<size_t>(count));
+        std::vector<int> idx(static_cast<size_t>(count));
+        for (int i = 0; i < count; i++)
+        {
+            reqs[i] = tm_request{queries + static_cast<size_t>(i) * m, m, TM_MODE_THRESHOLD, 1, 0, 1.0f, 0u};
+            idx[i] = i;
+        }
+        GroupPlan g;
+        uint64_t h2d = 0;
+        prepare_group(ctx, m, idx, reqs.data(), g, h2d);
+        LengthStats &ls = ensure_length(ctx, m);
+        const uint64_t W = ls.W;
+        if (W == 0 || W * static_cast<uint64_t>(count) > (1ull << 31))
+            throw Failure{TM_ERR_ARGUMENT, "diagnostics need 0 < windows x templates <= 2^31"};
+        const bool use_umma = ctx->kernel != TM_KERNEL_FP32 && g.t_rows > 0 && tmb::umma_supported(m, count, W);
+        for (int t = 0; t < count; t++)
+        {
+            g.htp[t].thr_ed = -FLT_MAX; // emit nothing
+            if (use_umma)
+                g.htp[t].a1_main = g.a1_umma[t];
+        }
+        cudaStream_t s = ctx->stream;
+        TM_CUDA(cudaMemcpyAsync(g.tp.p, g.htp.data(), sizeof(TemplParam) * g.T_pad, cudaMemcpyHostToDevice, s));
+        const size_t pairs = W * static_cast<size_t>(count);
+        DevBuf dd, de, dc;
+        dd.reserve(pairs * sizeof(float));
+        de.reserve(pairs * sizeof(float));
+        ctx->counters.reserve(4 * sizeof(uint32_t));
+        TM_CUDA(cudaMemsetAsync(ctx->counters.p, 0, 4 * sizeof(uint32_t), s));
+        TM_CUDA(cudaMemsetAsync(dd.p, 0xff, pairs * sizeof(float), s)); // NaN where nothing was written
+        TM_CUDA(cudaMemsetAsync(de.p, 0xff, pairs * sizeof(float), s));
+        ctx->cand.reserve(sizeof(Candidate) * 16);
+        tmb::ScanArgs a{};
+        a.x = ctx->clean.as<float>();
+        a.q = g.q.as<float>();
+        a.tp = g.tp.as<TemplParam>();
+        a.mean = ls.mean.as<float>();
+        a.inv = ls.inv.as<float>();
+        a.w0 = ls.w0;
+        a.W = static_cast<uint32_t>(W);
+        a.m_pad = g.m_pad;
+        a.T = count;
+        a.nb = 1;
+        a.cand = ctx->cand.as<Candidate>();
+        a.cand_count = ctx->counters.as<uint32_t>();
+        a.cand_cap = 0;
+        a.q_hi = g.q_hi.p;
+        a.q_lo = g.q_lo.p;
+        a.t_rows = g.t_rows;
+        a.err = reinterpret_cast<int *>(ctx->counters.as<uint32_t>() + 2);
+        a.dbg_d = dd.as<float>();
+        a.dbg_e = de.as<float>();
+        TM_CUDA(use_umma ? tmb::launch_scan_umma(a, s) : tmb::launch_scan_fp32(a, s));
+        count_launch(ctx);
+        TM_CUDA(cudaMemcpyAsync(d, dd.p, pairs * sizeof(float), cudaMemcpyDeviceToHost, s));
+        TM_CUDA(cudaMemcpyAsync(e, de.p, pairs * sizeof(float), cudaMemcpyDeviceToHost, s));
+        if (exact != nullptr)
+        {
+            std::vector<Candidate> all(pairs);
+            for (int t = 0; t < count; t++)
+                for (uint64_t j = 0; j < W; j++)
+                    all[static_cast<size_t>(t) * W + j] = Candidate{static_cast<uint32_t>(t), static_cast<uint32_t>(j)};
+            dc.reserve(pairs * sizeof(Candidate));
+            DevBuf dx;
+            dx.reserve(pairs * sizeof(float));
+            TM_CUDA(cudaMemcpyAsync(dc.p, all.data(), pairs * sizeof(Candidate), cudaMemcpyHostToDevice, s));
+            TM_CUDA(tmb::launch_rescore(dc.as<Candidate>(), static_cast<uint32_t>(pairs), g.tp.as<TemplParam>(),
+                                        g.q.as<float>(), g.order.as<int>(), ctx->raw.as<float>(), ls.w0, dx.as<float>(),
+                                        s));
+            count_launch(ctx);
+            TM_CUDA(cudaMemcpyAsync(exact, dx.p, pairs * sizeof(float), cudaMemcpyDeviceToHost, s));
+            TM_CUDA(cudaStreamSynchronize(s));
+            dx.release();
+        }
+        uint32_t err = 0;
+        TM_CUDA(cudaMemcpyAsync(&err, ctx->counters.as<uint32_t>() + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        TM_CUDA(cudaStreamSynchronize(s));
+        dd.release();
+        de.release();
+        dc.release();
+        g.release();
+        if (err != 0)
+            throw Failure{TM_ERR_TIMEOUT, "contraction kernel gave up waiting"};
+    });
 }
 
 int tm_d2h_bytes(tm_ctx *ctx, uint64_t *bytes)

@@ -23,6 +23,12 @@ struct ScanArgs
     Candidate *cand;
     uint32_t *cand_count;
     uint32_t cand_cap;
+    const void *q_hi;      // tensor-core kernel: BF16 high and low halves of q, t_rows x m_pad
+    const void *q_lo;
+    int t_rows;
+    int *err;              // set (non-zero) by a kernel that gave up waiting
+    float *dbg_d;          // diagnostics (tm_bound_diagnostics): every d and its bound e,
+    float *dbg_e;          //   [T][W]; null in searches
 };
 
 // Distance d of one (template, window) pair from its shifted dot product

@@ -140,6 +140,11 @@ __global__ void __launch_bounds__(F_THREADS, 2) k_scan_fp32(ScanArgs a)
                 continue; // excluded window (beyond range, missing start, degenerate)
             float d, e;
             fast_distance(p, p.a1_main, acc[w][tt], mu[w], iv[w], shift, d, e);
+            if (a.dbg_d != nullptr)
+            {
+                a.dbg_d[(size_t)t * a.W + j0 + w] = d;
+                a.dbg_e[(size_t)t * a.W + j0 + w] = e;
+            }
             const float lo = d - e, hi = d + e;
             if (p.mode == 1)
             {
