@@ -310,16 +310,24 @@ def run_ours(args, w):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     h2d = 0
     e0.record(stream)
+    phases = [0.0, 0.0, 0.0]
     for s in range(args.steps):
         chunk = reqs[((args.warmup + s) % nbatch) * per:((args.warmup + s) % nbatch + 1) * per]
+        t0 = time.perf_counter()
         b = ctx.batch(chunk)
+        t1 = time.perf_counter()
         h2d += b.h2d_bytes()
         b.run()
+        t2 = time.perf_counter()
         b.close()
+        t3 = time.perf_counter()
+        phases = [phases[0] + t1 - t0, phases[1] + t2 - t1, phases[2] + t3 - t2]
     e1.record(stream)
     barrier()
     e_ms = e0.elapsed_time(e1)
     d2h = ctx.d2h_bytes()
+    log('[bench] e2e host phases per step (create, run, close) ms: ' +
+        ', '.join(f'{1000 * p / args.steps:.1f}' for p in phases))
 
     t = torch.tensor([ms, e_ms, kms / max(launches, 1)], dtype=torch.float64, device=f'cuda:{local}')
     if dist:

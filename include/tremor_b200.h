@@ -50,6 +50,7 @@ extern "C" {
 #define TM_ERR_CAPACITY (-5)  /* caller buffer too small; the needed size was written */
 #define TM_ERR_NO_DEVICE (-6) /* no usable sm_100 device */
 #define TM_ERR_TIMEOUT (-7)   /* a kernel gave up waiting (bounded wait); the context stays usable */
+#define TM_ERR_TOO_LARGE (-8) /* input larger than the fixed scratch of tm_window_stats_noalloc */
 
 /* TREMOR_MISSING_VALUE (ZnormSearch.hpp:21): a missing sample counts as 0; a window
  * whose first sample is missing is not searched. */
@@ -134,6 +135,25 @@ int tm_batch_h2d_bytes(const tm_batch *batch, uint64_t *bytes);
 int tm_result_count(const tm_result *res, int request, uint64_t *count);
 int tm_result_get(const tm_result *res, int request, uint64_t *positions, float *distances, uint64_t capacity);
 void tm_result_free(tm_result *res);
+
+/* ---- allocation-free statistics ------------------------------------------------------ */
+
+/* No counterpart in the reference: an entry point for callers that must not allocate
+ * device memory (a live detector with a fixed latency budget, where cudaMalloc may
+ * synchronise the device; a runtime whose pool allocator holds the free memory; work
+ * recorded into a stream capture). It computes, on the calling thread's current device
+ * and on `stream` (a cudaStream_t, 0 for the default stream), the statistics of every
+ * window of length m of the device-resident waveform raw[0..n): mean, std and flags per
+ * window into caller-owned device arrays of n - m + 1 elements, with the meaning of
+ * tm_window_stats (equal to its values within a few float ulps) and flags bit 0 = first
+ * sample missing, bit 1 = constant window, bit 3 = two-pass statistics. It allocates
+ * nothing and does not synchronise: its only scratch is a fixed 8 MiB device array that
+ * every GPU loading the library holds until the process exits, so n + m must not exceed
+ * 524288 samples (larger inputs return TM_ERR_TOO_LARGE). The first call on a device
+ * looks that array up on the device (make it before any stream capture). All calls share
+ * the array: calls whose work overlaps on the GPU (other streams, other threads) race. */
+int tm_window_stats_noalloc(const float *raw, uint64_t n, int m, float *mean, float *stddev, uint8_t *flags,
+                            void *stream);
 
 /* ---- conversions (ZnormSearch.hpp:23-31, bit-identical) -------------------------- */
 float tm_cc_to_ed(float correlation, int m);
