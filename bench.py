@@ -214,6 +214,28 @@ def cpu_reference(w, x, q, budget_s=15.0, max_templates=32):
                   f'SkipSequentialScan sequential mode, {secs:.1f} s of search'}
 
 
+def cpu_mass(w, x, q, budget_s=8.0, max_templates=8):
+    """(pairs/s, info) of the reference's MASS V3 (dmass/DMASS_V3.c, restated in
+    oracle/mass_v3.py with scipy's pocketfft for FFTW) on the first 2^24 samples, all host
+    threads; its set-up (piece spectra, statistics) is not timed."""
+    sys.path.insert(0, str(ROOT / 'oracle'))
+    from mass_v3 import MassV3
+    n_s = min(len(x), 1 << 24)
+    t0 = time.time()
+    mass = MassV3(x[:n_s], w['m'])
+    log(f'[bench] MASS V3 set up in {time.time() - t0:.1f} s')
+    done, secs = 0, 0.0
+    while done < min(max_templates, len(q)) and (secs < budget_s or done == 0):
+        t0 = time.perf_counter()
+        mass.distances(q[done])
+        secs += time.perf_counter() - t0
+        done += 1
+    return done * mass.W / secs / 1e9, {'cores': mass.workers, 'kind': 'port',
+                                        'fft': 'scipy.fft pocketfft, double precision',
+                                        'sample': f'{done} templates x {mass.W} windows (first 2^24 samples), '
+                                                  f'{secs:.1f} s of queries'}
+
+
 def dist_setup(gpus):
     if gpus <= 1 or 'RANK' not in os.environ:
         return 0, 1, int(os.environ.get('LOCAL_RANK', 0)), None
@@ -355,6 +377,12 @@ def run_ours(args, w):
         roof['algorithmic_flops_per_launch'] = flops_per_launch
         roof['kernel_ms_per_launch'] = k_avg_ms
         cpu_v, cpu_info = (None, {'error': 'skipped'}) if args.no_cpu else cpu_reference(w, x, q)
+        if not args.no_cpu:
+            try:
+                mv, minfo = cpu_mass(w, x, q)
+                cpu_info['mass_v3'] = {'value': mv, 'unit': UNIT, **minfo}
+            except Exception as exc:  # the MASS leg is informative; the reference scan is the baseline
+                cpu_info['mass_v3'] = {'error': str(exc)[:200]}
         line = {'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
                 'warmup': args.warmup, 'ms_per_step': ms / args.steps, 'higher_is_better': True, 'scaling': 'weak',
                 'vs_baseline': None, 'dtype': 'bf16x3+f32' if kname == 'k_scan_umma' else 'f32',

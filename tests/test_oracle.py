@@ -128,3 +128,23 @@ def test_oracle_passes_validate_search_checks():
             assert actual == expected
             cc = [ob.ed_to_cc(d, m) for d in dist[qid == qi]]
             assert np.allclose(cc, corr[qi, sorted(actual)], atol=2e-4)
+
+
+def test_mass_v3_restatement_matches_fp64_oracle():
+    """oracle/mass_v3.py (DMASS_V3.c:798-996 with pocketfft for FFTW) gives the FP64
+    distances of validate_search's oracle to 1e-9 relative, and its kNN answers are the
+    FP64 expectations of validate_search.py:128-135."""
+    import sys
+    sys.path.insert(0, str(ob.ROOT / 'oracle'))
+    from mass_v3 import MassV3
+    meta, x, q = ob.load_golden('validate')
+    m, k = meta['m'], meta['k']
+    corr = _fp64_correlations(x, q, m)
+    mass = MassV3(x, m, workers=2)
+    for qi in range(len(q)):
+        d = mass.distances(q[qi])
+        ok = np.isfinite(corr[qi]) & (corr[qi] > -np.inf)
+        expect = 2 * m * (1 - corr[qi][ok])
+        assert np.allclose(d[ok], expect, rtol=1e-9, atol=1e-7 * m)
+        order = sorted(range(len(d)), key=lambda p: (d[p], p))[:k]
+        assert order == np.argsort(-corr[qi], kind='stable')[:k].tolist()
