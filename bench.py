@@ -52,6 +52,13 @@ WORKLOADS = {
                             per_step=64, seed=2028),
     'threshold': dict(n=1 << 26, q=256, m=2048, events=500, mode='threshold', k=1, merge=0, corr=0.8,
                       per_step=64, seed=2027),
+    # config 4: lengths log-uniform in [256, 8192] (multiples of 16), random centre
+    # frequencies, 50/50 kNN (k in {1, 10, 100}, merge m/2) and threshold (0.6-0.9); the
+    # whole batch is one step (one mixed-length launch)
+    'batching': dict(n=1 << 27, q=4096, m=(256, 8192), events=2000, mode='mixed', k=0, merge=0, corr=0.0,
+                     per_step=4096, seed=2029),
+    'batching_small': dict(n=1 << 25, q=512, m=(256, 8192), events=250, mode='mixed', k=0, merge=0, corr=0.0,
+                           per_step=512, seed=2029),
 }
 
 
@@ -62,13 +69,25 @@ def log(*a):
 def make_workload(w):
     from tremor_b200 import synth
     t0 = time.time()
-    x, q, _ = synth.workload(w['n'], w['q'], w['m'], w['events'], seed=w['seed'])
+    if w['mode'] == 'mixed':
+        x, q, _ = synth.mixed_workload(w['n'], w['q'], w['m'][0], w['m'][1], w['events'], seed=w['seed'])
+    else:
+        x, q, _ = synth.workload(w['n'], w['q'], w['m'], w['events'], seed=w['seed'])
     log(f'[bench] workload generated in {time.time() - t0:.1f} s')
     return x, q
 
 
 def requests_for(w, q):
     import tremor_b200 as tb
+    if w['mode'] == 'mixed':
+        rng = np.random.default_rng(w['seed'] + 1)
+        reqs = []
+        for i, t in enumerate(q):
+            if i % 2 == 0:
+                reqs.append(tb.Request(t, tb.MODE_KNN, k=int(rng.choice([1, 10, 100])), merge_offset=len(t) // 2))
+            else:
+                reqs.append(tb.Request(t, tb.MODE_THRESHOLD, correlation=float(rng.uniform(0.6, 0.9))))
+        return reqs
     if w['mode'] == 'knn':
         return [tb.Request(t, tb.MODE_KNN, k=w['k'], merge_offset=w['merge']) for t in q]
     return [tb.Request(t, tb.MODE_THRESHOLD, correlation=w['corr'], merge_offset=w['merge']) for t in q]
@@ -152,7 +171,7 @@ class RefScan:
     the first 2^24 samples of the waveform (its build is the reference's index step, not
     timed); search() times SkipSequentialScan::search_knn / search_threshold alone."""
 
-    def __init__(self, w, x, threads=None):
+    def __init__(self, w, x, m=None, threads=None):
         import ctypes
         from tests import oracle_bindings as ob
         self.w, self.ct, self.h = w, ctypes, None
@@ -170,21 +189,23 @@ class RefScan:
         ref.tmref_sss_destroy.argtypes = [ctypes.c_void_p]
         self.threads = threads or os.cpu_count() or 1
         n_s = min(len(x), 1 << 24)
-        self.windows = n_s - w['m'] + 1
+        self.m = m = m if m is not None else w['m']
+        self.windows = n_s - m + 1
         self.tmp = tempfile.TemporaryDirectory()
         wf = os.path.join(self.tmp.name, 'w.bin')
         x[:n_s].tofile(wf)
         t0 = time.time()
-        self.h = ref.tmref_sss_create(wf.encode(), n_s, w['m'], w['k'], w['merge'], 0, self.threads,
-                                      16 if w['m'] % 16 == 0 else 8)
+        self.h = ref.tmref_sss_create(wf.encode(), n_s, m, w['k'], w['merge'], 0, self.threads,
+                                      16 if m % 16 == 0 else 8)
         log(f'[bench] reference scan built in {time.time() - t0:.1f} s ({self.threads} threads)')
         self.error = None if self.h else 'reference build failed'
 
     def search(self, template) -> float:
         qi = np.ascontiguousarray(np.asarray(template, np.float32)[None, :])
         out = os.path.join(self.tmp.name, 'out.csv')
-        s = self.ref.tmref_sss_search(self.h, qi.ctypes.data_as(self.ct.c_void_p), 1,
-                                      1 if self.w['mode'] == 'knn' else 0, self.w['k'], self.w['corr'], out.encode())
+        knn = self.w['mode'] != 'threshold'
+        s = self.ref.tmref_sss_search(self.h, qi.ctypes.data_as(self.ct.c_void_p), 1, 1 if knn else 0,
+                                      max(self.w['k'], 10), self.w['corr'], out.encode())
         if s < 0:
             raise RuntimeError('reference search failed')
         return s
@@ -195,22 +216,39 @@ class RefScan:
             self.h = None
 
 
+def sample_templates(w, q):
+    """Templates of the CPU sample: all of them for single-length workloads; for the
+    mixed-length workload three templates spread over the lengths (one build each)."""
+    if w['mode'] != 'mixed':
+        return list(q)
+    order = sorted(range(len(q)), key=lambda i: len(q[i]))
+    return [q[order[len(order) * f // 4]] for f in (1, 2, 3)]
+
+
 def cpu_reference(w, x, q, budget_s=15.0, max_templates=32):
     """(pairs/s, info) of the reference's CPU scan over a bounded sample: as many templates as
     fit in about `budget_s` seconds of search, at least one."""
-    scan = RefScan(w, x)
-    if scan.error:
-        return None, {'error': scan.error}
+    tpls = sample_templates(w, q)
+    done, secs, pairs, threads = 0, 0.0, 0, 1
+    scans = {}
     try:
-        done, secs = 0, 0.0
-        while done < min(max_templates, len(q)) and (secs < budget_s or done == 0):
-            secs += scan.search(q[done])
+        while done < min(max_templates, len(tpls)) and (secs < budget_s or done == 0):
+            t = tpls[done]
+            if len(t) not in scans:
+                scans[len(t)] = RefScan(w, x, m=len(t))
+                if scans[len(t)].error:
+                    return None, {'error': scans[len(t)].error}
+            scan = scans[len(t)]
+            secs += scan.search(t)
+            pairs += scan.windows
+            threads = scan.threads
             done += 1
     finally:
-        scan.close()
-    return done * scan.windows / secs / 1e9, {
-        'cores': scan.threads, 'kind': 'reference',
-        'sample': f'{done} templates x {scan.windows} windows (first 2^24 samples of the waveform), '
+        for scan in scans.values():
+            scan.close()
+    return pairs / secs / 1e9, {
+        'cores': threads, 'kind': 'reference',
+        'sample': f'{done} templates x ~{pairs // max(done, 1)} windows (first 2^24 samples of the waveform), '
                   f'SkipSequentialScan sequential mode, {secs:.1f} s of search'}
 
 
@@ -221,19 +259,25 @@ def cpu_mass(w, x, q, budget_s=8.0, max_templates=8):
     sys.path.insert(0, str(ROOT / 'oracle'))
     from mass_v3 import MassV3
     n_s = min(len(x), 1 << 24)
-    t0 = time.time()
-    mass = MassV3(x[:n_s], w['m'])
-    log(f'[bench] MASS V3 set up in {time.time() - t0:.1f} s')
-    done, secs = 0, 0.0
-    while done < min(max_templates, len(q)) and (secs < budget_s or done == 0):
+    tpls = sample_templates(w, q)
+    done, secs, pairs, workers = 0, 0.0, 0, 1
+    masses = {}
+    while done < min(max_templates, len(tpls)) and (secs < budget_s or done == 0):
+        t = tpls[done]
+        if len(t) not in masses:
+            t0 = time.time()
+            masses[len(t)] = MassV3(x[:n_s], len(t))
+            log(f'[bench] MASS V3 set up in {time.time() - t0:.1f} s (m={len(t)})')
+        mass = masses[len(t)]
         t0 = time.perf_counter()
-        mass.distances(q[done])
+        mass.distances(t)
         secs += time.perf_counter() - t0
+        pairs += mass.W
+        workers = mass.workers
         done += 1
-    return done * mass.W / secs / 1e9, {'cores': mass.workers, 'kind': 'port',
-                                        'fft': 'scipy.fft pocketfft, double precision',
-                                        'sample': f'{done} templates x {mass.W} windows (first 2^24 samples), '
-                                                  f'{secs:.1f} s of queries'}
+    return pairs / secs / 1e9, {'cores': workers, 'kind': 'port', 'fft': 'scipy.fft pocketfft, double precision',
+                                'sample': f'{done} templates x ~{pairs // max(done, 1)} windows (first 2^24 samples), '
+                                          f'{secs:.1f} s of queries'}
 
 
 def dist_setup(gpus):
@@ -252,19 +296,28 @@ def run_reference(args, w):
             dist.destroy_process_group()
         return
     x, q = make_workload(w)  # the sample is the first 2^24 samples of the full waveform
-    scan = RefScan(w, x)
-    if scan.error:
-        print(json.dumps({'impl': 'reference', 'unavailable': scan.error}), flush=True)
-        return
+    tpls = sample_templates(w, q)
+    scans = {}
+    for t in tpls:
+        if len(t) not in scans:
+            scans[len(t)] = RefScan(w, x, m=len(t))
+            if scans[len(t)].error:
+                print(json.dumps({'impl': 'reference', 'unavailable': scans[len(t)].error}), flush=True)
+                return
     per_step = max(1, int(os.environ.get('TM_REF_TEMPLATES_PER_STEP', 2)))
     for s in range(args.warmup):
-        scan.search(q[s % len(q)])
-    secs = 0.0
+        t = tpls[s % len(tpls)]
+        scans[len(t)].search(t)
+    secs, pairs = 0.0, 0
     for s in range(args.steps):
-        for t in range(per_step):
-            secs += scan.search(q[(s * per_step + t) % len(q)])
-    scan.close()
-    value = args.steps * per_step * scan.windows / secs / 1e9
+        for i in range(per_step):
+            t = tpls[(s * per_step + i) % len(tpls)]
+            secs += scans[len(t)].search(t)
+            pairs += scans[len(t)].windows
+    for scan in scans.values():
+        scan.close()
+    scan = next(iter(scans.values()))
+    value = pairs / secs / 1e9
     info = {'cores': scan.threads, 'kind': 'reference',
             'sample': f'{per_step} templates x {scan.windows} windows per step (first 2^24 samples), '
                       'SkipSequentialScan sequential mode'}
@@ -290,14 +343,15 @@ def run_ours(args, w):
     ctx = tb.Context(x, device=local)
     ctx.set_kernel(kernel)
     t0 = time.time()
-    ctx.prepare_length(w['m'])
+    if w['mode'] != 'mixed':
+        ctx.prepare_length(w['m'])
     log(f'[bench] window statistics in {time.time() - t0:.2f} s')
     reqs = requests_for(w, q)
     per = w['per_step']
     nbatch = (len(reqs) + per - 1) // per
     batches = [ctx.batch(reqs[i * per:(i + 1) * per]) for i in range(nbatch)]
     stream = torch.cuda.ExternalStream(ctx.stream(), device=local)
-    windows = w['n'] - w['m'] + 1
+    pair_count = [sum(w['n'] - len(r.template) + 1 for r in reqs[i * per:(i + 1) * per]) for i in range(nbatch)]
 
     def barrier():
         torch.cuda.synchronize()
@@ -318,7 +372,7 @@ def run_ours(args, w):
     for s in range(args.steps):
         b = batches[(args.warmup + s) % nbatch]
         b.run()
-        pairs += b.count * windows
+        pairs += pair_count[(args.warmup + s) % nbatch]
     ev1.record(stream)
     barrier()
     clocks = sampler.stop()

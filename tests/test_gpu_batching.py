@@ -1,0 +1,116 @@
+"""Batches of templates of different lengths (one mixed-length contraction group whose
+window statistics come from the resident FP64 prefix sums) give exactly the reference's
+answers: positions and FP32 distance bits equal to the oracle's, for kNN and threshold
+requests mixed in one batch, on waveforms with missing samples, long constant stretches,
+a loud stretch followed by a quiet one (prefix-sum cancellation), and a large offset."""
+import numpy as np
+import pytest
+
+import tremor_b200 as tb
+from tests import oracle_bindings as ob
+
+pytestmark = pytest.mark.gpu
+
+
+def _waveform(n, seed, offset=0.0):
+    from tremor_b200 import synth
+    rng = np.random.default_rng(seed)
+    x = synth.ar2_waveform(n, rng) + np.float32(offset)
+    x[3000:9000] = np.float32(offset)               # long constant stretch
+    x[30000:34000] *= np.float32(1e5)               # loud ...
+    x[34000:40000] *= np.float32(1e-4)              # ... then quiet
+    x[rng.integers(0, n, 60)] = tb.MISSING_VALUE    # scattered missing samples
+    x[60000:60200] = tb.MISSING_VALUE               # a gap
+    return x
+
+
+def _requests(x, rng, lengths):
+    from tremor_b200 import synth
+    reqs = []
+    for i, m in enumerate(lengths):
+        if i % 3 == 0:
+            p = int(rng.integers(0, len(x) - m))
+            t = x[p:p + m].copy()
+            t[t == tb.MISSING_VALUE] = 0.0
+        else:
+            t = synth.chirp_templates(1, m, rng)[0]
+        if i % 2 == 0:
+            reqs.append(tb.Request(t, tb.MODE_KNN, k=int(rng.choice([1, 5, 20])),
+                                   merge_offset=int(rng.choice([0, m // 2]))))
+        else:
+            reqs.append(tb.Request(t, tb.MODE_THRESHOLD, correlation=float(rng.choice([0.3, 0.6, 0.85])),
+                                   merge_offset=int(rng.choice([0, 10]))))
+    return reqs
+
+
+def _check(x, reqs, answers):
+    for r, (pos, dist) in zip(reqs, answers):
+        m = len(r.template)
+        if r.mode == tb.MODE_KNN:
+            I, D = ob.scan_knn(x, r.template[None, :], m, r.k, r.merge_offset)
+            assert np.array_equal(pos, I[0]), (m, r.k, r.merge_offset)
+            assert np.array_equal(dist.view(np.uint32), D[0].view(np.uint32)), (m, r.k)
+        else:
+            qid, p, d = ob.scan_threshold(x, r.template[None, :], m, r.correlation, r.merge_offset)
+            assert np.array_equal(pos, p), (m, r.correlation, r.merge_offset)
+            assert np.array_equal(dist.view(np.uint32), d.view(np.uint32))
+
+
+@pytest.mark.parametrize('offset', [0.0, 5000.0])
+def test_mixed_lengths_match_oracle(offset):
+    x = _waveform(1 << 17, 5 + int(offset), offset)
+    rng = np.random.default_rng(6)
+    lengths = [int(v) for v in rng.choice([40, 64, 100, 128, 200, 333, 512, 1000, 2048], size=18)]
+    reqs = _requests(x, rng, lengths)
+    with tb.Context(x) as ctx:
+        answers = ctx.scan_batch(reqs)
+    _check(x, reqs, answers)
+
+
+def test_mixed_lengths_window_range():
+    x = _waveform(1 << 16, 8)
+    rng = np.random.default_rng(9)
+    reqs = _requests(x, rng, [64, 96, 150, 300, 64, 500])
+    first, count = 7000, 40000
+    with tb.Context(x) as ctx:
+        ctx.set_window_range(first, count)
+        answers = ctx.scan_batch(reqs)
+    for r, (pos, dist) in zip(reqs, answers):
+        m = len(r.template)
+        part = x[first:min(len(x), first + count + m - 1)]
+        if r.mode == tb.MODE_KNN:
+            I, D = ob.scan_knn(part, r.template[None, :], m, r.k, r.merge_offset)
+            assert np.array_equal(pos, np.where(D[0] < ob.FLT_MAX, I[0] + first, 0))
+            assert np.array_equal(dist.view(np.uint32), D[0].view(np.uint32))
+        else:
+            qid, p, d = ob.scan_threshold(part, r.template[None, :], m, r.correlation, r.merge_offset)
+            assert np.array_equal(pos, p + first)
+            assert np.array_equal(dist.view(np.uint32), d.view(np.uint32))
+
+
+def test_mixed_lengths_sparse_unbounded():
+    """So few windows that no kNN bound exists: constant windows (distance FLT_MAX) fill
+    the answers in position order, as the reference's unfilled queue makes them do."""
+    rng = np.random.default_rng(10)
+    x = rng.normal(size=600).astype(np.float32)
+    x[100:260] = 3.0
+    reqs = [tb.Request(x[20:84].copy(), tb.MODE_KNN, k=12, merge_offset=40),
+            tb.Request(rng.normal(size=100).astype(np.float32), tb.MODE_KNN, k=9, merge_offset=30),
+            tb.Request(rng.normal(size=48).astype(np.float32), tb.MODE_THRESHOLD, correlation=-0.2)]
+    with tb.Context(x) as ctx:
+        answers = ctx.scan_batch(reqs)
+    _check(x, reqs, answers)
+
+
+def test_constant_stretch_does_not_flood_candidates():
+    """Windows inside a long constant stretch are recognised from the constant-run lengths,
+    not handed one by one to the exact re-scoring."""
+    from tremor_b200 import synth
+    rng = np.random.default_rng(12)
+    x = synth.ar2_waveform(1 << 18, rng)
+    x[10000:200000] = 0.0
+    reqs = [tb.Request(synth.chirp_templates(1, m, rng)[0], tb.MODE_THRESHOLD, correlation=0.9)
+            for m in [64, 128, 256, 512]]
+    with tb.Context(x) as ctx:
+        ctx.scan_batch(reqs)
+        assert ctx.last_candidates() < 5000

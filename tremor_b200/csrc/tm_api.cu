@@ -43,6 +43,12 @@ cudaError_t launch_passb(const uint2 *list, uint32_t items, const float *x, cons
                          Candidate *cand, uint32_t *cand_count, uint32_t cand_cap, cudaStream_t s);
 cudaError_t launch_rescore(const Candidate *cand, uint32_t count, const TemplParam *tp, const float *q,
                            const int *order, const float *raw, uint64_t w0, float *dist, cudaStream_t s);
+cudaError_t launch_prefix(const float *clean, uint64_t n, double c, double2 *totals, double2 *P, uint16_t *run,
+                          uint16_t *run_tmp, cudaStream_t s);
+cudaError_t launch_passb_mixed(const uint2 *list, uint32_t items, const float *x, const float *raw, const double2 *P,
+                               const uint16_t *run, double center, const float *q, const TemplParam *tp,
+                               const uint32_t *tkey, uint64_t w0, Candidate *cand, uint32_t *cand_count,
+                               uint32_t cand_cap, cudaStream_t s);
 } // namespace tmb
 
 using tmb::Candidate;
@@ -166,6 +172,10 @@ struct tm_ctx
     uint64_t use_clock = 0;
     // scratch
     DevBuf suf, tkey, bmin_u, bmin_l, list, counters, cand, dist;
+    // length-independent statistics (mixed-length batches): FP64 prefix sums, constant runs
+    DevBuf prefix, run;
+    double center = 0.0;
+    bool prefix_ready = false;
     HostBuf h_split, h_q, h_order, h_slots, h_cand, h_dist, h_counters, h_tkey;
     uint32_t cand_cap = 1u << 22, list_cap = 1u << 20;
     std::string err;
@@ -294,8 +304,15 @@ struct GroupPlan
     std::vector<TemplParam> htp;
     DevBuf q, order, tp, slots, q_hi, q_lo;
     int t_rows = 0;
+    // templates of several lengths (sorted by length, longest first) in 128-row tiles
+    bool mixed = false;
+    int k_stride = 0;            // row stride of the template arrays
+    uint32_t w_max = 0;          // windows of the shortest template
+    std::vector<int> tile_kb;    // K blocks of 64 samples per tile
+    DevBuf d_tile_kb;
     void release()
     {
+        d_tile_kb.release();
         q_hi.release();
         q_lo.release();
         q.release();
@@ -419,6 +436,191 @@ void prepare_group(tm_ctx *ctx, int m, const std::vector<int> &idx, const tm_req
     TM_CUDA(cudaStreamSynchronize(s));
     h2d += sizeof(float) * static_cast<uint64_t>(T) * m + sizeof(int) * static_cast<uint64_t>(T) * nblk +
            sizeof(TemplParam) * T_pad;
+}
+
+// Resident FP64 prefix sums and constant-run lengths of the waveform (built once).
+void ensure_prefix(tm_ctx *ctx)
+{
+    if (ctx->prefix_ready)
+        return;
+    cudaStream_t s = ctx->stream;
+    const uint64_t n = ctx->n;
+    const uint64_t chunks = (n + 8191) / 8192;
+    ctx->prefix.reserve(sizeof(double2) * (n + 1));
+    ctx->run.reserve(sizeof(uint16_t) * n);
+    DevBuf totals, run_tmp;
+    totals.reserve(sizeof(double2) * chunks);
+    run_tmp.reserve(sizeof(uint16_t) * n);
+    // pass 1 without centring gives the mean; pass 2 centres on it
+    TM_CUDA(tmb::launch_prefix(ctx->clean.as<float>(), n, 0.0, totals.as<double2>(), ctx->prefix.as<double2>(),
+                               ctx->run.as<uint16_t>(), run_tmp.as<uint16_t>(), s));
+    double2 last;
+    TM_CUDA(cudaMemcpyAsync(&last, ctx->prefix.as<double2>() + n, sizeof(double2), cudaMemcpyDeviceToHost, s));
+    TM_CUDA(cudaStreamSynchronize(s));
+    ctx->center = last.x / static_cast<double>(n);
+    TM_CUDA(tmb::launch_prefix(ctx->clean.as<float>(), n, ctx->center, totals.as<double2>(),
+                               ctx->prefix.as<double2>(), ctx->run.as<uint16_t>(), run_tmp.as<uint16_t>(), s));
+    TM_CUDA(cudaStreamSynchronize(s));
+    count_launch(ctx, 2 * 16);
+    totals.release();
+    run_tmp.release();
+    ctx->prefix_ready = true;
+}
+
+// Host preparation of a mixed-length group: templates sorted by length (longest first),
+// 128-row tiles whose K extent is their longest template (shorter rows zero-padded, which
+// leaves their dot products unchanged), window statistics from the prefix sums.
+void prepare_group_mixed(tm_ctx *ctx, const std::vector<int> &idx_in, const tm_request *reqs, GroupPlan &g,
+                         uint64_t &h2d)
+{
+    std::vector<int> idx = idx_in;
+    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return reqs[a].m > reqs[b].m; });
+    const int T = static_cast<int>(idx.size());
+    const int m_max = reqs[idx[0]].m;
+    g.mixed = true;
+    g.m = m_max;
+    g.T = T;
+    g.T_pad = (T + 63) & ~63;
+    g.t_rows = (T + 127) & ~127;
+    g.k_stride = (m_max + 63) & ~63;
+    g.m_pad = g.k_stride;
+    g.nblk = std::max(1, g.k_stride / tm_host::kZnormBlock);
+    g.umma_constants = true;
+    g.index = idx;
+    const int rows = g.t_rows, stride = g.k_stride, nblk = g.nblk;
+    const size_t elems = static_cast<size_t>(rows) * stride;
+    ctx->h_q.reserve(sizeof(float) * elems);
+    ctx->h_order.reserve(sizeof(int) * static_cast<size_t>(T) * nblk);
+    ctx->h_slots.reserve(sizeof(int) * T);
+    ctx->h_split.reserve(2 * sizeof(uint16_t) * elems);
+    float *hq = ctx->h_q.as<float>();
+    int *ho = ctx->h_order.as<int>();
+    int *hslots = ctx->h_slots.as<int>();
+    uint16_t *hh = ctx->h_split.as<uint16_t>(), *hl = hh + elems;
+    std::memset(hq, 0, sizeof(float) * elems);
+    std::memset(ho, 0, sizeof(int) * static_cast<size_t>(T) * nblk);
+    std::memset(hh, 0, 2 * sizeof(uint16_t) * elems);
+    g.htp.assign(g.T_pad, TemplParam{});
+    g.mode.assign(T, 0);
+    g.k.assign(T, 0);
+    g.merge.assign(T, 0);
+    g.thr.assign(T, 0.0f);
+    g.a1_umma.assign(T, 0.0f);
+    g.nk = 0;
+    g.w_max = 0;
+    const uint64_t w0 = ctx->range_first;
+    for (int t = 0; t < T; t++)
+    {
+        const tm_request *r = &reqs[idx[t]];
+        const int m = r->m;
+        float *q = hq + static_cast<size_t>(t) * stride;
+        std::memcpy(q, r->templ, sizeof(float) * m);
+        if (!(r->flags & TM_FLAG_ZNORMALIZED))
+            tm_host::znormalize(q, m);
+        tm_host::block_order(q, m, ho + static_cast<size_t>(t) * nblk);
+        double q2 = 0.0, s1 = 0.0;
+        for (int i = 0; i < m; i++)
+        {
+            q2 += static_cast<double>(q[i]) * q[i];
+            s1 += q[i];
+            const size_t at = static_cast<size_t>(t) * stride + i;
+            hh[at] = bf16_bits(q[i]);
+            hl[at] = bf16_bits(q[i] - bf16_value(hh[at]));
+        }
+        TemplParam &p = g.htp[t];
+        fill_param(p, m, q2, s1, gamma_bf16(m), gamma_fp32(m));
+        g.a1_umma[t] = p.a1_main;
+        p.inv_m = 1.0 / static_cast<double>(m);
+        p.qs = static_cast<float>(std::sqrt(q2 * m));
+        const uint64_t total = ctx->n - static_cast<uint64_t>(m) + 1;
+        p.wcount = static_cast<uint32_t>(w0 >= total ? 0 : std::min<uint64_t>(ctx->range_count, total - w0));
+        g.w_max = std::max(g.w_max, p.wcount);
+        p.mode = g.mode[t] = r->mode;
+        p.k = g.k[t] = r->k;
+        p.merge = g.merge[t] = r->merge_offset;
+        p.q_offset = static_cast<int64_t>(t) * stride;
+        p.order_offset = static_cast<int64_t>(t) * nblk;
+        if (r->mode == TM_MODE_KNN)
+            hslots[g.nk++] = t;
+        else
+            p.thr_ed = g.thr[t] = tm_host::cc_to_ed(r->correlation, m);
+    }
+    for (int t = T; t < g.T_pad; t++)
+    {
+        g.htp[t].mode = TM_MODE_THRESHOLD;
+        g.htp[t].thr_ed = -FLT_MAX;
+        g.htp[t].m = m_max;
+    }
+    g.tile_kb.assign(rows / 128, 0);
+    for (int tt = 0; tt < rows / 128; tt++)
+        g.tile_kb[tt] = (reqs[idx[tt * 128]].m + 63) / 64; // longest template of the tile
+    cudaStream_t s = ctx->stream;
+    g.q.reserve(sizeof(float) * elems);
+    g.order.reserve(sizeof(int) * static_cast<size_t>(T) * nblk);
+    g.tp.reserve(sizeof(TemplParam) * g.T_pad);
+    g.slots.reserve(sizeof(int) * std::max(g.nk, 1));
+    g.q_hi.reserve(sizeof(uint16_t) * elems);
+    g.q_lo.reserve(sizeof(uint16_t) * elems);
+    g.d_tile_kb.reserve(sizeof(int) * g.tile_kb.size());
+    TM_CUDA(cudaMemcpyAsync(g.q.p, hq, sizeof(float) * elems, cudaMemcpyHostToDevice, s));
+    TM_CUDA(cudaMemcpyAsync(g.order.p, ho, sizeof(int) * static_cast<size_t>(T) * nblk, cudaMemcpyHostToDevice, s));
+    TM_CUDA(cudaMemcpyAsync(g.tp.p, g.htp.data(), sizeof(TemplParam) * g.T_pad, cudaMemcpyHostToDevice, s));
+    if (g.nk > 0)
+        TM_CUDA(cudaMemcpyAsync(g.slots.p, hslots, sizeof(int) * g.nk, cudaMemcpyHostToDevice, s));
+    TM_CUDA(cudaMemcpyAsync(g.q_hi.p, hh, sizeof(uint16_t) * elems, cudaMemcpyHostToDevice, s));
+    TM_CUDA(cudaMemcpyAsync(g.q_lo.p, hl, sizeof(uint16_t) * elems, cudaMemcpyHostToDevice, s));
+    TM_CUDA(cudaMemcpyAsync(g.d_tile_kb.p, g.tile_kb.data(), sizeof(int) * g.tile_kb.size(), cudaMemcpyHostToDevice,
+                            s));
+    TM_CUDA(cudaStreamSynchronize(s));
+    uint64_t samples = 0;
+    for (int t = 0; t < T; t++)
+        samples += static_cast<uint64_t>(reqs[idx[t]].m);
+    h2d += samples * (sizeof(float) + 2 * sizeof(uint16_t)) + sizeof(int) * static_cast<uint64_t>(T) * nblk +
+           sizeof(TemplParam) * g.T_pad;
+}
+
+// Canonical answers from the exactly re-scored candidates of each template of a group.
+// kNN: selection over (distance, position). When the bound was unbounded (too few
+// separated windows for the reference's queue to fill), the windows of distance FLT_MAX
+// (constant windows, which the contraction skips, plus any re-scored to FLT_MAX) follow
+// the finite ones in position order, as in the reference. Threshold: filter + merge.
+template <class Degenerate>
+void finish_answers(tm_ctx *ctx, const GroupPlan &g, std::vector<std::vector<Hit>> &per,
+                    std::vector<std::vector<Hit>> &answers, Degenerate degenerate_windows)
+{
+    const uint32_t *tkey = ctx->h_tkey.as<uint32_t>();
+    for (int t = 0; t < g.T; t++)
+    {
+        std::vector<Hit> &out = answers[g.index[t]];
+        out.clear();
+        if (g.mode[t] == TM_MODE_KNN)
+        {
+            std::vector<Hit> finite, infinite;
+            for (const Hit &h : per[t])
+                (h.dist < FLT_MAX ? finite : infinite).push_back(h);
+            tm_host::select_knn(finite, g.k[t], g.merge[t], out);
+            if (static_cast<int>(out.size()) < g.k[t] && tkey[t] == tmb::kEmptyKey)
+            {
+                degenerate_windows(t, infinite);
+                std::sort(infinite.begin(), infinite.end(), [](const Hit &a, const Hit &b) { return a.pos < b.pos; });
+                infinite.erase(std::unique(infinite.begin(), infinite.end(),
+                                           [](const Hit &a, const Hit &b) { return a.pos == b.pos; }),
+                               infinite.end());
+                tm_host::extend_knn(infinite, g.k[t], g.merge[t], out);
+            }
+            while (static_cast<int>(out.size()) < g.k[t])
+                out.push_back(Hit{0, FLT_MAX});
+        }
+        else
+        {
+            std::vector<Hit> hits;
+            hits.reserve(per[t].size());
+            for (const Hit &h : per[t])
+                if (h.dist <= g.thr[t])
+                    hits.push_back(h);
+            tm_host::threshold_merge(hits, g.merge[t], out);
+        }
+    }
 }
 
 // Device pipeline and selection for one prepared group; writes answers[index].
@@ -584,54 +786,217 @@ void execute_group(tm_ctx *ctx, GroupPlan &g, std::vector<std::vector<Hit>> &ans
     for (uint32_t i = 0; i < ncand; i++)
         per[hcand[i].templ].push_back(Hit{w0 + hcand[i].window, hdist[i]});
     std::vector<uint8_t> flags; // fetched only when some kNN bound is unbounded
-    for (int t = 0; t < T; t++)
-    {
-        std::vector<Hit> &out = answers[g.index[t]];
-        out.clear();
-        if (g.mode[t] == TM_MODE_KNN)
+    finish_answers(ctx, g, per, answers, [&](int, std::vector<Hit> &degenerate) {
+        if (flags.empty())
         {
-            tm_host::select_knn(per[t], g.k[t], g.merge[t], out);
-            const bool unbounded = ctx->h_tkey.as<uint32_t>()[t] == tmb::kEmptyKey;
-            if (static_cast<int>(out.size()) < g.k[t] && unbounded)
-            {
-                // Too few separated windows for a finite bound: the reference's queue never
-                // fills, so its constant windows (distance FLT_MAX) are candidates too.
-                if (flags.empty())
-                {
-                    flags.resize(W);
-                    TM_CUDA(cudaMemcpy(flags.data(), ls.flags.p, W, cudaMemcpyDeviceToHost));
-                }
-                std::vector<Hit> degenerate;
-                for (uint64_t j = 0; j < W; j++)
-                    if ((flags[j] & tmb::kFlagDegenerate) && !(flags[j] & tmb::kFlagMissingStart))
-                        degenerate.push_back(Hit{w0 + j, FLT_MAX});
-                tm_host::extend_knn(degenerate, g.k[t], g.merge[t], out);
-            }
-            while (static_cast<int>(out.size()) < g.k[t])
-                out.push_back(Hit{0, FLT_MAX});
+            flags.resize(W);
+            TM_CUDA(cudaMemcpy(flags.data(), ls.flags.p, W, cudaMemcpyDeviceToHost));
         }
-        else
-        {
-            std::vector<Hit> hits;
-            hits.reserve(per[t].size());
-            for (const Hit &h : per[t])
-                if (h.dist <= g.thr[t])
-                    hits.push_back(h);
-            tm_host::threshold_merge(hits, g.merge[t], out);
-        }
-    }
+        for (uint64_t j = 0; j < W; j++)
+            if ((flags[j] & tmb::kFlagDegenerate) && !(flags[j] & tmb::kFlagMissingStart))
+                degenerate.push_back(Hit{w0 + j, FLT_MAX});
+    });
 }
 
+// Device pipeline for a mixed-length group (tensor-core kernel only).
+void execute_group_mixed(tm_ctx *ctx, GroupPlan &g, std::vector<std::vector<Hit>> &answers)
+{
+    if (ctx->kernel == TM_KERNEL_FP32)
+        throw Failure{TM_ERR_STATE, "batch of several template lengths was prepared for the tensor-core kernel"};
+    ensure_prefix(ctx);
+    const int T = g.T, nk = g.nk;
+    const uint64_t w0 = ctx->range_first, W = g.w_max;
+    if (W == 0)
+    {
+        for (int t = 0; t < T; t++)
+            answers[g.index[t]] = g.mode[t] == TM_MODE_KNN
+                                      ? std::vector<Hit>(static_cast<size_t>(g.k[t]), Hit{0, FLT_MAX})
+                                      : std::vector<Hit>();
+        return;
+    }
+    if (W >= (1ull << 32))
+        throw Failure{TM_ERR_ARGUMENT, "more than 2^32 - 1 windows in one range; split the range"};
+    cudaStream_t s = ctx->stream;
+    ctx->tkey.reserve(sizeof(uint32_t) * T);
+    const uint32_t nb = static_cast<uint32_t>((W + tmb::kBucket - 1) / tmb::kBucket);
+    if (nk > 0)
+    {
+        ctx->bmin_u.reserve(sizeof(uint32_t) * static_cast<size_t>(T) * nb);
+        ctx->bmin_l.reserve(sizeof(uint32_t) * static_cast<size_t>(T) * nb);
+    }
+    ctx->counters.reserve(4 * sizeof(uint32_t));
+    ctx->h_counters.reserve(4 * sizeof(uint32_t));
+    uint32_t *hc = ctx->h_counters.as<uint32_t>();
+    double flops = 0.0;
+    for (int t = 0; t < T; t++)
+        flops += 2.0 * g.htp[t].m * static_cast<double>(g.htp[t].wcount);
+
+    uint32_t ncand = 0;
+    for (int attempt = 0; attempt < 3; attempt++)
+    {
+        ctx->cand.reserve(sizeof(Candidate) * static_cast<size_t>(ctx->cand_cap));
+        if (nk > 0)
+        {
+            TM_CUDA(cudaMemsetAsync(ctx->bmin_u.p, 0xff, sizeof(uint32_t) * static_cast<size_t>(T) * nb, s));
+            TM_CUDA(cudaMemsetAsync(ctx->bmin_l.p, 0xff, sizeof(uint32_t) * static_cast<size_t>(T) * nb, s));
+        }
+        TM_CUDA(cudaMemsetAsync(ctx->counters.p, 0, 4 * sizeof(uint32_t), s));
+        uint32_t *d_cand_count = ctx->counters.as<uint32_t>();
+        uint32_t *d_list_count = d_cand_count + 1;
+        tmb::ScanArgs a{};
+        a.x = ctx->clean.as<float>();
+        a.q = g.q.as<float>();
+        a.tp = g.tp.as<TemplParam>();
+        a.w0 = w0;
+        a.W = static_cast<uint32_t>(W);
+        a.m_pad = g.k_stride;
+        a.T = T;
+        a.bmin_u = ctx->bmin_u.as<uint32_t>();
+        a.bmin_l = ctx->bmin_l.as<uint32_t>();
+        a.nb = nb;
+        a.cand = ctx->cand.as<Candidate>();
+        a.cand_count = d_cand_count;
+        a.cand_cap = ctx->cand_cap;
+        a.q_hi = g.q_hi.p;
+        a.q_lo = g.q_lo.p;
+        a.t_rows = g.t_rows;
+        a.err = reinterpret_cast<int *>(d_cand_count + 2);
+        a.raw = ctx->raw.as<float>();
+        a.P = ctx->prefix.as<double2>();
+        a.run = ctx->run.as<uint16_t>();
+        a.center = ctx->center;
+        a.tile_kb = g.d_tile_kb.as<int>();
+        a.k_stride = g.k_stride;
+        if (ctx->profile)
+            TM_CUDA(cudaEventRecord(ctx->ev0, s));
+        TM_CUDA(tmb::launch_scan_umma(a, s));
+        count_launch(ctx);
+        if (ctx->profile)
+        {
+            TM_CUDA(cudaEventRecord(ctx->ev1, s));
+            TM_CUDA(cudaEventSynchronize(ctx->ev1));
+            float ms = 0.0f;
+            TM_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+            ctx->kname = "k_scan_umma";
+            ctx->prof_launches++;
+            ctx->prof_ms += ms;
+            ctx->prof_flops += flops;
+        }
+        if (nk > 0)
+        {
+            TM_CUDA(tmb::launch_bucket_select(ctx->bmin_u.as<uint32_t>(), nb, g.tp.as<TemplParam>(),
+                                              g.slots.as<int>(), nk, ctx->tkey.as<uint32_t>(), s));
+            for (int la = 0; la < 3; la++)
+            {
+                ctx->list.reserve(sizeof(uint2) * static_cast<size_t>(ctx->list_cap));
+                TM_CUDA(cudaMemsetAsync(d_list_count, 0, sizeof(uint32_t), s));
+                TM_CUDA(tmb::launch_list_buckets(ctx->bmin_l.as<uint32_t>(), nb, g.slots.as<int>(), nk,
+                                                 ctx->tkey.as<uint32_t>(), ctx->list.as<uint2>(), d_list_count,
+                                                 ctx->list_cap, s));
+                TM_CUDA(cudaMemcpyAsync(hc + 1, d_list_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+                TM_CUDA(cudaStreamSynchronize(s));
+                count_launch(ctx, 2);
+                if (hc[1] <= ctx->list_cap)
+                    break;
+                ctx->list_cap = hc[1] + hc[1] / 2;
+            }
+            if (hc[1] > ctx->list_cap)
+                throw Failure{TM_ERR_NO_MEMORY, "bucket list overflow"};
+            TM_CUDA(tmb::launch_passb_mixed(ctx->list.as<uint2>(), hc[1], ctx->clean.as<float>(),
+                                            ctx->raw.as<float>(), ctx->prefix.as<double2>(), ctx->run.as<uint16_t>(),
+                                            ctx->center, g.q.as<float>(), g.tp.as<TemplParam>(),
+                                            ctx->tkey.as<uint32_t>(), w0, ctx->cand.as<Candidate>(), d_cand_count,
+                                            ctx->cand_cap, s));
+            if (hc[1] > 0)
+                count_launch(ctx);
+        }
+        TM_CUDA(cudaMemcpyAsync(hc, d_cand_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        TM_CUDA(cudaMemcpyAsync(hc + 2, d_cand_count + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        TM_CUDA(cudaStreamSynchronize(s));
+        if (hc[2] != 0)
+            throw Failure{TM_ERR_TIMEOUT, "contraction kernel gave up waiting (code " + std::to_string(hc[2]) + ")"};
+        ncand = hc[0];
+        if (ncand <= ctx->cand_cap)
+            break;
+        ctx->cand_cap = ncand + ncand / 2;
+        if (attempt == 2)
+            throw Failure{TM_ERR_NO_MEMORY, "candidate buffer overflow"};
+    }
+    ctx->dist.reserve(sizeof(float) * std::max<uint32_t>(ncand, 1));
+    TM_CUDA(tmb::launch_rescore(ctx->cand.as<Candidate>(), ncand, g.tp.as<TemplParam>(), g.q.as<float>(),
+                                g.order.as<int>(), ctx->raw.as<float>(), w0, ctx->dist.as<float>(), s));
+    if (ncand > 0)
+        count_launch(ctx);
+    ctx->h_cand.reserve(sizeof(Candidate) * std::max<uint32_t>(ncand, 1));
+    ctx->h_dist.reserve(sizeof(float) * std::max<uint32_t>(ncand, 1));
+    ctx->h_tkey.reserve(sizeof(uint32_t) * std::max(T, 1));
+    if (ncand > 0)
+    {
+        TM_CUDA(cudaMemcpyAsync(ctx->h_cand.p, ctx->cand.p, sizeof(Candidate) * ncand, cudaMemcpyDeviceToHost, s));
+        TM_CUDA(cudaMemcpyAsync(ctx->h_dist.p, ctx->dist.p, sizeof(float) * ncand, cudaMemcpyDeviceToHost, s));
+    }
+    if (nk > 0)
+        TM_CUDA(cudaMemcpyAsync(ctx->h_tkey.p, ctx->tkey.p, sizeof(uint32_t) * T, cudaMemcpyDeviceToHost, s));
+    TM_CUDA(cudaStreamSynchronize(s));
+    ctx->last_candidates += ncand;
+    ctx->d2h_bytes += (sizeof(Candidate) + sizeof(float)) * static_cast<uint64_t>(ncand) + 8 +
+                      (nk > 0 ? sizeof(uint32_t) * T : 0);
+
+    std::vector<std::vector<Hit>> per(T);
+    const Candidate *hcand = ctx->h_cand.as<Candidate>();
+    const float *hdist = ctx->h_dist.as<float>();
+    for (uint32_t i = 0; i < ncand; i++)
+        per[hcand[i].templ].push_back(Hit{w0 + hcand[i].window, hdist[i]});
+    std::vector<uint16_t> run;
+    std::vector<float> raw;
+    finish_answers(ctx, g, per, answers, [&](int t, std::vector<Hit> &degenerate) {
+        if (run.empty())
+        {
+            run.resize(W);
+            raw.resize(W);
+            TM_CUDA(cudaMemcpy(run.data(), ctx->run.as<uint16_t>() + w0, W * sizeof(uint16_t), cudaMemcpyDeviceToHost));
+            TM_CUDA(cudaMemcpy(raw.data(), ctx->raw.as<float>() + w0, W * sizeof(float), cudaMemcpyDeviceToHost));
+        }
+        const TemplParam &p = g.htp[t];
+        for (uint64_t j = 0; j < p.wcount; j++)
+            if (run[j] >= p.m && raw[j] != TM_MISSING_VALUE)
+                degenerate.push_back(Hit{w0 + j, FLT_MAX});
+    });
+}
+
+// Groups of a batch. Lengths with a full 128-template tile (or any length, on the FP32
+// kernel) get their own group with per-length statistics; the remaining templates of
+// several lengths share one mixed-length group on the tensor cores.
 void create_batch(tm_ctx *ctx, const tm_request *requests, int count, tm_batch &b)
 {
     b.count = count;
     std::map<int, std::vector<int>> by_m;
     for (int i = 0; i < count; i++)
         by_m[requests[i].m].push_back(i);
-    b.groups.resize(by_m.size());
-    size_t gi = 0;
+    const bool tensor = ctx->kernel != TM_KERNEL_FP32 && tmb::umma_supported(0, 0, 0);
+    std::vector<int> rest;
+    std::vector<std::pair<int, std::vector<int>>> single;
     for (auto &kv : by_m)
+    {
+        if (!tensor || kv.second.size() >= 128 || kv.first > 16384)
+            single.emplace_back(kv.first, kv.second);
+        else
+            rest.insert(rest.end(), kv.second.begin(), kv.second.end());
+    }
+    std::map<int, int> rest_lengths;
+    for (int i : rest)
+        rest_lengths[requests[i].m]++;
+    if (rest_lengths.size() == 1)
+    {
+        single.emplace_back(rest_lengths.begin()->first, rest);
+        rest.clear();
+    }
+    b.groups.resize(single.size() + (rest.empty() ? 0 : 1));
+    size_t gi = 0;
+    for (auto &kv : single)
         prepare_group(ctx, kv.first, kv.second, requests, b.groups[gi++], b.h2d_bytes);
+    if (!rest.empty())
+        prepare_group_mixed(ctx, rest, requests, b.groups[gi++], b.h2d_bytes);
 }
 
 void run_batch(tm_ctx *ctx, tm_batch &b, tm_result &res)
@@ -639,7 +1004,12 @@ void run_batch(tm_ctx *ctx, tm_batch &b, tm_result &res)
     res.answers.assign(static_cast<size_t>(b.count), std::vector<Hit>());
     ctx->last_candidates = 0;
     for (GroupPlan &g : b.groups)
-        execute_group(ctx, g, res.answers);
+    {
+        if (g.mixed)
+            execute_group_mixed(ctx, g, res.answers);
+        else
+            execute_group(ctx, g, res.answers);
+    }
 }
 
 int validate_requests(const tm_ctx *ctx, const tm_request *reqs, int count)
@@ -716,7 +1086,7 @@ int tm_ctx_destroy(tm_ctx *ctx)
         kv.second->inv.release();
         kv.second->flags.release();
     }
-    for (DevBuf *b : {&ctx->raw, &ctx->clean, &ctx->suf, &ctx->tkey, &ctx->bmin_u, &ctx->bmin_l, &ctx->list, &ctx->counters, &ctx->cand, &ctx->dist})
+    for (DevBuf *b : {&ctx->prefix, &ctx->run, &ctx->raw, &ctx->clean, &ctx->suf, &ctx->tkey, &ctx->bmin_u, &ctx->bmin_l, &ctx->list, &ctx->counters, &ctx->cand, &ctx->dist})
         b->release();
     for (HostBuf *b : {&ctx->h_split, &ctx->h_q, &ctx->h_order, &ctx->h_slots, &ctx->h_cand, &ctx->h_dist,
                        &ctx->h_counters, &ctx->h_tkey})

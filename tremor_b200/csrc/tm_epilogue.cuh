@@ -29,6 +29,13 @@ struct ScanArgs
     int *err;              // set (non-zero) by a kernel that gave up waiting
     float *dbg_d;          // diagnostics (tm_bound_diagnostics): every d and its bound e,
     float *dbg_e;          //   [T][W]; null in searches
+    // templates of several lengths in one tile (statistics from prefix sums, tm_prefix.cu)
+    const float *raw;      // raw waveform (missing first samples)
+    const double2 *P;      // FP64 prefix sums of the centred waveform, n + 1
+    const uint16_t *run;   // constant-run lengths
+    double center;
+    const int *tile_kb;    // K blocks (64 samples) of each 128-template tile
+    int k_stride;          // row stride of the template arrays
 };
 
 // Distance d of one (template, window) pair from its shifted dot product

@@ -21,6 +21,7 @@ constexpr uint8_t kFlagExact = 8;        // statistics are the reference's two-p
 // Per-template constants of the fused epilogue (one per template in a batch).
 struct TemplParam
 {
+    double inv_m;  // 1 / m (statistics from prefix sums)
     float s1;      // sum of z-normalised template samples
     float c_lin;   // sum q^2 + m
     float thr_ed;  // threshold mode: cc_to_ed(correlation, m); kNN: unused
@@ -33,6 +34,8 @@ struct TemplParam
     int merge;        // merge offset
     int64_t q_offset; // float offset of the template in the packed template array
     int64_t order_offset; // int offset of its block order
+    uint32_t wcount;  // windows of this template in the searched range (mixed-length tiles)
+    float qs;         // |q| sqrt(m)
 };
 
 // A candidate window for exact re-scoring: template slot and window index relative

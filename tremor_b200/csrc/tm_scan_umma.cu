@@ -33,6 +33,7 @@
 #include <cudaTypedefs.h>
 
 #include "tm_epilogue.cuh"
+#include "tm_prefix.cuh"
 
 namespace tmb {
 
@@ -58,6 +59,9 @@ struct Smem
     uint8_t b_lo[STAGES][B_BYTES];
     float win_mean[2][TN];
     float win_inv[2][TN];
+    double2 win_p[2][TN];      // mixed-length tiles: prefix sums at each window start
+    uint16_t win_run[2][TN];   //   constant-run length at each window start
+    uint8_t win_miss[2][TN];   //   first sample missing
     uint64_t full_a[STAGES], full_b[STAGES], empty[STAGES];
     uint64_t acc_full[2], acc_empty[2], win_ready[2], drain;
     uint32_t tmem_base;
@@ -183,6 +187,15 @@ struct UmmaArgs
     int *err;
 };
 
+// Tile shift (the value subtracted from the waveform before the split): the mean of the
+// middle window for single-length launches; for mixed-length tiles the middle sample.
+template <bool MIXED> __device__ __forceinline__ float tile_shift(const ScanArgs &a, uint32_t j0)
+{
+    const uint32_t jm = min(j0 + TN / 2, a.W - 1);
+    return MIXED ? a.x[a.w0 + jm] : a.mean[jm];
+}
+
+template <bool MIXED>
 __global__ void __launch_bounds__(THREADS, 1)
     k_scan_umma(const UmmaArgs ua, const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CUtensorMap map_lo)
 {
@@ -230,7 +243,8 @@ __global__ void __launch_bounds__(THREADS, 1)
             for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x)
             {
                 const int tt = (int)(tile / ua.w_tiles);
-                for (int kb = 0; kb < ua.kblocks; kb++, it++)
+                const int kblocks = MIXED ? a.tile_kb[tt] : ua.kblocks;
+                for (int kb = 0; kb < kblocks; kb++, it++)
                 {
                     const int s = it % STAGES;
                     if (!mbar_wait(&sm.empty[s], ((it / STAGES) & 1) ^ 1, sm, ua.err, 1))
@@ -264,7 +278,8 @@ __global__ void __launch_bounds__(THREADS, 1)
                 }
                 tc_fence_after();
                 const uint32_t d = tmem + (uint32_t)(buf * TN);
-                for (int kb = 0; kb < ua.kblocks; kb++, it++)
+                const int kblocks = MIXED ? a.tile_kb[tile / ua.w_tiles] : ua.kblocks;
+                for (int kb = 0; kb < kblocks; kb++, it++)
                 {
                     const int s = it % STAGES;
                     const uint32_t ph = (it / STAGES) & 1;
@@ -303,9 +318,10 @@ __global__ void __launch_bounds__(THREADS, 1)
         for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x)
         {
             const uint32_t j0 = (uint32_t)(tile % ua.w_tiles) * TN;
-            const float shift = a.mean[min(j0 + TN / 2, a.W - 1)];
+            const float shift = tile_shift<MIXED>(a, j0);
             const float *xw = a.x + a.w0 + j0;
-            for (int kb = 0; kb < ua.kblocks; kb++, it++)
+            const int kblocks = MIXED ? a.tile_kb[tile / ua.w_tiles] : ua.kblocks;
+            for (int kb = 0; kb < kblocks; kb++, it++)
             {
                 const int s = it % STAGES;
                 if (!mbar_wait(&sm.empty[s], ((it / STAGES) & 1) ^ 1, sm, ua.err, 5))
@@ -356,13 +372,23 @@ __global__ void __launch_bounds__(THREADS, 1)
             for (int i = et; i < TN; i += 128)
             {
                 const uint32_t j = j0 + i;
-                sm.win_mean[buf][i] = j < a.W ? a.mean[j] : 0.0f;
-                sm.win_inv[buf][i] = j < a.W ? a.inv[j] : 0.0f;
+                if (MIXED)
+                {
+                    const bool in = j < a.W;
+                    sm.win_p[buf][i] = in ? a.P[a.w0 + j] : make_double2(0.0, 0.0);
+                    sm.win_run[buf][i] = in ? a.run[a.w0 + j] : (uint16_t)65535;
+                    sm.win_miss[buf][i] = in ? (uint8_t)(a.raw[a.w0 + j] == kMissing) : (uint8_t)1;
+                }
+                else
+                {
+                    sm.win_mean[buf][i] = j < a.W ? a.mean[j] : 0.0f;
+                    sm.win_inv[buf][i] = j < a.W ? a.inv[j] : 0.0f;
+                }
             }
             mbar_arrive(&sm.win_ready[buf]);
             if (!mbar_wait(&sm.win_ready[buf], (tc >> 1) & 1, sm, ua.err, 7))
                 goto done;
-            const float shift = a.mean[min(j0 + TN / 2, a.W - 1)];
+            const float shift = tile_shift<MIXED>(a, j0);
             const int t = tt * TM + row;
             const bool valid = t < a.T;
             TemplParam p;
@@ -383,7 +409,45 @@ __global__ void __launch_bounds__(THREADS, 1)
                 float v[16];
                 tmem_ld16(taddr + c * 16, v);
                 uint32_t mask = 0;
-                if (valid)
+                if (valid && MIXED)
+                {
+#pragma unroll
+                    for (int i = 0; i < 16; i++)
+                    {
+                        const int ci = c * 16 + i;
+                        const uint32_t j = j0 + ci;
+                        if (j >= p.wcount || sm.win_miss[buf][ci] || sm.win_run[buf][ci] >= p.m)
+                            continue; // beyond this template's windows, missing first sample, constant
+                        WindowStats ws;
+                        if (prefix_stats(sm.win_p[buf][ci], a.P[a.w0 + j + p.m], a.w0 + j, p.m, p.inv_m, a.center,
+                                         p.qs, p.s1, ws) != 0)
+                        {
+                            // statistics not trustworthy: the exact re-scoring decides this window
+                            if (p.mode == 1)
+                                lmin = -inf_f();
+                            else
+                                mask |= 1u << i;
+                            continue;
+                        }
+                        float dd, e;
+                        fast_distance_mixed(p, p.a1_main, v[i], ws.mu, ws.iv, shift, ws.estat, dd, e);
+                        if (a.dbg_d != nullptr)
+                        {
+                            const size_t at = (size_t)t * a.W + j;
+                            a.dbg_d[at] = dd;
+                            a.dbg_e[at] = e;
+                        }
+                        const float lo = dd - e;
+                        if (p.mode == 1)
+                        {
+                            umin = fminf(umin, dd + e);
+                            lmin = fminf(lmin, lo);
+                        }
+                        else if (lo <= p.thr_ed)
+                            mask |= 1u << i;
+                    }
+                }
+                else if (valid)
                 {
 #pragma unroll
                     for (int i = 0; i < 16; i++)
@@ -413,7 +477,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             }
             tc_fence_before();
             mbar_arrive(&sm.acc_empty[buf]);
-            if (valid && p.mode == 1 && umin <= kFltMax)
+            if (valid && p.mode == 1 && (umin <= kFltMax || lmin == -inf_f()))
             {
                 const size_t at = (size_t)t * a.nb + j0 / kBucket;
                 atomicMin(&a.bmin_u[at], float_key(umin));
@@ -485,8 +549,12 @@ cudaError_t launch_scan_umma(const ScanArgs &a, cudaStream_t s)
     using namespace umma;
     if (a.q_hi == nullptr || a.q_lo == nullptr || a.err == nullptr)
         return cudaErrorInvalidValue;
+    const bool mixed = a.tile_kb != nullptr;
+    if (mixed && (a.P == nullptr || a.run == nullptr || a.raw == nullptr))
+        return cudaErrorInvalidValue;
+    const int stride = mixed ? a.k_stride : a.m_pad;
     CUtensorMap mh, ml;
-    if (!make_map(&mh, a.q_hi, a.t_rows, a.m_pad) || !make_map(&ml, a.q_lo, a.t_rows, a.m_pad))
+    if (!make_map(&mh, a.q_hi, a.t_rows, stride) || !make_map(&ml, a.q_lo, a.t_rows, stride))
         return cudaErrorInvalidValue;
     UmmaArgs ua;
     ua.a = a;
@@ -498,7 +566,9 @@ cudaError_t launch_scan_umma(const ScanArgs &a, cudaStream_t s)
     static bool attr = false;
     if (!attr)
     {
-        cudaError_t e = cudaFuncSetAttribute(k_scan_umma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = cudaFuncSetAttribute(k_scan_umma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_scan_umma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess)
             return e;
         attr = true;
@@ -508,7 +578,10 @@ cudaError_t launch_scan_umma(const ScanArgs &a, cudaStream_t s)
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const long long tiles = (long long)ua.t_tiles * ua.w_tiles;
     const int grid = (int)std::min<long long>(tiles, sms);
-    k_scan_umma<<<grid, THREADS, smem, s>>>(ua, mh, ml);
+    if (mixed)
+        k_scan_umma<true><<<grid, THREADS, smem, s>>>(ua, mh, ml);
+    else
+        k_scan_umma<false><<<grid, THREADS, smem, s>>>(ua, mh, ml);
     return cudaGetLastError();
 }
 

@@ -18,6 +18,7 @@
 #include "tm_epilogue.cuh"
 #include "tm_exact.cuh"
 #include "tm_internal.cuh"
+#include "tm_prefix.cuh"
 
 namespace tmb {
 
@@ -193,6 +194,82 @@ __global__ void __launch_bounds__(B_THREADS) k_passb(const uint2 *__restrict__ l
     emit_candidates(mask, lane, t, j0, cand, cand_count, cand_cap);
 }
 
+// k_passb for tiles of several template lengths: statistics from the prefix sums, and
+// windows whose statistics are not trustworthy are always emitted (re-scored exactly).
+__global__ void __launch_bounds__(B_THREADS) k_passb_mixed(const uint2 *__restrict__ list, const float *__restrict__ x,
+                                                           const float *__restrict__ raw, const double2 *__restrict__ P,
+                                                           const uint16_t *__restrict__ run, double center,
+                                                           const float *__restrict__ q,
+                                                           const TemplParam *__restrict__ tp,
+                                                           const uint32_t *__restrict__ tkey, uint64_t w0,
+                                                           Candidate *cand, uint32_t *cand_count, uint32_t cand_cap)
+{
+    __shared__ __align__(16) float xs[kBucket + B_KC + 16];
+    __shared__ __align__(16) float qs[B_KC];
+    const uint2 item = list[blockIdx.x];
+    const uint32_t t = item.x;
+    const TemplParam p = tp[t];
+    const uint32_t tk = tkey[t];
+    const float T = tk == kEmptyKey ? inf_f() : key_float(tk);
+    const uint32_t jb = item.y * kBucket;
+    const float shift = x[w0 + min(jb + kBucket / 2, p.wcount - 1)];
+    const float *xg = x + w0 + jb;
+    const float *qg = q + p.q_offset;
+    const int m_pad = (p.m + 63) & ~63;
+    const int tid = threadIdx.x, lane = tid & 31;
+    float acc[8];
+#pragma unroll
+    for (int w = 0; w < 8; w++)
+        acc[w] = 0.0f;
+    for (int k0 = 0; k0 < m_pad; k0 += B_KC)
+    {
+        const int kc = min(B_KC, m_pad - k0);
+        for (int i = tid; i < kBucket + kc; i += B_THREADS)
+            xs[i] = xg[k0 + i] - shift;
+        for (int i = tid; i < kc; i += B_THREADS)
+            qs[i] = qg[k0 + i];
+        __syncthreads();
+        const float *xw = xs + 8 * tid;
+        for (int kk = 0; kk < kc; kk += 4)
+        {
+            const float4 xa = *reinterpret_cast<const float4 *>(xw + kk);
+            const float4 xb = *reinterpret_cast<const float4 *>(xw + kk + 4);
+            const float4 xc = *reinterpret_cast<const float4 *>(xw + kk + 8);
+            const float4 qv = *reinterpret_cast<const float4 *>(qs + kk);
+            const float xr[12] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y, xb.z, xb.w, xc.x, xc.y, xc.z, xc.w};
+#pragma unroll
+            for (int w = 0; w < 8; w++)
+            {
+                acc[w] = fmaf(xr[w + 0], qv.x, acc[w]);
+                acc[w] = fmaf(xr[w + 1], qv.y, acc[w]);
+                acc[w] = fmaf(xr[w + 2], qv.z, acc[w]);
+                acc[w] = fmaf(xr[w + 3], qv.w, acc[w]);
+            }
+        }
+        __syncthreads();
+    }
+    const uint32_t j0 = jb + 8 * tid;
+    uint32_t mask = 0;
+#pragma unroll
+    for (int w = 0; w < 8; w++)
+    {
+        const uint32_t j = j0 + w;
+        if (j >= p.wcount || raw[w0 + j] == kMissing || run[w0 + j] >= p.m)
+            continue;
+        WindowStats ws;
+        if (prefix_stats(P[w0 + j], P[w0 + j + p.m], w0 + j, p.m, p.inv_m, center, p.qs, p.s1, ws) != 0)
+        {
+            mask |= 1u << w;
+            continue;
+        }
+        float d, e;
+        fast_distance_mixed(p, p.a1_fp32, acc[w], ws.mu, ws.iv, shift, ws.estat, d, e);
+        if (d - e <= T)
+            mask |= 1u << w;
+    }
+    emit_candidates(mask, lane, t, j0, cand, cand_count, cand_cap);
+}
+
 // Exact (reference-arithmetic) distance of every candidate.
 __global__ void k_rescore(const Candidate *__restrict__ cand, uint32_t count, const TemplParam *__restrict__ tp,
                           const float *__restrict__ q, const int *__restrict__ order, const float *__restrict__ raw,
@@ -233,6 +310,17 @@ cudaError_t launch_passb(const uint2 *list, uint32_t items, const float *x, cons
 {
     if (items > 0)
         k_passb<<<items, B_THREADS, 0, s>>>(list, x, q, tp, mean, inv, tkey, w0, W, cand, cand_count, cand_cap);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_passb_mixed(const uint2 *list, uint32_t items, const float *x, const float *raw, const double2 *P,
+                               const uint16_t *run, double center, const float *q, const TemplParam *tp,
+                               const uint32_t *tkey, uint64_t w0, Candidate *cand, uint32_t *cand_count,
+                               uint32_t cand_cap, cudaStream_t s)
+{
+    if (items > 0)
+        k_passb_mixed<<<items, B_THREADS, 0, s>>>(list, x, raw, P, run, center, q, tp, tkey, w0, cand, cand_count,
+                                                  cand_cap);
     return cudaGetLastError();
 }
 

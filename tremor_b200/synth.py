@@ -89,3 +89,22 @@ def workload(n: int, q: int, m: int, events: int, seed: int, center_freq: bool =
     x = ar2_waveform(n, rng)
     offsets = inject_events(x, templates, events, rng)
     return x, templates, offsets
+
+
+def mixed_workload(n: int, q: int, m_lo: int, m_hi: int, events: int, seed: int):
+    """(waveform, list of templates with lengths log-uniform in [m_lo, m_hi] rounded to
+    multiples of 16, event offsets): the batching workload."""
+    rng = np.random.default_rng(seed)
+    lengths = np.exp(rng.uniform(np.log(m_lo), np.log(m_hi), size=q))
+    lengths = np.clip((np.round(lengths / 16) * 16).astype(int), m_lo, m_hi)
+    templates = [chirp_templates(1, int(m), rng, center_freq=True)[0] for m in lengths]
+    x = ar2_waveform(n, rng)
+    noise = float(np.std(x[: min(n, 1 << 20)]))
+    offsets = np.sort(rng.integers(0, n - m_hi, size=events))
+    for e, off in enumerate(offsets):
+        tpl = templates[e % q].astype(np.float64)
+        tpl = tpl / (np.sqrt(np.mean(tpl * tpl)) + 1e-30)
+        snr = rng.uniform(0.5, 3.0)
+        local = np.std(x[off:off + len(tpl)]) or noise
+        x[off:off + len(tpl)] += (snr * local * tpl).astype(np.float32)
+    return x, templates, offsets
