@@ -114,3 +114,26 @@ def test_constant_stretch_does_not_flood_candidates():
     with tb.Context(x) as ctx:
         ctx.scan_batch(reqs)
         assert ctx.last_candidates() < 5000
+
+
+def test_mixed_lengths_last_windows():
+    """A template planted in the last window of the waveform (or a few samples before it)
+    is found with its exact distance while templates of other lengths share its tiles
+    (the window-end prefix sums at the end of the record)."""
+    rng = np.random.default_rng(13)
+    n = 50000
+    lengths = [100, 333, 64, 1000]
+    temps = [rng.normal(size=m).astype(np.float32) for m in lengths]
+    for k, m in enumerate(lengths):
+        x = rng.normal(size=n).astype(np.float32)
+        end = n - 7 * k  # the last window, or a few before it
+        x[end - m:end] = temps[k] * np.float32(2.0) + np.float32(1.0)
+        reqs = []
+        for t in temps:
+            reqs.append(tb.Request(t, tb.MODE_KNN, k=1))
+            reqs.append(tb.Request(t, tb.MODE_THRESHOLD, correlation=0.99))
+        with tb.Context(x) as ctx:
+            answers = ctx.scan_batch(reqs)
+        assert int(answers[2 * k][0][0]) == end - m
+        assert end - m in set(int(p) for p in answers[2 * k + 1][0])
+        _check(x, reqs, answers)

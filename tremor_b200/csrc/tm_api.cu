@@ -308,11 +308,11 @@ struct GroupPlan
     bool mixed = false;
     int k_stride = 0;            // row stride of the template arrays
     uint32_t w_max = 0;          // windows of the shortest template
-    std::vector<int> tile_kb;    // K blocks of 64 samples per tile
-    DevBuf d_tile_kb;
+    std::vector<tmb::TileInfo> tiles; // per 128-row tile: K blocks, distinct lengths
+    DevBuf d_tiles;
     void release()
     {
-        d_tile_kb.release();
+        d_tiles.release();
         q_hi.release();
         q_lo.release();
         q.release();
@@ -446,7 +446,10 @@ void ensure_prefix(tm_ctx *ctx)
     cudaStream_t s = ctx->stream;
     const uint64_t n = ctx->n;
     const uint64_t chunks = (n + 8191) / 8192;
-    ctx->prefix.reserve(sizeof(double2) * (n + 1));
+    // zero tail: the contraction kernels read window-end sums in fixed-size chunks that may
+    // run past n (values there belong to no window and are never used)
+    ctx->prefix.reserve(sizeof(double2) * (n + 1 + tmb::kStagePad));
+    TM_CUDA(cudaMemsetAsync(ctx->prefix.p, 0, sizeof(double2) * (n + 1 + tmb::kStagePad), s));
     ctx->run.reserve(sizeof(uint16_t) * n);
     DevBuf totals, run_tmp;
     totals.reserve(sizeof(double2) * chunks);
@@ -467,52 +470,104 @@ void ensure_prefix(tm_ctx *ctx)
     ctx->prefix_ready = true;
 }
 
-// Host preparation of a mixed-length group: templates sorted by length (longest first),
-// 128-row tiles whose K extent is their longest template (shorter rows zero-padded, which
-// leaves their dot products unchanged), window statistics from the prefix sums.
+// Host preparation of a mixed-length group: templates sorted by length (longest first)
+// fill 128-row tiles, a tile closing early when a new length would be its 65th distinct
+// one (padding rows are inert); a tile's K extent is its longest template (shorter rows
+// are zero-padded, which leaves their dot products unchanged). Rows are the template
+// slots of the group: g.index[row] is the request (-1 for padding rows).
 void prepare_group_mixed(tm_ctx *ctx, const std::vector<int> &idx_in, const tm_request *reqs, GroupPlan &g,
                          uint64_t &h2d)
 {
     std::vector<int> idx = idx_in;
     std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return reqs[a].m > reqs[b].m; });
-    const int T = static_cast<int>(idx.size());
+    // rows: request per row (-1 = padding)
+    std::vector<int> rows;
+    std::vector<tmb::TileInfo> tiles;
+    std::vector<int> didx_of_row;
+    for (size_t i = 0; i < idx.size();)
+    {
+        tmb::TileInfo ti{};
+        const size_t start = rows.size();
+        while (i < idx.size() && rows.size() - start < 128)
+        {
+            const int m = reqs[idx[i]].m;
+            int d = 0;
+            while (d < ti.D && ti.len[d] != m)
+                d++;
+            if (d == ti.D)
+            {
+                if (ti.D == tmb::kTileLens)
+                    break;
+                ti.len[ti.D++] = m;
+            }
+            rows.push_back(idx[i]);
+            didx_of_row.push_back(d);
+            i++;
+        }
+        ti.kb = (ti.len[0] + 63) / 64; // longest length first
+        while (rows.size() - start < 128)
+        {
+            rows.push_back(-1);
+            didx_of_row.push_back(0);
+        }
+        tiles.push_back(ti);
+    }
+    const int R = static_cast<int>(rows.size()); // multiple of 128
     const int m_max = reqs[idx[0]].m;
     g.mixed = true;
     g.m = m_max;
-    g.T = T;
-    g.T_pad = (T + 63) & ~63;
-    g.t_rows = (T + 127) & ~127;
+    g.T = R;
+    g.T_pad = R;
+    g.t_rows = R;
     g.k_stride = (m_max + 63) & ~63;
     g.m_pad = g.k_stride;
     g.nblk = std::max(1, g.k_stride / tm_host::kZnormBlock);
     g.umma_constants = true;
-    g.index = idx;
-    const int rows = g.t_rows, stride = g.k_stride, nblk = g.nblk;
-    const size_t elems = static_cast<size_t>(rows) * stride;
+    g.index = rows;
+    const int stride = g.k_stride, nblk = g.nblk;
+    const size_t elems = static_cast<size_t>(R) * stride;
     ctx->h_q.reserve(sizeof(float) * elems);
-    ctx->h_order.reserve(sizeof(int) * static_cast<size_t>(T) * nblk);
-    ctx->h_slots.reserve(sizeof(int) * T);
+    ctx->h_order.reserve(sizeof(int) * static_cast<size_t>(R) * nblk);
+    ctx->h_slots.reserve(sizeof(int) * R);
     ctx->h_split.reserve(2 * sizeof(uint16_t) * elems);
     float *hq = ctx->h_q.as<float>();
     int *ho = ctx->h_order.as<int>();
     int *hslots = ctx->h_slots.as<int>();
     uint16_t *hh = ctx->h_split.as<uint16_t>(), *hl = hh + elems;
     std::memset(hq, 0, sizeof(float) * elems);
-    std::memset(ho, 0, sizeof(int) * static_cast<size_t>(T) * nblk);
+    std::memset(ho, 0, sizeof(int) * static_cast<size_t>(R) * nblk);
     std::memset(hh, 0, 2 * sizeof(uint16_t) * elems);
-    g.htp.assign(g.T_pad, TemplParam{});
-    g.mode.assign(T, 0);
-    g.k.assign(T, 0);
-    g.merge.assign(T, 0);
-    g.thr.assign(T, 0.0f);
-    g.a1_umma.assign(T, 0.0f);
+    g.htp.assign(R, TemplParam{});
+    g.mode.assign(R, TM_MODE_THRESHOLD);
+    g.k.assign(R, 0);
+    g.merge.assign(R, 0);
+    g.thr.assign(R, -FLT_MAX);
+    g.a1_umma.assign(R, 0.0f);
     g.nk = 0;
     g.w_max = 0;
     const uint64_t w0 = ctx->range_first;
-    for (int t = 0; t < T; t++)
+    auto wcount_of = [&](int m) {
+        const uint64_t total = ctx->n - static_cast<uint64_t>(m) + 1;
+        return static_cast<uint32_t>(w0 >= total ? 0 : std::min<uint64_t>(ctx->range_count, total - w0));
+    };
+    uint64_t samples = 0;
+    for (int t = 0; t < R; t++)
     {
-        const tm_request *r = &reqs[idx[t]];
+        TemplParam &p = g.htp[t];
+        const tmb::TileInfo &ti = tiles[t / 128];
+        p.didx = didx_of_row[t];
+        if (rows[t] < 0)
+        {
+            p.mode = TM_MODE_THRESHOLD;
+            p.thr_ed = -FLT_MAX;
+            p.m = ti.len[0];
+            p.inv_m = 1.0 / p.m;
+            p.wcount = 0;
+            continue;
+        }
+        const tm_request *r = &reqs[rows[t]];
         const int m = r->m;
+        samples += static_cast<uint64_t>(m);
         float *q = hq + static_cast<size_t>(t) * stride;
         std::memcpy(q, r->templ, sizeof(float) * m);
         if (!(r->flags & TM_FLAG_ZNORMALIZED))
@@ -527,13 +582,11 @@ void prepare_group_mixed(tm_ctx *ctx, const std::vector<int> &idx_in, const tm_r
             hh[at] = bf16_bits(q[i]);
             hl[at] = bf16_bits(q[i] - bf16_value(hh[at]));
         }
-        TemplParam &p = g.htp[t];
         fill_param(p, m, q2, s1, gamma_bf16(m), gamma_fp32(m));
         g.a1_umma[t] = p.a1_main;
         p.inv_m = 1.0 / static_cast<double>(m);
         p.qs = static_cast<float>(std::sqrt(q2 * m));
-        const uint64_t total = ctx->n - static_cast<uint64_t>(m) + 1;
-        p.wcount = static_cast<uint32_t>(w0 >= total ? 0 : std::min<uint64_t>(ctx->range_count, total - w0));
+        p.wcount = wcount_of(m);
         g.w_max = std::max(g.w_max, p.wcount);
         p.mode = g.mode[t] = r->mode;
         p.k = g.k[t] = r->k;
@@ -545,38 +598,33 @@ void prepare_group_mixed(tm_ctx *ctx, const std::vector<int> &idx_in, const tm_r
         else
             p.thr_ed = g.thr[t] = tm_host::cc_to_ed(r->correlation, m);
     }
-    for (int t = T; t < g.T_pad; t++)
-    {
-        g.htp[t].mode = TM_MODE_THRESHOLD;
-        g.htp[t].thr_ed = -FLT_MAX;
-        g.htp[t].m = m_max;
-    }
-    g.tile_kb.assign(rows / 128, 0);
-    for (int tt = 0; tt < rows / 128; tt++)
-        g.tile_kb[tt] = (reqs[idx[tt * 128]].m + 63) / 64; // longest template of the tile
+    for (tmb::TileInfo &ti : tiles)
+        for (int d = 0; d < ti.D; d++)
+        {
+            ti.wc[d] = wcount_of(ti.len[d]);
+            ti.inv_m[d] = 1.0 / static_cast<double>(ti.len[d]);
+        }
+    g.tiles = tiles;
     cudaStream_t s = ctx->stream;
     g.q.reserve(sizeof(float) * elems);
-    g.order.reserve(sizeof(int) * static_cast<size_t>(T) * nblk);
-    g.tp.reserve(sizeof(TemplParam) * g.T_pad);
+    g.order.reserve(sizeof(int) * static_cast<size_t>(R) * nblk);
+    g.tp.reserve(sizeof(TemplParam) * R);
     g.slots.reserve(sizeof(int) * std::max(g.nk, 1));
     g.q_hi.reserve(sizeof(uint16_t) * elems);
     g.q_lo.reserve(sizeof(uint16_t) * elems);
-    g.d_tile_kb.reserve(sizeof(int) * g.tile_kb.size());
+    g.d_tiles.reserve(sizeof(tmb::TileInfo) * tiles.size());
     TM_CUDA(cudaMemcpyAsync(g.q.p, hq, sizeof(float) * elems, cudaMemcpyHostToDevice, s));
-    TM_CUDA(cudaMemcpyAsync(g.order.p, ho, sizeof(int) * static_cast<size_t>(T) * nblk, cudaMemcpyHostToDevice, s));
-    TM_CUDA(cudaMemcpyAsync(g.tp.p, g.htp.data(), sizeof(TemplParam) * g.T_pad, cudaMemcpyHostToDevice, s));
+    TM_CUDA(cudaMemcpyAsync(g.order.p, ho, sizeof(int) * static_cast<size_t>(R) * nblk, cudaMemcpyHostToDevice, s));
+    TM_CUDA(cudaMemcpyAsync(g.tp.p, g.htp.data(), sizeof(TemplParam) * R, cudaMemcpyHostToDevice, s));
     if (g.nk > 0)
         TM_CUDA(cudaMemcpyAsync(g.slots.p, hslots, sizeof(int) * g.nk, cudaMemcpyHostToDevice, s));
     TM_CUDA(cudaMemcpyAsync(g.q_hi.p, hh, sizeof(uint16_t) * elems, cudaMemcpyHostToDevice, s));
     TM_CUDA(cudaMemcpyAsync(g.q_lo.p, hl, sizeof(uint16_t) * elems, cudaMemcpyHostToDevice, s));
-    TM_CUDA(cudaMemcpyAsync(g.d_tile_kb.p, g.tile_kb.data(), sizeof(int) * g.tile_kb.size(), cudaMemcpyHostToDevice,
+    TM_CUDA(cudaMemcpyAsync(g.d_tiles.p, g.tiles.data(), sizeof(tmb::TileInfo) * tiles.size(), cudaMemcpyHostToDevice,
                             s));
     TM_CUDA(cudaStreamSynchronize(s));
-    uint64_t samples = 0;
-    for (int t = 0; t < T; t++)
-        samples += static_cast<uint64_t>(reqs[idx[t]].m);
-    h2d += samples * (sizeof(float) + 2 * sizeof(uint16_t)) + sizeof(int) * static_cast<uint64_t>(T) * nblk +
-           sizeof(TemplParam) * g.T_pad;
+    h2d += samples * (sizeof(float) + 2 * sizeof(uint16_t)) + sizeof(int) * static_cast<uint64_t>(R) * nblk +
+           sizeof(TemplParam) * R + sizeof(tmb::TileInfo) * tiles.size();
 }
 
 // Canonical answers from the exactly re-scored candidates of each template of a group.
@@ -591,6 +639,8 @@ void finish_answers(tm_ctx *ctx, const GroupPlan &g, std::vector<std::vector<Hit
     const uint32_t *tkey = ctx->h_tkey.as<uint32_t>();
     for (int t = 0; t < g.T; t++)
     {
+        if (g.index[t] < 0)
+            continue; // padding row of a mixed-length tile
         std::vector<Hit> &out = answers[g.index[t]];
         out.clear();
         if (g.mode[t] == TM_MODE_KNN)
@@ -809,9 +859,10 @@ void execute_group_mixed(tm_ctx *ctx, GroupPlan &g, std::vector<std::vector<Hit>
     if (W == 0)
     {
         for (int t = 0; t < T; t++)
-            answers[g.index[t]] = g.mode[t] == TM_MODE_KNN
-                                      ? std::vector<Hit>(static_cast<size_t>(g.k[t]), Hit{0, FLT_MAX})
-                                      : std::vector<Hit>();
+            if (g.index[t] >= 0)
+                answers[g.index[t]] = g.mode[t] == TM_MODE_KNN
+                                          ? std::vector<Hit>(static_cast<size_t>(g.k[t]), Hit{0, FLT_MAX})
+                                          : std::vector<Hit>();
         return;
     }
     if (W >= (1ull << 32))
@@ -865,8 +916,9 @@ void execute_group_mixed(tm_ctx *ctx, GroupPlan &g, std::vector<std::vector<Hit>
         a.P = ctx->prefix.as<double2>();
         a.run = ctx->run.as<uint16_t>();
         a.center = ctx->center;
-        a.tile_kb = g.d_tile_kb.as<int>();
+        a.tiles = g.d_tiles.as<tmb::TileInfo>();
         a.k_stride = g.k_stride;
+        a.n = ctx->n;
         if (ctx->profile)
             TM_CUDA(cudaEventRecord(ctx->ev0, s));
         TM_CUDA(tmb::launch_scan_umma(a, s));

@@ -34,8 +34,9 @@ struct ScanArgs
     const double2 *P;      // FP64 prefix sums of the centred waveform, n + 1
     const uint16_t *run;   // constant-run lengths
     double center;
-    const int *tile_kb;    // K blocks (64 samples) of each 128-template tile
+    const TileInfo *tiles; // per 128-row tile: K blocks and distinct lengths
     int k_stride;          // row stride of the template arrays
+    uint64_t n;            // samples of the waveform (P has n + 1 entries)
 };
 
 // Distance d of one (template, window) pair from its shifted dot product
@@ -93,6 +94,61 @@ __device__ __forceinline__ void emit_candidates(uint32_t mask, int lane, uint32_
             cand[pos] = Candidate{t, j0 + (uint32_t)w};
         pos++;
     }
+}
+
+// Per-warp staging of candidates in shared memory: a warp appends to its own buffer and
+// reserves global slots with one atomicAdd per flush instead of one per emission, so many
+// warps emitting at once do not serialise on the global counter. `n` is warp-uniform.
+
+__device__ __forceinline__ void stage_flush(Candidate *sbuf, uint32_t &n, int lane, Candidate *cand, uint32_t *count,
+                                            uint32_t cap)
+{
+    if (n == 0)
+        return;
+    uint32_t base = 0;
+    if (lane == 0)
+        base = atomicAdd(count, n);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    for (uint32_t i = lane; i < n; i += 32)
+        if (base + i < cap)
+            cand[base + i] = sbuf[i];
+    __syncwarp();
+    n = 0;
+}
+
+// emit_candidates through the warp's staging buffer (every lane must call it).
+template <uint32_t kStageCap>
+__device__ __forceinline__ void stage_emit(uint32_t mask, int lane, uint32_t t, uint32_t j0, Candidate *sbuf,
+                                           uint32_t &n, Candidate *cand, uint32_t *count, uint32_t cap)
+{
+    const int c = __popc(mask);
+    int incl = c;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1)
+    {
+        const int v = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off)
+            incl += v;
+    }
+    const uint32_t total = (uint32_t)__shfl_sync(0xffffffffu, incl, 31);
+    if (total == 0)
+        return;
+    if (total > kStageCap)
+    {
+        emit_candidates(mask, lane, t, j0, cand, count, cap); // rare: more than a buffer at once
+        return;
+    }
+    if (n + total > kStageCap)
+        stage_flush(sbuf, n, lane, cand, count, cap);
+    uint32_t pos = n + (uint32_t)(incl - c);
+    while (mask)
+    {
+        const int w = __ffs(mask) - 1;
+        mask &= mask - 1;
+        sbuf[pos++] = Candidate{t, j0 + (uint32_t)w};
+    }
+    __syncwarp();
+    n += total;
 }
 
 } // namespace tmb

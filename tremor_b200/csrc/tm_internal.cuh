@@ -36,6 +36,18 @@ struct TemplParam
     int64_t order_offset; // int offset of its block order
     uint32_t wcount;  // windows of this template in the searched range (mixed-length tiles)
     float qs;         // |q| sqrt(m)
+    int didx;         // mixed-length tiles: index of m in its tile's distinct lengths
+};
+
+// A 128-row tile of a mixed-length group: its distinct template lengths (at most 64).
+constexpr int kTileLens = 64;
+struct TileInfo
+{
+    int kb;                   // K blocks of 64 samples (longest template of the tile)
+    int D;                    // distinct lengths
+    int len[kTileLens];
+    uint32_t wc[kTileLens];   // windows of each length in the searched range
+    double inv_m[kTileLens];  // 1 / length
 };
 
 // A candidate window for exact re-scoring: template slot and window index relative

@@ -14,43 +14,49 @@ constexpr double kEps64 = 1.1102230246251565e-16;
 
 struct WindowStats
 {
-    float mu;    // window mean (float)
-    float iv;    // 1 / std (float)
-    float estat; // bound on the distance error these statistics can cause (added to e)
+    float mu;     // window mean (float)
+    float iv;     // 1 / std (float)
+    float rel_sd; // bound on the relative error of the std
+    float e_mu;   // bound on the absolute error of the mean
 };
 
-// Statistics of window j (global start index) of length m. Returns 0 when the statistics
-// are trustworthy, 2 when cancellation may have destroyed them (the window must then be
-// re-scored exactly, whatever its distance). Pa = P[j], Pb = P[j + m].
-//   var relative error  <= e_var / var   (prefix errors: gamma * sum of |terms| up to each end,
-//                                          |sum (x - c)| <= sqrt(i * sum (x - c)^2))
+// Bound on the distance error that statistics with these error bounds can cause, for a
+// template of length m with |q| sqrt(m) = qs and sum q = s1q (added to e).
+__device__ __forceinline__ float stats_error(const WindowStats &w, int m, float qs, float s1q)
+{
+    return 1.25f * ((4.0f * (float)m + 2.0f * qs) * w.rel_sd + 2.0f * fabsf(s1q) * w.e_mu * w.iv);
+}
+
+// Statistics of window j (global start index) of length m (independent of the template).
+// Returns 0 when the statistics are trustworthy, 2 when cancellation may have destroyed them (the window must then be
+// re-scored exactly, whatever its distance). Pa = P[j] (a2 = (float)Pa.y), Pb = P[j + m].
+//   prefix errors: gamma * (sum of |terms| up to each end); sum (x - c)^2 up to i is P2[i],
+//   and sum |x - c| up to i <= sqrt(i * P2[i]) <= sqrt((j + m) * P2[j + m]) for i <= j + m
+//   var relative error  <= e_var / var
 //   std relative error  <= 0.5 e_var / var + rsqrtf's 2^-22 + float rounding
-//   d error from stats  <= (4m + 2 |q| sqrt(m)) * (std rel. error) + 2 |sum q| * |mean error| / std
-__device__ __forceinline__ int prefix_stats(double2 Pa, double2 Pb, uint64_t j, int m, double inv_m, double center,
-                                            float qs, float s1q, WindowStats &w)
+// The error terms are evaluated in float with margins (they are bounds, not values).
+__device__ __forceinline__ int prefix_stats(double2 Pa, float a2, double2 Pb, uint64_t j, int m, double inv_m,
+                                            float center_f, WindowStats &w)
 {
     const double s1 = Pb.x - Pa.x, s2 = Pb.y - Pa.y;
     const double mu_c = s1 * inv_m;
-    const double var = s2 * inv_m - mu_c * mu_c;
+    const double var = fma(-mu_c, mu_c, s2 * inv_m);
     // var < 1e-22 (std < 1e-11): near the reference's 1e-12 cut, decided by the exact path
     if (!(var > 1e-22) || !(var < 1e36))
         return 2;
-    // error terms in float with a 1.01 margin for their own rounding (they are bounds,
-    // not values: a few ulps do not matter)
-    const float fg = (float)kPrefixGamma * 1.01f, fe = (float)kEps64 * 1.01f, fm = (float)inv_m;
-    const float a2 = (float)Pa.y, b2 = (float)Pb.y, fs2 = (float)s2, fmu = (float)mu_c;
-    const float e_s2 = fg * (a2 + b2) + 4.0f * fe * fs2;
-    const float e_s1 = fg * (sqrtf((float)j * a2) + sqrtf((float)(j + m) * b2)) * 1.001f + 4.0f * fe * fabsf((float)s1);
-    const float e_var = (e_s2 + 2.0f * fabsf(fmu) * e_s1) * fm + 8.0f * fe * fs2 * fm;
-    const float fvar = (float)var;
+    const float fvar = (float)var, fmu = (float)mu_c, fb2 = (float)Pb.y;
+    const float fm = (float)m, fim = 1.0f / fm;
+    const float fg = (float)kPrefixGamma * 1.01f, fe = (float)kEps64 * 1.01f;
+    const float fs2 = fm * (fvar + fmu * fmu) * 1.0001f;
+    const float e_s2 = fg * (a2 + fb2) + 4.0f * fe * fs2;
+    const float e_s1 = 2.002f * fg * sqrtf((float)(j + (uint64_t)m) * fb2) + 4.0f * fe * fm * fabsf(fmu);
+    const float e_var = (e_s2 + 2.0f * fabsf(fmu) * e_s1 + 8.0f * fe * fs2) * fim * 1.0001f;
     if (e_var > 1e-4f * fvar)
         return 2;
-    const double mu = mu_c + center;
-    w.mu = (float)mu;
     w.iv = rsqrtf(fvar);
-    const float rel_sd = 0.5f * e_var / fvar + 6.0e-7f;
-    const float e_mu = e_s1 * fm + 6.0e-8f * fabsf(w.mu) + 4.0f * fe * fabsf(w.mu);
-    w.estat = 1.25f * ((4.0f * (float)m + 2.0f * qs) * rel_sd + 2.0f * fabsf(s1q) * e_mu * w.iv);
+    w.mu = fmu + center_f;
+    w.rel_sd = 0.5f * e_var * w.iv * w.iv * 1.001f + 6.0e-7f;
+    w.e_mu = e_s1 * fim + 1.2e-7f * (fabsf(w.mu) + fabsf(center_f)) + 4.0f * fe * fabsf(w.mu);
     return 0;
 }
 

@@ -42,28 +42,46 @@ namespace umma {
 constexpr int TM = 128;       // templates per tile (MMA M)
 constexpr int TN = 256;       // windows per tile (MMA N)
 constexpr int KB = 64;        // samples per stage (one 128-byte swizzle atom of BF16)
-constexpr int STAGES = 4;
 constexpr int STRIP_CHUNKS = TN / 8 + KB / 8; // 40 core matrices of 128 bytes
 constexpr int A_BYTES = TM * KB * 2;          // 16 KiB per half
 constexpr int B_BYTES = STRIP_CHUNKS * 128;   // 5 KiB per half
-constexpr int THREADS = 256;
+constexpr int THREADS = 384;  // 4 role warps + 8 epilogue warps
 constexpr int BUILDERS = 64;
+constexpr int EPI = 256;      // epilogue threads
+constexpr int CH = 16;        // mixed tiles: windows per statistics chunk
+constexpr int NCH = TN / CH;
 constexpr uint32_t TMEM_COLS = 2 * TN;
 constexpr long long TIMEOUT_CYCLES = 4000000000ll; // ~2 s at 2 GHz
 
-struct Smem
+// Shared memory. Mixed-length tiles trade one operand stage for the statistics pipeline:
+// window-end prefix sums of each distinct length (a 3-slot ring of 16-window chunks,
+// filled by bulk copies two chunks ahead) and the per-(window, length) statistics
+// (double-buffered by chunk).
+template <bool MIXED> struct SmemT
 {
-    uint8_t a_hi[STAGES][A_BYTES]; // 1024-byte aligned (swizzle atoms)
-    uint8_t a_lo[STAGES][A_BYTES];
-    uint8_t b_hi[STAGES][B_BYTES];
-    uint8_t b_lo[STAGES][B_BYTES];
-    float win_mean[2][TN];
-    float win_inv[2][TN];
-    double2 win_p[2][TN];      // mixed-length tiles: prefix sums at each window start
-    uint16_t win_run[2][TN];   //   constant-run length at each window start
-    uint8_t win_miss[2][TN];   //   first sample missing
-    uint64_t full_a[STAGES], full_b[STAGES], empty[STAGES];
-    uint64_t acc_full[2], acc_empty[2], win_ready[2], drain;
+    static constexpr int S = MIXED ? 3 : 4;    // operand stages
+    static constexpr int R = MIXED ? 3 : 1;    // ring slots of window-end prefix sums
+    static constexpr int W2 = MIXED ? 1 : 2;   // single-length window statistics buffers
+    static constexpr int M2 = MIXED ? 2 : 1;   // mixed-length per-tile buffers
+    static constexpr uint32_t STAGE = MIXED ? 64 : 256; // staged candidates per epilogue warp
+    uint8_t a_hi[S][A_BYTES]; // 1024-byte aligned (swizzle atoms)
+    uint8_t a_lo[S][A_BYTES];
+    uint8_t b_hi[S][B_BYTES];
+    uint8_t b_lo[S][B_BYTES];
+    double2 pend[R][MIXED ? kTileLens : 1][CH];  // P[j + len_d] per distinct length d
+    float4 st[M2][CH][MIXED ? kTileLens : 1];    // (mean, 1/std or 0 / -1, rel. std error, mean error)
+    double2 win_p[M2][TN];                       // mixed: prefix sums at each window start
+    float win_a2[M2][TN];                        //   their sums of squares as float
+    uint16_t win_run[M2][TN];                    //   constant-run length at each window start
+    uint8_t win_miss[M2][TN];                    //   first sample missing
+    int lens[M2][kTileLens];                     //   distinct lengths of the tile
+    uint32_t lwc[M2][kTileLens];                 //   their window counts
+    double linv[M2][kTileLens];                  //   their inverses
+    float win_mean[W2][TN];                      // single-length tiles: window statistics
+    float win_inv[W2][TN];
+    Candidate stage[8][STAGE];                   // per epilogue warp: candidates before their flush
+    uint64_t full_a[S], full_b[S], empty[S];
+    uint64_t acc_full[2], acc_empty[2], win_ready[2], drain, pend_bar[R], st_ready[2];
     uint32_t tmem_base;
     int abort;
 };
@@ -94,7 +112,7 @@ __device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity)
     return ok != 0;
 }
 // Bounded wait: false on timeout or when another role aborted (the CTA then unwinds).
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, Smem &sm, int *err, int where)
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int &abort_flag, int *err, int where)
 {
     if (mbar_try(bar, parity))
         return true;
@@ -103,15 +121,22 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, Smem &
     {
         if (mbar_try(bar, parity))
             return true;
-        if (*(volatile int *)&sm.abort)
+        if (*(volatile int *)&abort_flag)
             return false;
         if (clock64() - t0 > TIMEOUT_CYCLES)
         {
-            *(volatile int *)&sm.abort = 1;
+            *(volatile int *)&abort_flag = 1;
             atomicExch(err, 1000 + where);
             return false;
         }
     }
+}
+
+// mbar_wait agreed by the whole warp: every lane continues only if all lanes succeeded, so a
+// warp-collective instruction after the wait is never reached by part of a warp.
+__device__ __forceinline__ bool mbar_wait_warp(uint64_t *bar, uint32_t parity, int &abort_flag, int *err, int where)
+{
+    return __all_sync(0xffffffffu, mbar_wait(bar, parity, abort_flag, err, where));
 }
 
 // Short bounded wait used while unwinding after an abort (ignores the abort flag).
@@ -174,11 +199,35 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v)
         v[i] = __uint_as_float(r[i]);
 }
 
+// 1-D bulk copy global -> shared (16-byte aligned addresses, size a multiple of 16).
+__device__ __forceinline__ void bulk_copy(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     saddr(dst)),
+                 "l"(src), "r"(bytes), "r"(saddr(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float *v)
+{
+    uint32_t r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+        v[i] = __uint_as_float(r[i]);
+}
+
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b)
 {
     const __nv_bfloat162 h = __floats2bfloat162_rn(a, b); // .x = a (low half), .y = b
     return *reinterpret_cast<const uint32_t *>(&h);
 }
+
+static_assert(sizeof(SmemT<false>) + 1024 <= 227 * 1024, "shared memory of k_scan_umma");
+static_assert(sizeof(SmemT<true>) + 1024 <= 227 * 1024, "shared memory of k_scan_umma (mixed)");
 
 struct UmmaArgs
 {
@@ -200,7 +249,9 @@ __global__ void __launch_bounds__(THREADS, 1)
     k_scan_umma(const UmmaArgs ua, const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CUtensorMap map_lo)
 {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    Smem &sm = *reinterpret_cast<Smem *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    using Sm = SmemT<MIXED>;
+    constexpr int STAGES = Sm::S;
+    Sm &sm = *reinterpret_cast<Sm *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const ScanArgs &a = ua.a;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const long long tiles = (long long)ua.t_tiles * ua.w_tiles;
@@ -216,10 +267,13 @@ __global__ void __launch_bounds__(THREADS, 1)
         for (int b = 0; b < 2; b++)
         {
             mbar_init(&sm.acc_full[b], 1);
-            mbar_init(&sm.acc_empty[b], 128);
-            mbar_init(&sm.win_ready[b], 128);
+            mbar_init(&sm.acc_empty[b], EPI);
+            mbar_init(&sm.win_ready[b], EPI);
+            mbar_init(&sm.st_ready[b], EPI);
         }
         mbar_init(&sm.drain, 1);
+        for (int r = 0; r < Sm::R; r++)
+            mbar_init(&sm.pend_bar[r], EPI);
         sm.abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -243,11 +297,11 @@ __global__ void __launch_bounds__(THREADS, 1)
             for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x)
             {
                 const int tt = (int)(tile / ua.w_tiles);
-                const int kblocks = MIXED ? a.tile_kb[tt] : ua.kblocks;
+                const int kblocks = MIXED ? a.tiles[tt].kb : ua.kblocks;
                 for (int kb = 0; kb < kblocks; kb++, it++)
                 {
                     const int s = it % STAGES;
-                    if (!mbar_wait(&sm.empty[s], ((it / STAGES) & 1) ^ 1, sm, ua.err, 1))
+                    if (!mbar_wait(&sm.empty[s], ((it / STAGES) & 1) ^ 1, sm.abort, ua.err, 1))
                     {
                         // unwinding: let the copies already issued land before the CTA exits
                         for (uint32_t i = it > STAGES ? it - STAGES : 0; i < it; i++)
@@ -270,7 +324,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x, tc++)
             {
                 const int buf = tc & 1;
-                if (!mbar_wait(&sm.acc_empty[buf], ((tc >> 1) & 1) ^ 1, sm, ua.err, 2))
+                if (!mbar_wait(&sm.acc_empty[buf], ((tc >> 1) & 1) ^ 1, sm.abort, ua.err, 2))
                 {
                     mma_commit(&sm.drain);
                     mbar_drain(&sm.drain, 0);
@@ -278,12 +332,12 @@ __global__ void __launch_bounds__(THREADS, 1)
                 }
                 tc_fence_after();
                 const uint32_t d = tmem + (uint32_t)(buf * TN);
-                const int kblocks = MIXED ? a.tile_kb[tile / ua.w_tiles] : ua.kblocks;
+                const int kblocks = MIXED ? a.tiles[tile / ua.w_tiles].kb : ua.kblocks;
                 for (int kb = 0; kb < kblocks; kb++, it++)
                 {
                     const int s = it % STAGES;
                     const uint32_t ph = (it / STAGES) & 1;
-                    if (!mbar_wait(&sm.full_a[s], ph, sm, ua.err, 3) || !mbar_wait(&sm.full_b[s], ph, sm, ua.err, 4))
+                    if (!mbar_wait(&sm.full_a[s], ph, sm.abort, ua.err, 3) || !mbar_wait(&sm.full_b[s], ph, sm.abort, ua.err, 4))
                     {
                         // unwinding: wait for the MMAs already issued before TMEM is released
                         mma_commit(&sm.drain);
@@ -320,11 +374,11 @@ __global__ void __launch_bounds__(THREADS, 1)
             const uint32_t j0 = (uint32_t)(tile % ua.w_tiles) * TN;
             const float shift = tile_shift<MIXED>(a, j0);
             const float *xw = a.x + a.w0 + j0;
-            const int kblocks = MIXED ? a.tile_kb[tile / ua.w_tiles] : ua.kblocks;
+            const int kblocks = MIXED ? a.tiles[tile / ua.w_tiles].kb : ua.kblocks;
             for (int kb = 0; kb < kblocks; kb++, it++)
             {
                 const int s = it % STAGES;
-                if (!mbar_wait(&sm.empty[s], ((it / STAGES) & 1) ^ 1, sm, ua.err, 5))
+                if (!mbar_wait(&sm.empty[s], ((it / STAGES) & 1) ^ 1, sm.abort, ua.err, 5))
                     goto done;
                 const float *xs = xw + kb * KB;
                 for (int row = tid; row < STRIP_CHUNKS * 8; row += BUILDERS)
@@ -359,124 +413,213 @@ __global__ void __launch_bounds__(THREADS, 1)
     }
     else
     {
-        // ---- epilogue: TMEM -> distances, bounds, candidates / bucket minima ----
+        // ---- epilogue (8 warps): TMEM -> distances, bounds, candidates / bucket minima ----
+        // Warps w and w + 4 read the same TMEM lane quarter (warp % 4) and split the columns.
         const int quarter = warp & 3;
-        const int row = quarter * 32 + lane; // TMEM lane = template within the tile
-        const int et = threadIdx.x - 128;    // 0..127
-        uint32_t tc = 0;
+        const int ew = warp - 4;              // epilogue warp 0..7
+        const int half = ew >> 2;
+        const int row = quarter * 32 + lane;  // TMEM lane = template row within the tile
+        const int et = threadIdx.x - 128;     // 0..255
+        constexpr uint32_t STAGE = Sm::STAGE;
+        uint32_t tc = 0, pend_it = 0, st_it = 0, staged = 0;
         for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x, tc++)
         {
             const int buf = tc & 1;
+            const int mb = MIXED ? buf : 0;
             const int tt = (int)(tile / ua.w_tiles);
             const uint32_t j0 = (uint32_t)(tile % ua.w_tiles) * TN;
-            for (int i = et; i < TN; i += 128)
             {
+                const int i = et; // one window per epilogue thread
                 const uint32_t j = j0 + i;
                 if (MIXED)
                 {
                     const bool in = j < a.W;
-                    sm.win_p[buf][i] = in ? a.P[a.w0 + j] : make_double2(0.0, 0.0);
-                    sm.win_run[buf][i] = in ? a.run[a.w0 + j] : (uint16_t)65535;
-                    sm.win_miss[buf][i] = in ? (uint8_t)(a.raw[a.w0 + j] == kMissing) : (uint8_t)1;
+                    const double2 pv = in ? a.P[a.w0 + j] : make_double2(0.0, 0.0);
+                    sm.win_p[mb][i] = pv;
+                    sm.win_a2[mb][i] = (float)pv.y;
+                    sm.win_run[mb][i] = in ? a.run[a.w0 + j] : (uint16_t)65535;
+                    sm.win_miss[mb][i] = in ? (uint8_t)(a.raw[a.w0 + j] == kMissing) : (uint8_t)1;
+                    if (et < kTileLens)
+                    {
+                        sm.lens[mb][et] = a.tiles[tt].len[et];
+                        sm.lwc[mb][et] = a.tiles[tt].wc[et];
+                        sm.linv[mb][et] = a.tiles[tt].inv_m[et];
+                    }
                 }
                 else
                 {
-                    sm.win_mean[buf][i] = j < a.W ? a.mean[j] : 0.0f;
-                    sm.win_inv[buf][i] = j < a.W ? a.inv[j] : 0.0f;
+                    sm.win_mean[buf & (Sm::W2 - 1)][i] = j < a.W ? a.mean[j] : 0.0f;
+                    sm.win_inv[buf & (Sm::W2 - 1)][i] = j < a.W ? a.inv[j] : 0.0f;
                 }
             }
             mbar_arrive(&sm.win_ready[buf]);
-            if (!mbar_wait(&sm.win_ready[buf], (tc >> 1) & 1, sm, ua.err, 7))
+            if (!mbar_wait_warp(&sm.win_ready[buf], (tc >> 1) & 1, sm.abort, ua.err, 7))
                 goto done;
             const float shift = tile_shift<MIXED>(a, j0);
             const int t = tt * TM + row;
-            const bool valid = t < a.T;
             TemplParam p;
+            bool valid = t < a.T;
             if (valid)
+            {
                 p = a.tp[t];
-            else
+                valid = !MIXED || p.wcount > 0; // padding rows of mixed tiles
+            }
+            if (!valid)
             {
                 p.mode = 0;
                 p.thr_ed = -kFltMax;
+                p.didx = 0;
             }
-            if (!mbar_wait(&sm.acc_full[buf], (tc >> 1) & 1, sm, ua.err, 6))
+            if (!mbar_wait_warp(&sm.acc_full[buf], (tc >> 1) & 1, sm.abort, ua.err, 6))
                 goto done;
             tc_fence_after();
             float umin = inf_f(), lmin = inf_f();
             const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(buf * TN);
-            for (int c = 0; c < TN / 16; c++)
+            if (MIXED)
             {
-                float v[16];
-                tmem_ld16(taddr + c * 16, v);
-                uint32_t mask = 0;
-                if (valid && MIXED)
-                {
-#pragma unroll
-                    for (int i = 0; i < 16; i++)
+                // Phase A per 16-window chunk: statistics of every (window, distinct length)
+                // from the window-start prefix sums and the window-end prefix sums, which
+                // bulk copies (one per length, issued by thread d) bring two chunks ahead.
+                // Phase B: each lane's distances from its length's statistics.
+                const int D = a.tiles[tt].D;
+                constexpr uint32_t RING = Sm::R;
+                const float center_f = (float)a.center;
+                auto issue = [&](int cc, uint32_t k) {
+                    const uint32_t slot = k % RING;
+                    if (et < D)
                     {
-                        const int ci = c * 16 + i;
+                        // within the zero-padded prefix array: j0 + CH*cc < W + 256, len <= 16384
+                        const uint64_t src = a.w0 + j0 + (uint64_t)(CH * cc) + (uint64_t)sm.lens[mb][et];
+                        fence_proxy_async();
+                        mbar_expect_tx(&sm.pend_bar[slot], CH * 16);
+                        bulk_copy(&sm.pend[slot][et][0], a.P + src, CH * 16, &sm.pend_bar[slot]);
+                    }
+                    else
+                        mbar_arrive(&sm.pend_bar[slot]);
+                };
+                for (int cc = 0; cc < (int)RING - 1; cc++)
+                    issue(cc, pend_it + cc);
+                for (int cc = 0; cc < NCH; cc++, pend_it++, st_it++)
+                {
+                    if (cc + (int)RING - 1 < NCH)
+                        issue(cc + RING - 1, pend_it + RING - 1);
+                    if (!mbar_wait_warp(&sm.pend_bar[pend_it % RING], (pend_it / RING) & 1, sm.abort, ua.err, 8))
+                    {
+                        for (uint32_t k = 1; k < RING && cc + (int)k < NCH; k++) // copies in flight land first
+                            mbar_drain(&sm.pend_bar[(pend_it + k) % RING], ((pend_it + k) / RING) & 1);
+                        goto done;
+                    }
+                    const int sb = st_it & 1;
+                    for (int q = et; q < D * CH; q += EPI)
+                    {
+                        const int d = q % D, i = q / D;
+                        const int ci = CH * cc + i;
                         const uint32_t j = j0 + ci;
-                        if (j >= p.wcount || sm.win_miss[buf][ci] || sm.win_run[buf][ci] >= p.m)
-                            continue; // beyond this template's windows, missing first sample, constant
-                        WindowStats ws;
-                        if (prefix_stats(sm.win_p[buf][ci], a.P[a.w0 + j + p.m], a.w0 + j, p.m, p.inv_m, a.center,
-                                         p.qs, p.s1, ws) != 0)
+                        float4 r = make_float4(0.0f, 0.0f, 0.0f, 0.0f); // iv 0: not searched
+                        const int len = sm.lens[mb][d];
+                        if (j < sm.lwc[mb][d] && !sm.win_miss[mb][ci] && sm.win_run[mb][ci] < len)
                         {
-                            // statistics not trustworthy: the exact re-scoring decides this window
-                            if (p.mode == 1)
-                                lmin = -inf_f();
+                            WindowStats ws;
+                            if (prefix_stats(sm.win_p[mb][ci], sm.win_a2[mb][ci], sm.pend[pend_it % RING][d][i],
+                                             a.w0 + j, len, sm.linv[mb][d], center_f, ws) == 0)
+                                r = make_float4(ws.mu, ws.iv, ws.rel_sd, ws.e_mu);
                             else
-                                mask |= 1u << i;
-                            continue;
+                                r.y = -1.0f; // statistics not trustworthy: exact re-scoring decides
                         }
-                        float dd, e;
-                        fast_distance_mixed(p, p.a1_main, v[i], ws.mu, ws.iv, shift, ws.estat, dd, e);
-                        if (a.dbg_d != nullptr)
-                        {
-                            const size_t at = (size_t)t * a.W + j;
-                            a.dbg_d[at] = dd;
-                            a.dbg_e[at] = e;
-                        }
-                        const float lo = dd - e;
-                        if (p.mode == 1)
-                        {
-                            umin = fminf(umin, dd + e);
-                            lmin = fminf(lmin, lo);
-                        }
-                        else if (lo <= p.thr_ed)
-                            mask |= 1u << i;
+                        sm.st[sb][i][d] = r;
                     }
-                }
-                else if (valid)
-                {
-#pragma unroll
-                    for (int i = 0; i < 16; i++)
+                    mbar_arrive(&sm.st_ready[sb]);
+                    if (!mbar_wait_warp(&sm.st_ready[sb], (st_it >> 1) & 1, sm.abort, ua.err, 9))
+                        goto done;
+                    float v[8];
+                    const int c0 = CH * cc + 8 * half; // this warp's 8 columns of the chunk
+                    tmem_ld8(taddr + c0, v);
+                    uint32_t mask = 0;
+                    if (valid)
                     {
-                        const float iv = sm.win_inv[buf][c * 16 + i];
-                        if (iv == 0.0f)
-                            continue;
-                        float dd, e;
-                        fast_distance(p, p.a1_main, v[i], sm.win_mean[buf][c * 16 + i], iv, shift, dd, e);
-                        if (a.dbg_d != nullptr)
+#pragma unroll
+                        for (int i = 0; i < 8; i++)
                         {
-                            const size_t at = (size_t)t * a.W + j0 + c * 16 + i;
-                            a.dbg_d[at] = dd;
-                            a.dbg_e[at] = e;
+                            const float4 r = sm.st[sb][8 * half + i][p.didx];
+                            if (r.y == 0.0f)
+                                continue; // beyond the template's windows, missing first sample, constant
+                            if (r.y < 0.0f)
+                            {
+                                if (p.mode == 1)
+                                    lmin = -inf_f();
+                                else
+                                    mask |= 1u << i;
+                                continue;
+                            }
+                            WindowStats ws;
+                            ws.mu = r.x;
+                            ws.iv = r.y;
+                            ws.rel_sd = r.z;
+                            ws.e_mu = r.w;
+                            float dd, e;
+                            fast_distance_mixed(p, p.a1_main, v[i], ws.mu, ws.iv, shift, stats_error(ws, p.m, p.qs, p.s1),
+                                                dd, e);
+                            if (a.dbg_d != nullptr)
+                            {
+                                const size_t at = (size_t)t * a.W + j0 + c0 + i;
+                                a.dbg_d[at] = dd;
+                                a.dbg_e[at] = e;
+                            }
+                            const float lo = dd - e;
+                            if (p.mode == 1)
+                            {
+                                umin = fminf(umin, dd + e);
+                                lmin = fminf(lmin, lo);
+                            }
+                            else if (lo <= p.thr_ed)
+                                mask |= 1u << i;
                         }
-                        const float lo = dd - e;
-                        if (p.mode == 1)
-                        {
-                            umin = fminf(umin, dd + e);
-                            lmin = fminf(lmin, lo);
-                        }
-                        else if (lo <= p.thr_ed)
-                            mask |= 1u << i;
                     }
+                    stage_emit<STAGE>(mask, lane, (uint32_t)t, j0 + c0, sm.stage[ew], staged, a.cand, a.cand_count,
+                                      a.cand_cap);
                 }
-                emit_candidates(mask, lane, (uint32_t)t, j0 + c * 16, a.cand, a.cand_count, a.cand_cap);
+            }
+            else
+            {
+                const int wb = buf & (Sm::W2 - 1);
+                for (int c = 8 * half; c < 8 * half + 8; c++) // this warp's 128 of the 256 columns
+                {
+                    float v[16];
+                    tmem_ld16(taddr + c * 16, v);
+                    uint32_t mask = 0;
+                    if (valid)
+                    {
+#pragma unroll
+                        for (int i = 0; i < 16; i++)
+                        {
+                            const float iv = sm.win_inv[wb][c * 16 + i];
+                            if (iv == 0.0f)
+                                continue;
+                            float dd, e;
+                            fast_distance(p, p.a1_main, v[i], sm.win_mean[wb][c * 16 + i], iv, shift, dd, e);
+                            if (a.dbg_d != nullptr)
+                            {
+                                const size_t at = (size_t)t * a.W + j0 + c * 16 + i;
+                                a.dbg_d[at] = dd;
+                                a.dbg_e[at] = e;
+                            }
+                            const float lo = dd - e;
+                            if (p.mode == 1)
+                            {
+                                umin = fminf(umin, dd + e);
+                                lmin = fminf(lmin, lo);
+                            }
+                            else if (lo <= p.thr_ed)
+                                mask |= 1u << i;
+                        }
+                    }
+                    stage_emit<STAGE>(mask, lane, (uint32_t)t, j0 + c * 16, sm.stage[ew], staged, a.cand, a.cand_count,
+                                      a.cand_cap);
+                }
             }
             tc_fence_before();
             mbar_arrive(&sm.acc_empty[buf]);
+            stage_flush(sm.stage[ew], staged, lane, a.cand, a.cand_count, a.cand_cap);
             if (valid && p.mode == 1 && (umin <= kFltMax || lmin == -inf_f()))
             {
                 const size_t at = (size_t)t * a.nb + j0 / kBucket;
@@ -549,7 +692,7 @@ cudaError_t launch_scan_umma(const ScanArgs &a, cudaStream_t s)
     using namespace umma;
     if (a.q_hi == nullptr || a.q_lo == nullptr || a.err == nullptr)
         return cudaErrorInvalidValue;
-    const bool mixed = a.tile_kb != nullptr;
+    const bool mixed = a.tiles != nullptr;
     if (mixed && (a.P == nullptr || a.run == nullptr || a.raw == nullptr))
         return cudaErrorInvalidValue;
     const int stride = mixed ? a.k_stride : a.m_pad;
@@ -562,13 +705,15 @@ cudaError_t launch_scan_umma(const ScanArgs &a, cudaStream_t s)
     ua.w_tiles = (int)((a.W + TN - 1) / TN);
     ua.kblocks = a.m_pad / KB;
     ua.err = a.err;
-    const size_t smem = sizeof(Smem) + 1024;
+    const size_t smem = (mixed ? sizeof(SmemT<true>) : sizeof(SmemT<false>)) + 1024;
     static bool attr = false;
     if (!attr)
     {
-        cudaError_t e = cudaFuncSetAttribute(k_scan_umma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = cudaFuncSetAttribute(k_scan_umma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)(sizeof(SmemT<false>) + 1024));
         if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_scan_umma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            e = cudaFuncSetAttribute(k_scan_umma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(sizeof(SmemT<true>) + 1024));
         if (e != cudaSuccess)
             return e;
         attr = true;

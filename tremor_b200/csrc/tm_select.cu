@@ -257,13 +257,14 @@ __global__ void __launch_bounds__(B_THREADS) k_passb_mixed(const uint2 *__restri
         if (j >= p.wcount || raw[w0 + j] == kMissing || run[w0 + j] >= p.m)
             continue;
         WindowStats ws;
-        if (prefix_stats(P[w0 + j], P[w0 + j + p.m], w0 + j, p.m, p.inv_m, center, p.qs, p.s1, ws) != 0)
+        const double2 pa = P[w0 + j];
+        if (prefix_stats(pa, (float)pa.y, P[w0 + j + p.m], w0 + j, p.m, p.inv_m, (float)center, ws) != 0)
         {
             mask |= 1u << w;
             continue;
         }
         float d, e;
-        fast_distance_mixed(p, p.a1_fp32, acc[w], ws.mu, ws.iv, shift, ws.estat, d, e);
+        fast_distance_mixed(p, p.a1_fp32, acc[w], ws.mu, ws.iv, shift, stats_error(ws, p.m, p.qs, p.s1), d, e);
         if (d - e <= T)
             mask |= 1u << w;
     }
