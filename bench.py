@@ -102,20 +102,27 @@ class ClockSampler:
 
     def __init__(self, device):
         self.device, self.proc, self.lines = device, None, []
+        self.first = threading.Event()
 
     def start(self):
+        """Starts sampling and returns once the first sample is in (at most 10 s): NVML's
+        start-up in nvidia-smi can hold the driver for about a second, which must not
+        fall inside the timed region."""
         try:
             self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.device), f'--query-gpu={self.FIELDS}',
                                           '--format=csv,noheader,nounits', '-lms', '200'],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            self.first.wait(timeout=10.0)
         except Exception:
             self.proc = None
 
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
+            self.first.set()
+        self.first.set()
 
     def stop(self):
         if self.proc is None:
@@ -362,6 +369,7 @@ def run_ours(args, w):
         batches[s % nbatch].run()
     ctx.profile_enable(True)
     ctx.profile_read()
+    ctx.profile_phases()
     ctx.d2h_bytes()
     sampler = ClockSampler(local)
     sampler.start()
@@ -369,16 +377,27 @@ def run_ours(args, w):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     pairs = 0
+    step_ev, step_host = [ev0], []
     for s in range(args.steps):
         b = batches[(args.warmup + s) % nbatch]
+        h0 = time.perf_counter()
         b.run()
+        step_host.append(1000 * (time.perf_counter() - h0))
         pairs += pair_count[(args.warmup + s) % nbatch]
+        if s + 1 < args.steps:
+            step_ev.append(torch.cuda.Event(enable_timing=True))
+            step_ev[-1].record(stream)
     ev1.record(stream)
+    step_ev.append(ev1)
     barrier()
     clocks = sampler.stop()
+    log('[bench] steps (device ms / host run ms): ' +
+        ', '.join(f'{a.elapsed_time(b):.1f}/{h:.1f}' for a, b, h in zip(step_ev, step_ev[1:], step_host)))
     ms = ev0.elapsed_time(ev1)
     kname, launches, kms, kflops, all_launches = ctx.profile_read()
+    phase_ms = {k: v / args.steps for k, v in ctx.profile_phases().items()}
     ctx.profile_enable(False)
+    log('[bench] phases per step (ms): ' + ', '.join(f'{k} {v:.1f}' for k, v in phase_ms.items()))
     d2h_value = ctx.d2h_bytes()
 
     # e2e: host templates through the public call, copies inside the timed region
@@ -451,7 +470,8 @@ def run_ours(args, w):
                         'd2h_bytes_per_step': d2h // args.steps},
                 'gpu_launches': all_launches, 'clocks': clocks,
                 'd2h_bytes_per_step_value': d2h_value // args.steps,
-                'candidates_last_step': ctx.last_candidates()}
+                'candidates_last_step': ctx.last_candidates(),
+                'phases_ms_per_step': phase_ms}
         print(json.dumps(line), flush=True)
     for b in batches:
         b.close()

@@ -169,6 +169,15 @@ int tm_profile_enable(tm_ctx *ctx, int enable);
  * kernel launches of this library since the last reset. Resets the counters. */
 int tm_profile_read(tm_ctx *ctx, char *name, size_t name_capacity, int64_t *launches, double *milliseconds,
                     double *flops, int64_t *all_launches);
+/* Milliseconds spent, since the last call and while profiling was enabled, in each of the
+ * TM_PHASES phases of a search: [0] contraction kernel, [1] kNN bound, bucket list and
+ * FP32 re-pass, [2] exact re-scoring, [3] answer filter and sort on the device, [4] copy
+ * of the answers to the host, [5] answer selection on the host. Device phases are
+ * CUDA-event spans on the context's stream. Writes min(capacity, TM_PHASES) values,
+ * resets the counters, returns TM_PHASES. No counterpart in the reference (its searches
+ * report wall-clock totals only). */
+#define TM_PHASES 6
+int tm_profile_phases(tm_ctx *ctx, double *milliseconds, int capacity);
 /* Diagnostic: for `count` raw templates of length m, the contraction kernel's distance d
  * and error bound e of every (template, window) pair, and (if `exact` is not null) the
  * reference's exact FP32 distance of every pair; count x windows floats each, for the

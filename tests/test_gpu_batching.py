@@ -137,3 +137,41 @@ def test_mixed_lengths_last_windows():
         assert int(answers[2 * k][0][0]) == end - m
         assert end - m in set(int(p) for p in answers[2 * k + 1][0])
         _check(x, reqs, answers)
+
+
+def test_results_outlive_later_searches():
+    """A result keeps its answers while later searches of the same context run and are
+    freed (the answers live in pinned blocks that the result holds)."""
+    import ctypes
+    x = _waveform(1 << 16, 14)
+    rng = np.random.default_rng(15)
+    reqs_a = _requests(x, rng, [64, 100, 200, 64])
+    reqs_b = _requests(x, rng, [128, 300, 96, 512, 40])
+    with tb.Context(x) as ctx:
+        ref_a, ref_b = ctx.scan_batch(reqs_a), ctx.scan_batch(reqs_b)
+        held = []
+        for reqs in (reqs_a, reqs_b, reqs_a):
+            res = ctypes.c_void_p()
+            ctx._check(ctx._lib.tm_scan_batch(ctx._h, ctx._requests(reqs), len(reqs), ctypes.byref(res)))
+            held.append(res)
+        ctx.scan_batch(reqs_b)  # one more search, its result freed at once
+        got = [ctx._take(r, n) for r, n in zip(held, (len(reqs_a), len(reqs_b), len(reqs_a)))]
+    for answers, ref in zip(got, (ref_a, ref_b, ref_a)):
+        for (p, d), (rp, rd) in zip(answers, ref):
+            assert np.array_equal(p, rp) and np.array_equal(d.view(np.uint32), rd.view(np.uint32))
+    _check(x, reqs_a, ref_a)
+    _check(x, reqs_b, ref_b)
+
+
+def test_large_k_selected_on_host():
+    """k above the device selection's limit (1024 kept windows per template) takes the
+    host selection over the sorted run; its answers match the oracle too, next to a
+    request that the device selects."""
+    x = _waveform(1 << 15, 16)
+    rng = np.random.default_rng(17)
+    reqs = [tb.Request(x[500:564].copy(), tb.MODE_KNN, k=1500, merge_offset=3),
+            tb.Request(x[900:1028].copy(), tb.MODE_KNN, k=20, merge_offset=64),
+            tb.Request(rng.normal(size=96).astype(np.float32), tb.MODE_THRESHOLD, correlation=0.5)]
+    with tb.Context(x) as ctx:
+        answers = ctx.scan_batch(reqs)
+    _check(x, reqs, answers)

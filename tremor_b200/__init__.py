@@ -78,6 +78,7 @@ def load_library():
         'tm_profile_read': (i, [_vp, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_int64),
                                 ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                 ctypes.POINTER(ctypes.c_int64)]),
+        'tm_profile_phases': (i, [_vp, _vp, i]),
         'tm_last_candidates': (i, [_vp, ctypes.POINTER(u64)]),
         'tm_batch_create': (i, [_vp, _vp, i, pp]),
         'tm_batch_run': (i, [_vp, _vp, pp]),
@@ -231,6 +232,16 @@ class Context:
         self._check(self._lib.tm_profile_read(self._h, name, 64, ctypes.byref(launches), ctypes.byref(ms),
                                               ctypes.byref(flops), ctypes.byref(allk)))
         return name.value.decode(), launches.value, ms.value, flops.value, allk.value
+
+    PHASES = ('contraction', 'bound_list_repass', 'rescore', 'answer_sort', 'copy_back', 'host_answers')
+
+    def profile_phases(self):
+        """{phase: milliseconds} spent in each phase of the searches since the last call,
+        while profiling was enabled (tm_profile_phases); resets."""
+        out = np.zeros(8, dtype=np.float64)
+        n = self._lib.tm_profile_phases(self._h, out.ctypes.data, len(out))
+        self._check(min(n, 0))
+        return dict(zip(self.PHASES, out[:n].tolist()))
 
     def bound_diagnostics(self, queries: np.ndarray, exact: bool = True):
         """(d, e, exact) arrays [templates, windows]: the contraction kernel's distance, its

@@ -10,6 +10,7 @@
 //   4. device: every candidate re-scored with the reference's exact arithmetic;
 //   5. host: canonical exclusion selection / threshold merge on the exact distances.
 #include <algorithm>
+#include <chrono>
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
@@ -49,6 +50,16 @@ cudaError_t launch_passb_mixed(const uint2 *list, uint32_t items, const float *x
                                const uint16_t *run, double center, const float *q, const TemplParam *tp,
                                const uint32_t *tkey, uint64_t w0, Candidate *cand, uint32_t *cand_count,
                                uint32_t cand_cap, cudaStream_t s);
+cudaError_t launch_answer_keys(const Candidate *cand, const float *dist, uint32_t count, const TemplParam *tp,
+                               unsigned long long *keys, float *vals, uint32_t *kept, cudaStream_t s);
+size_t answer_sort_scratch(uint32_t count, int T);
+cudaError_t launch_answer_order(unsigned long long *const keys[2], float *const vals32[2],
+                                unsigned long long *const vals64[2], uint32_t count, uint32_t knn_count,
+                                const TemplParam *tp, int T, void *scratch, size_t scratch_bytes, uint32_t *start,
+                                uint32_t *end, uint32_t *window, float *dist, cudaStream_t s);
+cudaError_t launch_select_knn(const int *slots, int nk, const TemplParam *tp, const uint32_t *start,
+                              const uint32_t *end, const uint32_t *window, const float *dist, int kcap,
+                              uint32_t *out_n, uint32_t *out_win, float *out_dist, cudaStream_t s);
 } // namespace tmb
 
 using tmb::Candidate;
@@ -155,9 +166,49 @@ constexpr double kE64 = 1.1102230246251565e-16; // 2^-53
 
 } // namespace
 
+// Pinned host memory holding the answers of one group; results keep it alive (shared)
+// while the context hands its pool's idle blocks to later searches.
+struct PinnedBlock
+{
+    void *p = nullptr;
+    size_t bytes = 0;
+    explicit PinnedBlock(size_t b)
+    {
+        TM_CUDA(cudaMallocHost(&p, b));
+        bytes = b;
+    }
+    PinnedBlock(const PinnedBlock &) = delete;
+    PinnedBlock &operator=(const PinnedBlock &) = delete;
+    ~PinnedBlock()
+    {
+        if (p)
+            cudaFreeHost(p);
+    }
+};
+
+// Answers of one request: hits selected on the host (kNN, empty searches), or a run of
+// a pinned block (threshold requests: window numbers relative to w0 and ED^2, in
+// position order, as the device sorted them).
+struct Answer
+{
+    std::vector<Hit> hits;
+    const uint32_t *win = nullptr;
+    const float *dist = nullptr;
+    uint64_t w0 = 0, count = 0;
+    bool run = false;
+    uint64_t size() const { return run ? count : hits.size(); }
+    Hit at(uint64_t i) const { return run ? Hit{w0 + win[i], dist[i]} : hits[i]; }
+    void set_hits(std::vector<Hit> h)
+    {
+        hits = std::move(h);
+        run = false;
+    }
+};
+
 struct tm_result
 {
-    std::vector<std::vector<Hit>> answers;
+    std::vector<Answer> answers;
+    std::vector<std::shared_ptr<PinnedBlock>> blocks;
 };
 
 struct tm_ctx
@@ -172,17 +223,23 @@ struct tm_ctx
     uint64_t use_clock = 0;
     // scratch
     DevBuf suf, tkey, bmin_u, bmin_l, list, counters, cand, dist;
+    // answer assembly: sort keys and values (double buffers), sort scratch, runs
+    DevBuf akeys, avals, avals64, sort_tmp, segs;
+    std::vector<std::shared_ptr<PinnedBlock>> pool;
     // length-independent statistics (mixed-length batches): FP64 prefix sums, constant runs
     DevBuf prefix, run;
     double center = 0.0;
     bool prefix_ready = false;
-    HostBuf h_split, h_q, h_order, h_slots, h_cand, h_dist, h_counters, h_tkey;
+    HostBuf h_split, h_q, h_order, h_slots, h_counters;
     uint32_t cand_cap = 1u << 22, list_cap = 1u << 20;
     std::string err;
     // instrumentation
     bool profile = false;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr, ev4 = nullptr;
     std::string kname;
+    // milliseconds per phase: contraction, kNN bound + bucket list + re-pass, exact
+    // re-scoring, answer sort, copy to the host, answer selection on the host
+    double phase_ms[TM_PHASES] = {};
     int64_t prof_launches = 0, all_launches = 0;
     double prof_ms = 0.0, prof_flops = 0.0;
     uint64_t last_candidates = 0;
@@ -627,54 +684,252 @@ void prepare_group_mixed(tm_ctx *ctx, const std::vector<int> &idx_in, const tm_r
            sizeof(TemplParam) * R + sizeof(tmb::TileInfo) * tiles.size();
 }
 
-// Canonical answers from the exactly re-scored candidates of each template of a group.
-// kNN: selection over (distance, position). When the bound was unbounded (too few
-// separated windows for the reference's queue to fill), the windows of distance FLT_MAX
-// (constant windows, which the contraction skips, plus any re-scored to FLT_MAX) follow
-// the finite ones in position order, as in the reference. Threshold: filter + merge.
-template <class Degenerate>
-void finish_answers(tm_ctx *ctx, const GroupPlan &g, std::vector<std::vector<Hit>> &per,
-                    std::vector<std::vector<Hit>> &answers, Degenerate degenerate_windows)
+// A pinned block of at least `need` bytes that no result holds, from the pool or new.
+std::shared_ptr<PinnedBlock> acquire_block(tm_ctx *ctx, size_t need)
 {
-    const uint32_t *tkey = ctx->h_tkey.as<uint32_t>();
+    auto &pool = ctx->pool;
+    for (auto &b : pool)
+        if (b.use_count() == 1 && b->bytes >= need)
+            return b;
+    pool.erase(std::remove_if(pool.begin(), pool.end(),
+                              [](const std::shared_ptr<PinnedBlock> &b) { return b.use_count() == 1; }),
+               pool.end());
+    pool.push_back(std::make_shared<PinnedBlock>(std::max<size_t>(need + need / 4, 1u << 20)));
+    return pool.back();
+}
+
+// Largest k whose selection runs on the device (k_select_knn keeps k windows per warp in
+// shared memory); groups with a larger k select on the host.
+constexpr int kMaxDeviceK = 1024;
+
+// What the device left for a group's answers (host pointers into the pinned block,
+// device pointers for the runs that stay on the device).
+struct AnswerView
+{
+    uint32_t *win = nullptr; // threshold runs: windows relative to w0, then ED^2
+    float *dist = nullptr;
+    const uint32_t *start = nullptr, *end = nullptr, *tkey = nullptr;
+    bool device_knn = false; // kNN selections made by k_select_knn:
+    int kcap = 0;            //   slot s: knn_n[s] answers at s * kcap
+    const uint32_t *knn_n = nullptr, *knn_win = nullptr;
+    const float *knn_dist = nullptr;
+    const uint32_t *d_win = nullptr; // the sorted runs on the device
+    const float *d_dist = nullptr;
+};
+
+// Canonical answers of each template of a group.
+// Threshold: the template's run (position order, no repeats), thinned in place by the
+// merge offset. kNN: the device's exclusion selection over the finite distances. When
+// that leaves fewer than k answers and the bound was unbounded (too few separated
+// windows for the reference's queue to fill), or k is too large for the device, the
+// template's run (in (distance, position) order) is fetched and selected here: the
+// windows of distance FLT_MAX (constant windows, which the contraction skips, plus any
+// re-scored to FLT_MAX) follow the finite ones in position order, as in the reference.
+template <class Degenerate>
+void finish_answers(tm_ctx *ctx, const GroupPlan &g, const AnswerView &v, uint64_t w0, tm_result &res,
+                    Degenerate degenerate_windows)
+{
+    int slot = -1;
     for (int t = 0; t < g.T; t++)
     {
+        const bool knn = g.mode[t] == TM_MODE_KNN;
+        slot += knn ? 1 : 0;
         if (g.index[t] < 0)
             continue; // padding row of a mixed-length tile
-        std::vector<Hit> &out = answers[g.index[t]];
-        out.clear();
-        if (g.mode[t] == TM_MODE_KNN)
+        Answer &out = res.answers[g.index[t]];
+        const uint32_t a = v.start[t], b = v.end[t];
+        if (!knn)
         {
-            std::vector<Hit> finite, infinite;
-            for (const Hit &h : per[t])
-                (h.dist < FLT_MAX ? finite : infinite).push_back(h);
-            tm_host::select_knn(finite, g.k[t], g.merge[t], out);
-            if (static_cast<int>(out.size()) < g.k[t] && tkey[t] == tmb::kEmptyKey)
+            uint32_t count = b - a;
+            if (g.merge[t] > 0) // SkipSequential.cpp:358-370: skip pos < last kept + merge + 1
             {
-                degenerate_windows(t, infinite);
-                std::sort(infinite.begin(), infinite.end(), [](const Hit &a, const Hit &b) { return a.pos < b.pos; });
-                infinite.erase(std::unique(infinite.begin(), infinite.end(),
-                                           [](const Hit &a, const Hit &b) { return a.pos == b.pos; }),
-                               infinite.end());
-                tm_host::extend_knn(infinite, g.k[t], g.merge[t], out);
+                const uint64_t gap = static_cast<uint64_t>(g.merge[t]) + 1;
+                uint32_t w = a;
+                for (uint32_t i = a; i < b; i++)
+                {
+                    if (w > a && static_cast<uint64_t>(v.win[i]) < static_cast<uint64_t>(v.win[w - 1]) + gap)
+                        continue;
+                    v.win[w] = v.win[i];
+                    v.dist[w] = v.dist[i];
+                    w++;
+                }
+                count = w - a;
             }
-            while (static_cast<int>(out.size()) < g.k[t])
-                out.push_back(Hit{0, FLT_MAX});
+            out.hits.clear();
+            out.run = true;
+            out.win = v.win + a;
+            out.dist = v.dist + a;
+            out.w0 = w0;
+            out.count = count;
+            continue;
+        }
+        std::vector<Hit> kept;
+        const bool unbounded = v.tkey[t] == tmb::kEmptyKey;
+        if (v.device_knn && (static_cast<int>(v.knn_n[slot]) >= g.k[t] || !unbounded))
+        {
+            const size_t at = static_cast<size_t>(slot) * v.kcap;
+            for (uint32_t i = 0; i < v.knn_n[slot]; i++)
+                kept.push_back(Hit{w0 + v.knn_win[at + i], v.knn_dist[at + i]});
         }
         else
         {
-            std::vector<Hit> hits;
-            hits.reserve(per[t].size());
-            for (const Hit &h : per[t])
-                if (h.dist <= g.thr[t])
-                    hits.push_back(h);
-            tm_host::threshold_merge(hits, g.merge[t], out);
+            std::vector<uint32_t> rw(b - a);
+            std::vector<float> rd(b - a);
+            if (b > a)
+            {
+                TM_CUDA(cudaMemcpyAsync(rw.data(), v.d_win + a, sizeof(uint32_t) * (b - a), cudaMemcpyDeviceToHost,
+                                        ctx->stream));
+                TM_CUDA(cudaMemcpyAsync(rd.data(), v.d_dist + a, sizeof(float) * (b - a), cudaMemcpyDeviceToHost,
+                                        ctx->stream));
+                TM_CUDA(cudaStreamSynchronize(ctx->stream));
+                ctx->d2h_bytes += 8ull * (b - a);
+            }
+            std::vector<Hit> finite, infinite;
+            for (uint32_t i = 0; i < b - a; i++)
+                (rd[i] < FLT_MAX ? finite : infinite).push_back(Hit{w0 + rw[i], rd[i]});
+            tm_host::select_knn(finite, g.k[t], g.merge[t], kept);
+            if (static_cast<int>(kept.size()) < g.k[t] && unbounded)
+            {
+                degenerate_windows(t, infinite);
+                std::sort(infinite.begin(), infinite.end(), [](const Hit &x, const Hit &y) { return x.pos < y.pos; });
+                infinite.erase(std::unique(infinite.begin(), infinite.end(),
+                                           [](const Hit &x, const Hit &y) { return x.pos == y.pos; }),
+                               infinite.end());
+                tm_host::extend_knn(infinite, g.k[t], g.merge[t], kept);
+            }
         }
+        while (static_cast<int>(kept.size()) < g.k[t])
+            kept.push_back(Hit{0, FLT_MAX});
+        out.set_hits(std::move(kept));
     }
 }
 
+void add_span(tm_ctx *ctx, int phase, cudaEvent_t a, cudaEvent_t b)
+{
+    float ms = 0.0f;
+    TM_CUDA(cudaEventElapsedTime(&ms, a, b));
+    ctx->phase_ms[phase] += ms;
+}
+
+// Exact re-scoring of a group's ncand candidates, answer order and kNN selection on the
+// device, one copy to a pinned block that the result keeps, canonical answers.
+template <class Degenerate>
+void rescore_and_answer(tm_ctx *ctx, const GroupPlan &g, uint32_t ncand, uint64_t w0, tm_result &res,
+                        Degenerate degenerate_windows)
+{
+    cudaStream_t s = ctx->stream;
+    const int T = g.T, nk = g.nk;
+    int kcap = 1;
+    for (int t = 0; t < T; t++)
+        if (g.mode[t] == TM_MODE_KNN)
+            kcap = std::max(kcap, g.k[t]);
+    const bool device_knn = nk > 0 && kcap <= kMaxDeviceK;
+    const size_t cn = std::max<uint32_t>(ncand, 1);
+    ctx->dist.reserve(sizeof(float) * cn);
+    ctx->akeys.reserve(2 * sizeof(unsigned long long) * cn);
+    ctx->avals.reserve(2 * sizeof(float) * cn);
+    if (nk > 0)
+        ctx->avals64.reserve(2 * sizeof(unsigned long long) * cn);
+    ctx->segs.reserve(sizeof(uint32_t) * (2 * static_cast<size_t>(std::max(T, 1)) +
+                                          (device_knn ? static_cast<size_t>(nk) * (1 + 2 * kcap) : 0)));
+    uint32_t *hc = ctx->h_counters.as<uint32_t>();
+    uint32_t *d_kept = ctx->counters.as<uint32_t>() + 3;
+    if (ctx->profile)
+        TM_CUDA(cudaEventRecord(ctx->ev2, s));
+    TM_CUDA(tmb::launch_rescore(ctx->cand.as<Candidate>(), ncand, g.tp.as<TemplParam>(), g.q.as<float>(),
+                                g.order.as<int>(), ctx->raw.as<float>(), w0, ctx->dist.as<float>(), s));
+    if (ncand > 0)
+        count_launch(ctx);
+    if (ctx->profile)
+        TM_CUDA(cudaEventRecord(ctx->ev3, s));
+    unsigned long long *keys[2] = {ctx->akeys.as<unsigned long long>(), ctx->akeys.as<unsigned long long>() + cn};
+    float *vals32[2] = {ctx->avals.as<float>(), ctx->avals.as<float>() + cn};
+    unsigned long long *vals64[2] = {ctx->avals64.as<unsigned long long>(),
+                                     ctx->avals64.as<unsigned long long>() + (nk > 0 ? cn : 0)};
+    TM_CUDA(cudaMemsetAsync(d_kept, 0, 2 * sizeof(uint32_t), s));
+    TM_CUDA(tmb::launch_answer_keys(ctx->cand.as<Candidate>(), ctx->dist.as<float>(), ncand, g.tp.as<TemplParam>(),
+                                    keys[0], vals32[0], d_kept, s));
+    TM_CUDA(cudaMemcpyAsync(hc + 3, d_kept, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    TM_CUDA(cudaStreamSynchronize(s));
+    if (ncand > 0)
+        count_launch(ctx);
+    const uint32_t kept = hc[3], knn_kept = hc[4], thr_kept = kept - knn_kept;
+    const size_t scratch = tmb::answer_sort_scratch(kept, T);
+    ctx->sort_tmp.reserve(scratch);
+    uint32_t *d_start = ctx->segs.as<uint32_t>(), *d_end = d_start + T;
+    uint32_t *d_knn_n = d_end + T, *d_knn_win = d_knn_n + nk;
+    float *d_knn_dist = reinterpret_cast<float *>(d_knn_win + static_cast<size_t>(nk) * kcap);
+    uint32_t *d_win = reinterpret_cast<uint32_t *>(ctx->cand.p); // the candidates are consumed: reuse
+    float *d_dist = ctx->dist.as<float>();                       // likewise the re-scored distances
+    TM_CUDA(cudaMemsetAsync(d_start, 0, 2 * sizeof(uint32_t) * T, s));
+    TM_CUDA(tmb::launch_answer_order(keys, vals32, vals64, kept, knn_kept, g.tp.as<TemplParam>(), T, ctx->sort_tmp.p,
+                                     scratch, d_start, d_end, d_win, d_dist, s));
+    if (kept > 0)
+        count_launch(ctx, knn_kept > 0 ? 4 : 2); // each radix sort counted as one launch
+    if (device_knn)
+    {
+        TM_CUDA(tmb::launch_select_knn(g.slots.as<int>(), nk, g.tp.as<TemplParam>(), d_start, d_end, d_win, d_dist,
+                                       kcap, d_knn_n, d_knn_win, d_knn_dist, s));
+        count_launch(ctx);
+    }
+    if (ctx->profile)
+        TM_CUDA(cudaEventRecord(ctx->ev4, s));
+
+    // block layout: win[thr_kept] | dist[thr_kept] | start[T] | end[T] | tkey[T] |
+    //               knn_n[nk] | knn_win[nk * kcap] | knn_dist[nk * kcap]
+    const size_t knn_words = device_knn ? static_cast<size_t>(nk) * (1 + 2 * kcap) : 0;
+    std::shared_ptr<PinnedBlock> block = acquire_block(
+        ctx, sizeof(uint32_t) * (2 * static_cast<size_t>(thr_kept) + 3 * static_cast<size_t>(T) + knn_words) + 64);
+    AnswerView v;
+    v.win = static_cast<uint32_t *>(block->p);
+    v.dist = reinterpret_cast<float *>(v.win + thr_kept);
+    uint32_t *h_start = reinterpret_cast<uint32_t *>(v.dist + thr_kept);
+    uint32_t *h_tkey = h_start + 2 * static_cast<size_t>(T);
+    uint32_t *h_knn = h_tkey + T;
+    if (thr_kept > 0)
+    {
+        TM_CUDA(cudaMemcpyAsync(v.win, d_win, sizeof(uint32_t) * thr_kept, cudaMemcpyDeviceToHost, s));
+        TM_CUDA(cudaMemcpyAsync(v.dist, d_dist, sizeof(float) * thr_kept, cudaMemcpyDeviceToHost, s));
+    }
+    TM_CUDA(cudaMemcpyAsync(h_start, d_start, 2 * sizeof(uint32_t) * T, cudaMemcpyDeviceToHost, s));
+    if (nk > 0)
+        TM_CUDA(cudaMemcpyAsync(h_tkey, ctx->tkey.p, sizeof(uint32_t) * T, cudaMemcpyDeviceToHost, s));
+    else
+        std::fill(h_tkey, h_tkey + T, 0u);
+    if (device_knn)
+        TM_CUDA(cudaMemcpyAsync(h_knn, d_knn_n, sizeof(uint32_t) * knn_words, cudaMemcpyDeviceToHost, s));
+    if (ctx->profile)
+        TM_CUDA(cudaEventRecord(ctx->ev1, s));
+    TM_CUDA(cudaStreamSynchronize(s));
+    ctx->last_candidates += ncand;
+    ctx->d2h_bytes += sizeof(uint32_t) * (2 * static_cast<uint64_t>(thr_kept) + 2 * static_cast<uint64_t>(T) +
+                                          (nk > 0 ? T : 0) + knn_words) +
+                      16;
+    const auto t0 = std::chrono::steady_clock::now();
+    if (ctx->profile)
+    {
+        add_span(ctx, 2, ctx->ev2, ctx->ev3);
+        add_span(ctx, 3, ctx->ev3, ctx->ev4);
+        add_span(ctx, 4, ctx->ev4, ctx->ev1);
+    }
+    v.start = h_start;
+    v.end = h_start + T;
+    v.tkey = h_tkey;
+    v.device_knn = device_knn;
+    v.kcap = kcap;
+    v.knn_n = h_knn;
+    v.knn_win = h_knn + nk;
+    v.knn_dist = reinterpret_cast<const float *>(h_knn + nk + static_cast<size_t>(nk) * kcap);
+    v.d_win = d_win;
+    v.d_dist = d_dist;
+    res.blocks.push_back(block);
+    finish_answers(ctx, g, v, w0, res, degenerate_windows);
+    if (ctx->profile)
+        ctx->phase_ms[5] += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
 // Device pipeline and selection for one prepared group; writes answers[index].
-void execute_group(tm_ctx *ctx, GroupPlan &g, std::vector<std::vector<Hit>> &answers)
+void execute_group(tm_ctx *ctx, GroupPlan &g, tm_result &res)
 {
     const int m = g.m;
     LengthStats &ls = ensure_length(ctx, m);
@@ -683,9 +938,9 @@ void execute_group(tm_ctx *ctx, GroupPlan &g, std::vector<std::vector<Hit>> &ans
     if (W == 0)
     {
         for (int t = 0; t < T; t++)
-            answers[g.index[t]] = g.mode[t] == TM_MODE_KNN
-                                      ? std::vector<Hit>(static_cast<size_t>(g.k[t]), Hit{0, FLT_MAX})
-                                      : std::vector<Hit>();
+            res.answers[g.index[t]].set_hits(g.mode[t] == TM_MODE_KNN
+                                                 ? std::vector<Hit>(static_cast<size_t>(g.k[t]), Hit{0, FLT_MAX})
+                                                 : std::vector<Hit>());
         return;
     }
     if (W >= (1ull << 32))
@@ -709,8 +964,8 @@ void execute_group(tm_ctx *ctx, GroupPlan &g, std::vector<std::vector<Hit>> &ans
         ctx->bmin_u.reserve(sizeof(uint32_t) * static_cast<size_t>(T) * nb);
         ctx->bmin_l.reserve(sizeof(uint32_t) * static_cast<size_t>(T) * nb);
     }
-    ctx->counters.reserve(4 * sizeof(uint32_t));
-    ctx->h_counters.reserve(4 * sizeof(uint32_t));
+    ctx->counters.reserve(8 * sizeof(uint32_t));
+    ctx->h_counters.reserve(8 * sizeof(uint32_t));
     uint32_t *hc = ctx->h_counters.as<uint32_t>();
 
     uint32_t ncand = 0;
@@ -764,6 +1019,7 @@ void execute_group(tm_ctx *ctx, GroupPlan &g, std::vector<std::vector<Hit>> &ans
             ctx->kname = use_umma ? "k_scan_umma" : "k_scan_fp32";
             ctx->prof_launches++;
             ctx->prof_ms += ms;
+            ctx->phase_ms[0] += ms;
             ctx->prof_flops += 2.0 * m * static_cast<double>(W) * T;
         }
 
@@ -795,9 +1051,13 @@ void execute_group(tm_ctx *ctx, GroupPlan &g, std::vector<std::vector<Hit>> &ans
             if (hc[1] > 0)
                 count_launch(ctx);
         }
+        if (ctx->profile)
+            TM_CUDA(cudaEventRecord(ctx->ev2, s));
         TM_CUDA(cudaMemcpyAsync(hc, d_cand_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
         TM_CUDA(cudaMemcpyAsync(hc + 2, d_cand_count + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
         TM_CUDA(cudaStreamSynchronize(s));
+        if (ctx->profile)
+            add_span(ctx, 1, ctx->ev1, ctx->ev2);
         if (hc[2] != 0)
             throw Failure{TM_ERR_TIMEOUT, "contraction kernel gave up waiting (code " + std::to_string(hc[2]) + ")"};
         ncand = hc[0];
@@ -808,35 +1068,8 @@ void execute_group(tm_ctx *ctx, GroupPlan &g, std::vector<std::vector<Hit>> &ans
             throw Failure{TM_ERR_NO_MEMORY, "candidate buffer overflow"};
     }
 
-    // 4. exact re-scoring
-    ctx->dist.reserve(sizeof(float) * std::max<uint32_t>(ncand, 1));
-    TM_CUDA(tmb::launch_rescore(ctx->cand.as<Candidate>(), ncand, g.tp.as<TemplParam>(), g.q.as<float>(),
-                                g.order.as<int>(), ctx->raw.as<float>(), w0, ctx->dist.as<float>(), s));
-    if (ncand > 0)
-        count_launch(ctx);
-    ctx->h_cand.reserve(sizeof(Candidate) * std::max<uint32_t>(ncand, 1));
-    ctx->h_dist.reserve(sizeof(float) * std::max<uint32_t>(ncand, 1));
-    ctx->h_tkey.reserve(sizeof(uint32_t) * std::max(T, 1));
-    if (ncand > 0)
-    {
-        TM_CUDA(cudaMemcpyAsync(ctx->h_cand.p, ctx->cand.p, sizeof(Candidate) * ncand, cudaMemcpyDeviceToHost, s));
-        TM_CUDA(cudaMemcpyAsync(ctx->h_dist.p, ctx->dist.p, sizeof(float) * ncand, cudaMemcpyDeviceToHost, s));
-    }
-    if (nk > 0)
-        TM_CUDA(cudaMemcpyAsync(ctx->h_tkey.p, ctx->tkey.p, sizeof(uint32_t) * T, cudaMemcpyDeviceToHost, s));
-    TM_CUDA(cudaStreamSynchronize(s));
-    ctx->last_candidates += ncand;
-    ctx->d2h_bytes += (sizeof(Candidate) + sizeof(float)) * static_cast<uint64_t>(ncand) + 8 +
-                      (nk > 0 ? sizeof(uint32_t) * T : 0);
-
-    // 5. answers
-    std::vector<std::vector<Hit>> per(T);
-    const Candidate *hcand = ctx->h_cand.as<Candidate>();
-    const float *hdist = ctx->h_dist.as<float>();
-    for (uint32_t i = 0; i < ncand; i++)
-        per[hcand[i].templ].push_back(Hit{w0 + hcand[i].window, hdist[i]});
     std::vector<uint8_t> flags; // fetched only when some kNN bound is unbounded
-    finish_answers(ctx, g, per, answers, [&](int, std::vector<Hit> &degenerate) {
+    rescore_and_answer(ctx, g, ncand, w0, res, [&](int, std::vector<Hit> &degenerate) {
         if (flags.empty())
         {
             flags.resize(W);
@@ -849,7 +1082,7 @@ void execute_group(tm_ctx *ctx, GroupPlan &g, std::vector<std::vector<Hit>> &ans
 }
 
 // Device pipeline for a mixed-length group (tensor-core kernel only).
-void execute_group_mixed(tm_ctx *ctx, GroupPlan &g, std::vector<std::vector<Hit>> &answers)
+void execute_group_mixed(tm_ctx *ctx, GroupPlan &g, tm_result &res)
 {
     if (ctx->kernel == TM_KERNEL_FP32)
         throw Failure{TM_ERR_STATE, "batch of several template lengths was prepared for the tensor-core kernel"};
@@ -860,9 +1093,9 @@ void execute_group_mixed(tm_ctx *ctx, GroupPlan &g, std::vector<std::vector<Hit>
     {
         for (int t = 0; t < T; t++)
             if (g.index[t] >= 0)
-                answers[g.index[t]] = g.mode[t] == TM_MODE_KNN
-                                          ? std::vector<Hit>(static_cast<size_t>(g.k[t]), Hit{0, FLT_MAX})
-                                          : std::vector<Hit>();
+                res.answers[g.index[t]].set_hits(g.mode[t] == TM_MODE_KNN
+                                                     ? std::vector<Hit>(static_cast<size_t>(g.k[t]), Hit{0, FLT_MAX})
+                                                     : std::vector<Hit>());
         return;
     }
     if (W >= (1ull << 32))
@@ -875,8 +1108,8 @@ void execute_group_mixed(tm_ctx *ctx, GroupPlan &g, std::vector<std::vector<Hit>
         ctx->bmin_u.reserve(sizeof(uint32_t) * static_cast<size_t>(T) * nb);
         ctx->bmin_l.reserve(sizeof(uint32_t) * static_cast<size_t>(T) * nb);
     }
-    ctx->counters.reserve(4 * sizeof(uint32_t));
-    ctx->h_counters.reserve(4 * sizeof(uint32_t));
+    ctx->counters.reserve(8 * sizeof(uint32_t));
+    ctx->h_counters.reserve(8 * sizeof(uint32_t));
     uint32_t *hc = ctx->h_counters.as<uint32_t>();
     double flops = 0.0;
     for (int t = 0; t < T; t++)
@@ -932,6 +1165,7 @@ void execute_group_mixed(tm_ctx *ctx, GroupPlan &g, std::vector<std::vector<Hit>
             ctx->kname = "k_scan_umma";
             ctx->prof_launches++;
             ctx->prof_ms += ms;
+            ctx->phase_ms[0] += ms;
             ctx->prof_flops += flops;
         }
         if (nk > 0)
@@ -962,9 +1196,13 @@ void execute_group_mixed(tm_ctx *ctx, GroupPlan &g, std::vector<std::vector<Hit>
             if (hc[1] > 0)
                 count_launch(ctx);
         }
+        if (ctx->profile)
+            TM_CUDA(cudaEventRecord(ctx->ev2, s));
         TM_CUDA(cudaMemcpyAsync(hc, d_cand_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
         TM_CUDA(cudaMemcpyAsync(hc + 2, d_cand_count + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
         TM_CUDA(cudaStreamSynchronize(s));
+        if (ctx->profile)
+            add_span(ctx, 1, ctx->ev1, ctx->ev2);
         if (hc[2] != 0)
             throw Failure{TM_ERR_TIMEOUT, "contraction kernel gave up waiting (code " + std::to_string(hc[2]) + ")"};
         ncand = hc[0];
@@ -974,34 +1212,9 @@ void execute_group_mixed(tm_ctx *ctx, GroupPlan &g, std::vector<std::vector<Hit>
         if (attempt == 2)
             throw Failure{TM_ERR_NO_MEMORY, "candidate buffer overflow"};
     }
-    ctx->dist.reserve(sizeof(float) * std::max<uint32_t>(ncand, 1));
-    TM_CUDA(tmb::launch_rescore(ctx->cand.as<Candidate>(), ncand, g.tp.as<TemplParam>(), g.q.as<float>(),
-                                g.order.as<int>(), ctx->raw.as<float>(), w0, ctx->dist.as<float>(), s));
-    if (ncand > 0)
-        count_launch(ctx);
-    ctx->h_cand.reserve(sizeof(Candidate) * std::max<uint32_t>(ncand, 1));
-    ctx->h_dist.reserve(sizeof(float) * std::max<uint32_t>(ncand, 1));
-    ctx->h_tkey.reserve(sizeof(uint32_t) * std::max(T, 1));
-    if (ncand > 0)
-    {
-        TM_CUDA(cudaMemcpyAsync(ctx->h_cand.p, ctx->cand.p, sizeof(Candidate) * ncand, cudaMemcpyDeviceToHost, s));
-        TM_CUDA(cudaMemcpyAsync(ctx->h_dist.p, ctx->dist.p, sizeof(float) * ncand, cudaMemcpyDeviceToHost, s));
-    }
-    if (nk > 0)
-        TM_CUDA(cudaMemcpyAsync(ctx->h_tkey.p, ctx->tkey.p, sizeof(uint32_t) * T, cudaMemcpyDeviceToHost, s));
-    TM_CUDA(cudaStreamSynchronize(s));
-    ctx->last_candidates += ncand;
-    ctx->d2h_bytes += (sizeof(Candidate) + sizeof(float)) * static_cast<uint64_t>(ncand) + 8 +
-                      (nk > 0 ? sizeof(uint32_t) * T : 0);
-
-    std::vector<std::vector<Hit>> per(T);
-    const Candidate *hcand = ctx->h_cand.as<Candidate>();
-    const float *hdist = ctx->h_dist.as<float>();
-    for (uint32_t i = 0; i < ncand; i++)
-        per[hcand[i].templ].push_back(Hit{w0 + hcand[i].window, hdist[i]});
     std::vector<uint16_t> run;
     std::vector<float> raw;
-    finish_answers(ctx, g, per, answers, [&](int t, std::vector<Hit> &degenerate) {
+    rescore_and_answer(ctx, g, ncand, w0, res, [&](int t, std::vector<Hit> &degenerate) {
         if (run.empty())
         {
             run.resize(W);
@@ -1053,14 +1266,15 @@ void create_batch(tm_ctx *ctx, const tm_request *requests, int count, tm_batch &
 
 void run_batch(tm_ctx *ctx, tm_batch &b, tm_result &res)
 {
-    res.answers.assign(static_cast<size_t>(b.count), std::vector<Hit>());
+    res.answers.assign(static_cast<size_t>(b.count), Answer());
+    res.blocks.clear();
     ctx->last_candidates = 0;
     for (GroupPlan &g : b.groups)
     {
         if (g.mixed)
-            execute_group_mixed(ctx, g, res.answers);
+            execute_group_mixed(ctx, g, res);
         else
-            execute_group(ctx, g, res.answers);
+            execute_group(ctx, g, res);
     }
 }
 
@@ -1108,6 +1322,9 @@ int tm_ctx_create(const float *raw, uint64_t n, int device, tm_ctx **out)
         TM_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
         TM_CUDA(cudaEventCreate(&ctx->ev0));
         TM_CUDA(cudaEventCreate(&ctx->ev1));
+        TM_CUDA(cudaEventCreate(&ctx->ev2));
+        TM_CUDA(cudaEventCreate(&ctx->ev3));
+        TM_CUDA(cudaEventCreate(&ctx->ev4));
         const uint64_t total = n + tmb::kStagePad;
         ctx->raw.reserve(sizeof(float) * total);
         ctx->clean.reserve(sizeof(float) * total);
@@ -1138,15 +1355,18 @@ int tm_ctx_destroy(tm_ctx *ctx)
         kv.second->inv.release();
         kv.second->flags.release();
     }
-    for (DevBuf *b : {&ctx->prefix, &ctx->run, &ctx->raw, &ctx->clean, &ctx->suf, &ctx->tkey, &ctx->bmin_u, &ctx->bmin_l, &ctx->list, &ctx->counters, &ctx->cand, &ctx->dist})
+    for (DevBuf *b : {&ctx->prefix, &ctx->run, &ctx->raw, &ctx->clean, &ctx->suf, &ctx->tkey, &ctx->bmin_u,
+                      &ctx->bmin_l, &ctx->list, &ctx->counters, &ctx->cand, &ctx->dist, &ctx->akeys, &ctx->avals,
+                      &ctx->avals64, &ctx->sort_tmp, &ctx->segs})
         b->release();
-    for (HostBuf *b : {&ctx->h_split, &ctx->h_q, &ctx->h_order, &ctx->h_slots, &ctx->h_cand, &ctx->h_dist,
-                       &ctx->h_counters, &ctx->h_tkey})
+    for (HostBuf *b : {&ctx->h_split, &ctx->h_q, &ctx->h_order, &ctx->h_slots, &ctx->h_counters})
         b->release();
+    ctx->pool.clear(); // blocks still held by results are freed with the last of them
     if (ctx->ev0)
         cudaEventDestroy(ctx->ev0);
-    if (ctx->ev1)
-        cudaEventDestroy(ctx->ev1);
+    for (cudaEvent_t e : {ctx->ev1, ctx->ev2, ctx->ev3, ctx->ev4})
+        if (e)
+            cudaEventDestroy(e);
     if (ctx->stream)
         cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -1293,8 +1513,9 @@ int tm_search_knn(tm_ctx *ctx, const float *queries, int count, int m, int k, in
     for (int i = 0; i < count; i++)
         for (int j = 0; j < k; j++)
         {
-            I[static_cast<size_t>(i) * k + j] = res->answers[i][j].pos;
-            D[static_cast<size_t>(i) * k + j] = res->answers[i][j].dist;
+            const Hit h = res->answers[i].at(j);
+            I[static_cast<size_t>(i) * k + j] = h.pos;
+            D[static_cast<size_t>(i) * k + j] = h.dist;
         }
     tm_result_free(res);
     return TM_OK;
@@ -1324,15 +1545,24 @@ int tm_result_get(const tm_result *res, int request, uint64_t *positions, float 
 {
     if (res == nullptr || request < 0 || request >= static_cast<int>(res->answers.size()))
         return TM_ERR_ARGUMENT;
-    const std::vector<Hit> &a = res->answers[request];
+    const Answer &a = res->answers[request];
     if (capacity < a.size())
         return TM_ERR_CAPACITY;
-    for (size_t i = 0; i < a.size(); i++)
+    if (a.run)
     {
         if (positions)
-            positions[i] = a[i].pos;
+            for (uint64_t i = 0; i < a.count; i++)
+                positions[i] = a.w0 + a.win[i];
+        if (distances && a.count > 0)
+            std::memcpy(distances, a.dist, sizeof(float) * a.count);
+        return TM_OK;
+    }
+    for (size_t i = 0; i < a.hits.size(); i++)
+    {
+        if (positions)
+            positions[i] = a.hits[i].pos;
         if (distances)
-            distances[i] = a[i].dist;
+            distances[i] = a.hits[i].dist;
     }
     return TM_OK;
 }
@@ -1372,6 +1602,19 @@ int tm_profile_read(tm_ctx *ctx, char *name, size_t name_capacity, int64_t *laun
     ctx->prof_flops = 0.0;
     ctx->all_launches = 0;
     return TM_OK;
+}
+
+int tm_profile_phases(tm_ctx *ctx, double *milliseconds, int capacity)
+{
+    if (ctx == nullptr || capacity < 0 || (capacity > 0 && milliseconds == nullptr))
+        return TM_ERR_ARGUMENT;
+    for (int i = 0; i < TM_PHASES; i++)
+    {
+        if (i < capacity)
+            milliseconds[i] = ctx->phase_ms[i];
+        ctx->phase_ms[i] = 0.0;
+    }
+    return TM_PHASES;
 }
 
 int tm_bound_diagnostics(tm_ctx *ctx, const float *queries, int count, int m, float *d, float *e, float *exact)
