@@ -59,6 +59,13 @@ WORKLOADS = {
                      per_step=4096, seed=2029),
     'batching_small': dict(n=1 << 25, q=512, m=(256, 8192), events=250, mode='mixed', k=0, merge=0, corr=0.0,
                            per_step=512, seed=2029),
+    # config 5: 2^29 samples resident with their prefix sums; a Poisson stream of requests
+    # (lengths log-uniform in [128, 16384], 50/50 kNN / threshold as in config 4) served
+    # with continuous batching; one step = one request
+    'serving': dict(n=1 << 29, q=1024, m=(128, 16384), events=4000, mode='mixed', k=0, merge=0, corr=0.0,
+                    per_step=1, seed=2030, serve=True, requests=400, rate=200.0),
+    'serving_small': dict(n=1 << 26, q=256, m=(128, 16384), events=500, mode='mixed', k=0, merge=0, corr=0.0,
+                          per_step=1, seed=2030, serve=True, requests=200, rate=200.0),
 }
 
 
@@ -340,6 +347,114 @@ def run_reference(args, w):
         dist.destroy_process_group()
 
 
+def run_serving(args, w):
+    """Config 5: a Poisson stream of requests against a served context. Throughput is total
+    pairs over the span from the first submission to the last completion (the server's
+    steady clock); latency is completion minus submission per request. Warm-up requests
+    are served and discarded first."""
+    import threading as th
+    import torch
+    import tremor_b200 as tb
+    rank, world, local, dist = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    x, q = make_workload(w)
+    reqs = requests_for(w, q)
+    rate = args.rate or w['rate']
+    count = args.requests or w['requests']
+    rng = np.random.default_rng(w['seed'] + 2 + rank)
+    pick = rng.integers(0, len(reqs), size=count)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=count))
+    ctx = tb.Context(x, device=local)
+    t0 = time.time()
+    server = ctx.serve(workers=args.workers, max_batch=args.max_batch)
+    log(f'[bench] server started (prefix sums) in {time.time() - t0:.2f} s')
+    for s in range(args.warmup):  # untimed: a few batches of 8 requests
+        for i in range(8):
+            server.submit(reqs[(s * 8 + i) % len(reqs)])
+        got = 0
+        while got < 8:
+            got += len(server.poll(64, 1000))
+    launches0 = server.status()[3]
+    sampler = ClockSampler(local)
+    sampler.start()
+    if dist:
+        dist.barrier()
+    tickets = {}
+
+    def submitter():
+        start = time.perf_counter()
+        for i in range(count):
+            delay = arrivals[i] - (time.perf_counter() - start)
+            if delay > 0:
+                time.sleep(delay)
+            tickets[server.submit(reqs[pick[i]])] = i
+
+    sub = th.Thread(target=submitter)
+    sub.start()
+    done = {}
+    while len(done) < count:
+        for c in server.poll(256, 500):
+            done[c.ticket] = c
+    sub.join()
+    clocks = sampler.stop()
+    launches = server.status()[3] - launches0
+    server.stop()
+    comps = list(done.values())
+    bad = [c for c in comps if c.status != 0]
+    if bad:
+        raise RuntimeError(f'{len(bad)} served requests failed (status {bad[0].status})')
+    span_ms = max(c.done_ms for c in comps) - min(c.submit_ms for c in comps)
+    lens = [len(reqs[pick[tickets[c.ticket]]].template) for c in comps]
+    pairs = sum(w['n'] - m + 1 for m in lens)
+    flops = sum(2.0 * m * (w['n'] - m + 1) for m in lens)
+    lat = np.array([c.done_ms - c.submit_ms for c in comps])
+    queue = np.array([c.start_ms - c.submit_ms for c in comps])
+    service = np.array([c.done_ms - c.start_ms for c in comps])
+    answers = sum(len(c.answers[0]) for c in comps)
+    t = torch.tensor([pairs, flops, span_ms], dtype=torch.float64, device=f'cuda:{local}')
+    if dist:
+        tot = t.clone()
+        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+        mx = t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        t = torch.stack([tot[0], tot[1], mx[2]])
+    pairs_all, flops_all, span_ms = t.tolist()
+    value = pairs_all / (span_ms / 1e3) / 1e9
+    if rank == 0:
+        bf16_peak, _, peak_kind = peaks()
+        achieved = flops_all / world / (span_ms / 1e3) / 1e12
+        roof = {'bound': 'tensor', 'achieved': achieved, 'peak': bf16_peak / 3.0, 'unit': 'TFLOP/s',
+                'frac': achieved / (bf16_peak / 3.0), 'traffic': None, 'kernel': 'k_scan_umma',
+                'peak_note': f'{peak_kind} bf16 dense / 3; achieved = algorithmic flops over the whole '
+                             'serving span (a lower bound on the kernel rate: queue gaps included)'}
+        cpu_v, cpu_info = (None, {'error': 'skipped'}) if args.no_cpu else cpu_reference(w, x, q)
+        pct = lambda a, p: float(np.percentile(a, p))
+        line = {'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': count,
+                'warmup': args.warmup, 'ms_per_step': span_ms / count, 'higher_is_better': True,
+                'scaling': 'weak', 'vs_baseline': None, 'dtype': 'bf16x3+f32', 'data': 'synthetic',
+                'config': {'workload': args.workload, 'n': w['n'], 'templates': w['q'], 'm': w['m'],
+                           'requests': count, 'arrival': f'poisson {rate} req/s', 'seed': w['seed'],
+                           'workers': args.workers, 'max_batch': args.max_batch,
+                           'l2': 'inputs larger than L2 (waveform 4n bytes)', 'parallelism': f'replicas x{world}',
+                           'timing': 'server steady clock, first submission to last completion'},
+                'latency_ms': {'p50': pct(lat, 50), 'p99': pct(lat, 99), 'mean': float(lat.mean()),
+                               'queue_p50': pct(queue, 50), 'queue_p99': pct(queue, 99),
+                               'service_p50': pct(service, 50), 'service_p99': pct(service, 99)},
+                'offered_rate_rps': rate, 'achieved_rate_rps': count / (span_ms / 1e3),
+                'batch_size': {'mean': float(np.mean([c.batch_size for c in comps])),
+                               'max': int(max(c.batch_size for c in comps))},
+                'roofline': roof,
+                'cpu_baseline': {'value': cpu_v, 'unit': UNIT, **cpu_info},
+                'e2e': {'value': value, 'unit': UNIT,
+                        'h2d_bytes_per_step': int(4 * sum(lens) / count),
+                        'd2h_bytes_per_step': int(8 * answers / count)},
+                'gpu_launches': launches, 'clocks': clocks}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
 def run_ours(args, w):
     import torch
     import tremor_b200 as tb
@@ -489,12 +604,18 @@ def main():
     p.add_argument('--workload', choices=sorted(WORKLOADS), default='precision')
     p.add_argument('--kernel', choices=['auto', 'fp32', 'bf16'], default='auto')
     p.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline leg')
+    p.add_argument('--rate', type=float, default=0.0, help='serving: Poisson arrival rate (req/s)')
+    p.add_argument('--requests', type=int, default=0, help='serving: requests in the timed stream')
+    p.add_argument('--workers', type=int, default=2, help='serving: batches in flight at once')
+    p.add_argument('--max-batch', type=int, default=256, help='serving: requests per batch at most')
     args = p.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     w = WORKLOADS[args.workload]
     if args.impl == 'reference':
         run_reference(args, w)
+    elif w.get('serve'):
+        run_serving(args, w)
     else:
         run_ours(args, w)
 

@@ -191,6 +191,51 @@ int tm_ctx_stream(tm_ctx *ctx, void **stream);
 /* Candidates re-scored exactly in the last search (diagnostic). */
 int tm_last_candidates(const tm_ctx *ctx, uint64_t *count);
 
+/* ---- Serving: continuous batching over the resident waveform ----------------------
+ * No counterpart in the reference, which hands template ids to MPI ranks
+ * (Tremor.cpp:796-905, SkipSequential.cpp:97-136); this is the single-GPU equivalent.
+ * tm_serve_start builds the resident FP64 prefix sums and starts `workers` threads, each
+ * with its own stream and scratch. tm_submit queues one request (its template is copied;
+ * any thread may submit). Each worker admits the oldest pending requests, at most
+ * max_batch and within the device-memory budget for requests in flight, runs them as one
+ * batch of mixed lengths and completes them; batches of different workers overlap on the
+ * device. tm_poll returns completions (one consumer). Every request's answers equal those
+ * of the same request searched alone. Lengths up to 16384; needs the tensor-core kernel.
+ * While serving, tm_set_kernel and tm_set_window_range return TM_ERR_STATE; the other
+ * calls stay usable. */
+typedef struct tm_serve_config
+{
+    int workers;            /* batches in flight at once (1-8; default 2) */
+    int max_batch;          /* requests per batch at most (default 256) */
+    uint64_t memory_budget; /* device bytes for requests in flight; 0: a quarter of the free memory */
+} tm_serve_config;
+
+typedef struct tm_completion
+{
+    uint64_t ticket;   /* as returned by tm_submit */
+    int status;        /* TM_OK, or the error of the batch that carried the request */
+    int batch_size;    /* requests in that batch */
+    tm_result *result; /* the request's answers (request index 0); free with tm_result_free */
+    double submit_ms;  /* milliseconds since tm_serve_start: submitted, */
+    double start_ms;   /*   its batch admitted, */
+    double done_ms;    /*   answers complete */
+} tm_completion;
+
+/* config may be null (defaults). TM_ERR_STATE if already serving or the tensor-core
+ * kernel is not available. */
+int tm_serve_start(tm_ctx *ctx, const tm_serve_config *config);
+int tm_submit(tm_ctx *ctx, const tm_request *request, uint64_t *ticket);
+/* Up to `capacity` completions; waits up to timeout_ms for the first (0: no wait, <0: no
+ * limit). *count = completions written. */
+int tm_poll(tm_ctx *ctx, tm_completion *out, int capacity, int timeout_ms, int *count);
+/* Completes everything submitted, then stops the workers; completions stay pollable
+ * until the next tm_serve_start or tm_ctx_destroy (which stops serving too). */
+int tm_serve_stop(tm_ctx *ctx);
+/* Requests queued, requests in batches on the GPU, their admitted device bytes, and the
+ * kernel launches of the served batches so far (any pointer may be null). */
+int tm_serve_status(tm_ctx *ctx, uint64_t *pending, uint64_t *in_flight, uint64_t *in_flight_bytes,
+                    uint64_t *launches);
+
 #ifdef __cplusplus
 }
 #endif

@@ -49,6 +49,16 @@ class _Request(ctypes.Structure):
                 ('merge_offset', ctypes.c_int32), ('correlation', ctypes.c_float), ('flags', ctypes.c_uint32)]
 
 
+class _ServeConfig(ctypes.Structure):
+    _fields_ = [('workers', ctypes.c_int32), ('max_batch', ctypes.c_int32), ('memory_budget', ctypes.c_uint64)]
+
+
+class _Completion(ctypes.Structure):
+    _fields_ = [('ticket', ctypes.c_uint64), ('status', ctypes.c_int32), ('batch_size', ctypes.c_int32),
+                ('result', _vp), ('submit_ms', ctypes.c_double), ('start_ms', ctypes.c_double),
+                ('done_ms', ctypes.c_double)]
+
+
 def load_library():
     """Loads libtremor_b200.so; raises ImportError when it was not built."""
     global _lib
@@ -79,6 +89,12 @@ def load_library():
                                 ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                 ctypes.POINTER(ctypes.c_int64)]),
         'tm_profile_phases': (i, [_vp, _vp, i]),
+        'tm_serve_start': (i, [_vp, _vp]),
+        'tm_submit': (i, [_vp, _vp, ctypes.POINTER(u64)]),
+        'tm_poll': (i, [_vp, _vp, i, i, ctypes.POINTER(i)]),
+        'tm_serve_stop': (i, [_vp]),
+        'tm_serve_status': (i, [_vp, ctypes.POINTER(u64), ctypes.POINTER(u64), ctypes.POINTER(u64),
+                                ctypes.POINTER(u64)]),
         'tm_last_candidates': (i, [_vp, ctypes.POINTER(u64)]),
         'tm_batch_create': (i, [_vp, _vp, i, pp]),
         'tm_batch_run': (i, [_vp, _vp, pp]),
@@ -192,6 +208,10 @@ class Context:
         self._check(self._lib.tm_scan_batch(self._h, arr, len(requests), ctypes.byref(res)))
         return self._take(res, len(requests))
 
+    def serve(self, workers: int = 2, max_batch: int = 256, memory_budget: int = 0) -> 'Server':
+        """Starts continuous batching over this context's waveform (tm_serve_start)."""
+        return Server(self, workers, max_batch, memory_budget)
+
     def batch(self, requests: Sequence[Request]) -> 'Batch':
         """A prepared batch whose templates stay resident on the device (tm_batch)."""
         return Batch(self, requests)
@@ -293,6 +313,67 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+class Completion:
+    """One served request: its ticket, status (0 = answers present), answers (positions,
+    distances) and times in ms since the server started (submitted, batch admitted,
+    done), with the size of the batch that carried it."""
+
+    def __init__(self, ticket, status, answers, submit_ms, start_ms, done_ms, batch_size):
+        self.ticket, self.status, self.answers = ticket, status, answers
+        self.submit_ms, self.start_ms, self.done_ms, self.batch_size = submit_ms, start_ms, done_ms, batch_size
+
+    @property
+    def latency_ms(self) -> float:
+        return self.done_ms - self.submit_ms
+
+
+class Server:
+    """Continuous batching over a context's resident waveform (tm_serve_*): submit() from
+    any thread, poll() from one."""
+
+    def __init__(self, ctx: Context, workers: int = 2, max_batch: int = 256, memory_budget: int = 0):
+        self.ctx = ctx
+        cfg = _ServeConfig(workers, max_batch, memory_budget)
+        ctx._check(ctx._lib.tm_serve_start(ctx._h, ctypes.byref(cfg)))
+        self._running = True
+
+    def submit(self, request: Request) -> int:
+        arr = Context._requests([request])
+        t = ctypes.c_uint64(0)
+        self.ctx._check(self.ctx._lib.tm_submit(self.ctx._h, arr, ctypes.byref(t)))
+        return t.value
+
+    def poll(self, max_count: int = 256, timeout_ms: int = 100) -> List[Completion]:
+        buf = (_Completion * max_count)()
+        n = ctypes.c_int(0)
+        self.ctx._check(self.ctx._lib.tm_poll(self.ctx._h, buf, max_count, int(timeout_ms), ctypes.byref(n)))
+        out = []
+        for c in buf[:n.value]:
+            answers = self.ctx._take(_vp(c.result), 1)[0] if c.status == 0 and c.result else None
+            out.append(Completion(c.ticket, c.status, answers, c.submit_ms, c.start_ms, c.done_ms, c.batch_size))
+        return out
+
+    def status(self):
+        """(requests pending, requests in flight, admitted device bytes in flight, kernel
+        launches of the served batches so far)."""
+        a, b, c, d = (ctypes.c_uint64(0) for _ in range(4))
+        self.ctx._check(self.ctx._lib.tm_serve_status(self.ctx._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c),
+                                                      ctypes.byref(d)))
+        return a.value, b.value, c.value, d.value
+
+    def stop(self):
+        """Completes everything submitted; completions stay pollable."""
+        if self._running:
+            self._running = False
+            self.ctx._check(self.ctx._lib.tm_serve_stop(self.ctx._h))
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.stop()
 
 
 def ed_to_cc(ed: float, m: int) -> float:

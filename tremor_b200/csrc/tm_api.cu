@@ -10,6 +10,10 @@
 //   4. device: every candidate re-scored with the reference's exact arithmetic;
 //   5. host: canonical exclusion selection / threshold merge on the exact distances.
 #include <algorithm>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
+#include <thread>
 #include <chrono>
 #include <cfloat>
 #include <cmath>
@@ -211,28 +215,19 @@ struct tm_result
     std::vector<std::shared_ptr<PinnedBlock>> blocks;
 };
 
-struct tm_ctx
+// The device state of one search in flight: a stream, its events, the search's scratch
+// buffers and pinned staging, and its counters. The synchronous calls use the context's
+// main lane; each serving worker owns one more, so searches on different lanes overlap
+// (one's host work and copies with another's kernels).
+struct Lane
 {
-    int device = 0;
     cudaStream_t stream = nullptr;
-    uint64_t n = 0;
-    DevBuf raw, clean;
-    uint64_t range_first = 0, range_count = UINT64_MAX;
-    int kernel = TM_KERNEL_AUTO;
-    std::map<int, std::unique_ptr<LengthStats>> lengths;
-    uint64_t use_clock = 0;
-    // scratch
-    DevBuf suf, tkey, bmin_u, bmin_l, list, counters, cand, dist;
+    DevBuf tkey, bmin_u, bmin_l, list, counters, cand, dist;
     // answer assembly: sort keys and values (double buffers), sort scratch, runs
     DevBuf akeys, avals, avals64, sort_tmp, segs;
     std::vector<std::shared_ptr<PinnedBlock>> pool;
-    // length-independent statistics (mixed-length batches): FP64 prefix sums, constant runs
-    DevBuf prefix, run;
-    double center = 0.0;
-    bool prefix_ready = false;
     HostBuf h_split, h_q, h_order, h_slots, h_counters;
     uint32_t cand_cap = 1u << 22, list_cap = 1u << 20;
-    std::string err;
     // instrumentation
     bool profile = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr, ev4 = nullptr;
@@ -244,6 +239,54 @@ struct tm_ctx
     double prof_ms = 0.0, prof_flops = 0.0;
     uint64_t last_candidates = 0;
     uint64_t d2h_bytes = 0;
+
+    void open()
+    {
+        TM_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        for (cudaEvent_t *e : {&ev0, &ev1, &ev2, &ev3, &ev4})
+            TM_CUDA(cudaEventCreate(e));
+    }
+    void close()
+    {
+        if (stream)
+            cudaStreamSynchronize(stream);
+        for (DevBuf *b : {&tkey, &bmin_u, &bmin_l, &list, &counters, &cand, &dist, &akeys, &avals, &avals64, &sort_tmp,
+                          &segs})
+            b->release();
+        for (HostBuf *b : {&h_split, &h_q, &h_order, &h_slots, &h_counters})
+            b->release();
+        pool.clear(); // blocks still held by results are freed with the last of them
+        for (cudaEvent_t *e : {&ev0, &ev1, &ev2, &ev3, &ev4})
+            if (*e)
+            {
+                cudaEventDestroy(*e);
+                *e = nullptr;
+            }
+        if (stream)
+            cudaStreamDestroy(stream);
+        stream = nullptr;
+    }
+};
+
+struct Server;
+
+struct tm_ctx
+{
+    int device = 0;
+    uint64_t n = 0;
+    DevBuf raw, clean;
+    uint64_t range_first = 0, range_count = UINT64_MAX;
+    int kernel = TM_KERNEL_AUTO;
+    std::map<int, std::unique_ptr<LengthStats>> lengths;
+    uint64_t use_clock = 0;
+    DevBuf suf; // window-statistics scratch (per-length statistics)
+    // length-independent statistics (mixed-length batches): FP64 prefix sums, constant runs
+    DevBuf prefix, run;
+    double center = 0.0;
+    bool prefix_ready = false;
+    std::string err;
+    Lane main;                      // the synchronous calls' lane
+    std::unique_ptr<Server> server; // serving engine, while started
 };
 
 namespace {
@@ -274,9 +317,9 @@ template <class F> int guarded(tm_ctx *ctx, F body)
     }
 }
 
-void count_launch(tm_ctx *ctx, int k = 1) { ctx->all_launches += k; }
+void count_launch(Lane &L, int k = 1) { L.all_launches += k; }
 
-LengthStats &ensure_length(tm_ctx *ctx, int m)
+LengthStats &ensure_length(tm_ctx *ctx, Lane &L, int m)
 {
     auto it = ctx->lengths.find(m);
     if (it != ctx->lengths.end())
@@ -316,8 +359,8 @@ LengthStats &ensure_length(tm_ctx *ctx, int m)
         ctx->suf.reserve(a_count * static_cast<uint64_t>(m) * sizeof(double2));
         TM_CUDA(tmb::launch_window_stats(ctx->clean.as<float>(), ctx->raw.as<float>(), ctx->n, m, w0, W,
                                         ctx->suf.as<double2>(), ls->mean.as<float>(), ls->inv.as<float>(),
-                                        ls->flags.as<uint8_t>(), ctx->stream));
-        count_launch(ctx, 3);
+                                        ls->flags.as<uint8_t>(), L.stream));
+        count_launch(L, 3);
     }
     ls->last_use = ++ctx->use_clock;
     LengthStats &ref = *ls;
@@ -397,7 +440,7 @@ namespace {
 
 // Host preparation of one group (bit-identical template z-normalisation and block
 // order, epilogue constants) and its upload.
-void prepare_group(tm_ctx *ctx, int m, const std::vector<int> &idx, const tm_request *reqs, GroupPlan &g,
+void prepare_group(tm_ctx *ctx, Lane &L, int m, const std::vector<int> &idx, const tm_request *reqs, GroupPlan &g,
                    uint64_t &h2d)
 {
     g.m = m;
@@ -408,12 +451,12 @@ void prepare_group(tm_ctx *ctx, int m, const std::vector<int> &idx, const tm_req
     g.umma_constants = false;
     g.index = idx;
     const int T = g.T, T_pad = g.T_pad, m_pad = g.m_pad, nblk = g.nblk;
-    ctx->h_q.reserve(sizeof(float) * static_cast<size_t>(T_pad) * m_pad);
-    ctx->h_order.reserve(sizeof(int) * static_cast<size_t>(T) * nblk);
-    ctx->h_slots.reserve(sizeof(int) * T);
-    float *hq = ctx->h_q.as<float>();
-    int *ho = ctx->h_order.as<int>();
-    int *hslots = ctx->h_slots.as<int>();
+    L.h_q.reserve(sizeof(float) * static_cast<size_t>(T_pad) * m_pad);
+    L.h_order.reserve(sizeof(int) * static_cast<size_t>(T) * nblk);
+    L.h_slots.reserve(sizeof(int) * T);
+    float *hq = L.h_q.as<float>();
+    int *ho = L.h_order.as<int>();
+    int *hslots = L.h_slots.as<int>();
     std::memset(hq, 0, sizeof(float) * static_cast<size_t>(T_pad) * m_pad);
     std::memset(ho, 0, sizeof(int) * static_cast<size_t>(T) * nblk);
     g.htp.assign(T_pad, TemplParam{});
@@ -457,7 +500,7 @@ void prepare_group(tm_ctx *ctx, int m, const std::vector<int> &idx, const tm_req
         g.htp[t].thr_ed = -FLT_MAX;
         g.htp[t].m = m;
     }
-    cudaStream_t s = ctx->stream;
+    cudaStream_t s = L.stream;
     g.q.reserve(sizeof(float) * static_cast<size_t>(T_pad) * m_pad);
     g.order.reserve(sizeof(int) * static_cast<size_t>(T) * nblk);
     g.tp.reserve(sizeof(TemplParam) * T_pad);
@@ -472,8 +515,8 @@ void prepare_group(tm_ctx *ctx, int m, const std::vector<int> &idx, const tm_req
         // BF16 halves for the tensor-core kernel: q = hi + lo (round to nearest even)
         g.t_rows = (T + 127) & ~127;
         const size_t elems = static_cast<size_t>(g.t_rows) * m_pad;
-        ctx->h_split.reserve(2 * sizeof(uint16_t) * elems);
-        uint16_t *hh = ctx->h_split.as<uint16_t>(), *hl = hh + elems;
+        L.h_split.reserve(2 * sizeof(uint16_t) * elems);
+        uint16_t *hh = L.h_split.as<uint16_t>(), *hl = hh + elems;
         std::memset(hh, 0, 2 * sizeof(uint16_t) * elems);
         for (int t = 0; t < T; t++)
             for (int i = 0; i < m; i++)
@@ -496,11 +539,11 @@ void prepare_group(tm_ctx *ctx, int m, const std::vector<int> &idx, const tm_req
 }
 
 // Resident FP64 prefix sums and constant-run lengths of the waveform (built once).
-void ensure_prefix(tm_ctx *ctx)
+void ensure_prefix(tm_ctx *ctx, Lane &L)
 {
     if (ctx->prefix_ready)
         return;
-    cudaStream_t s = ctx->stream;
+    cudaStream_t s = L.stream;
     const uint64_t n = ctx->n;
     const uint64_t chunks = (n + 8191) / 8192;
     // zero tail: the contraction kernels read window-end sums in fixed-size chunks that may
@@ -521,7 +564,7 @@ void ensure_prefix(tm_ctx *ctx)
     TM_CUDA(tmb::launch_prefix(ctx->clean.as<float>(), n, ctx->center, totals.as<double2>(),
                                ctx->prefix.as<double2>(), ctx->run.as<uint16_t>(), run_tmp.as<uint16_t>(), s));
     TM_CUDA(cudaStreamSynchronize(s));
-    count_launch(ctx, 2 * 16);
+    count_launch(L, 2 * 16);
     totals.release();
     run_tmp.release();
     ctx->prefix_ready = true;
@@ -532,7 +575,7 @@ void ensure_prefix(tm_ctx *ctx)
 // one (padding rows are inert); a tile's K extent is its longest template (shorter rows
 // are zero-padded, which leaves their dot products unchanged). Rows are the template
 // slots of the group: g.index[row] is the request (-1 for padding rows).
-void prepare_group_mixed(tm_ctx *ctx, const std::vector<int> &idx_in, const tm_request *reqs, GroupPlan &g,
+void prepare_group_mixed(tm_ctx *ctx, Lane &L, const std::vector<int> &idx_in, const tm_request *reqs, GroupPlan &g,
                          uint64_t &h2d)
 {
     std::vector<int> idx = idx_in;
@@ -583,14 +626,14 @@ void prepare_group_mixed(tm_ctx *ctx, const std::vector<int> &idx_in, const tm_r
     g.index = rows;
     const int stride = g.k_stride, nblk = g.nblk;
     const size_t elems = static_cast<size_t>(R) * stride;
-    ctx->h_q.reserve(sizeof(float) * elems);
-    ctx->h_order.reserve(sizeof(int) * static_cast<size_t>(R) * nblk);
-    ctx->h_slots.reserve(sizeof(int) * R);
-    ctx->h_split.reserve(2 * sizeof(uint16_t) * elems);
-    float *hq = ctx->h_q.as<float>();
-    int *ho = ctx->h_order.as<int>();
-    int *hslots = ctx->h_slots.as<int>();
-    uint16_t *hh = ctx->h_split.as<uint16_t>(), *hl = hh + elems;
+    L.h_q.reserve(sizeof(float) * elems);
+    L.h_order.reserve(sizeof(int) * static_cast<size_t>(R) * nblk);
+    L.h_slots.reserve(sizeof(int) * R);
+    L.h_split.reserve(2 * sizeof(uint16_t) * elems);
+    float *hq = L.h_q.as<float>();
+    int *ho = L.h_order.as<int>();
+    int *hslots = L.h_slots.as<int>();
+    uint16_t *hh = L.h_split.as<uint16_t>(), *hl = hh + elems;
     std::memset(hq, 0, sizeof(float) * elems);
     std::memset(ho, 0, sizeof(int) * static_cast<size_t>(R) * nblk);
     std::memset(hh, 0, 2 * sizeof(uint16_t) * elems);
@@ -662,7 +705,7 @@ void prepare_group_mixed(tm_ctx *ctx, const std::vector<int> &idx_in, const tm_r
             ti.inv_m[d] = 1.0 / static_cast<double>(ti.len[d]);
         }
     g.tiles = tiles;
-    cudaStream_t s = ctx->stream;
+    cudaStream_t s = L.stream;
     g.q.reserve(sizeof(float) * elems);
     g.order.reserve(sizeof(int) * static_cast<size_t>(R) * nblk);
     g.tp.reserve(sizeof(TemplParam) * R);
@@ -685,9 +728,9 @@ void prepare_group_mixed(tm_ctx *ctx, const std::vector<int> &idx_in, const tm_r
 }
 
 // A pinned block of at least `need` bytes that no result holds, from the pool or new.
-std::shared_ptr<PinnedBlock> acquire_block(tm_ctx *ctx, size_t need)
+std::shared_ptr<PinnedBlock> acquire_block(Lane &L, size_t need)
 {
-    auto &pool = ctx->pool;
+    auto &pool = L.pool;
     for (auto &b : pool)
         if (b.use_count() == 1 && b->bytes >= need)
             return b;
@@ -726,7 +769,7 @@ struct AnswerView
 // windows of distance FLT_MAX (constant windows, which the contraction skips, plus any
 // re-scored to FLT_MAX) follow the finite ones in position order, as in the reference.
 template <class Degenerate>
-void finish_answers(tm_ctx *ctx, const GroupPlan &g, const AnswerView &v, uint64_t w0, tm_result &res,
+void finish_answers(Lane &L, const GroupPlan &g, const AnswerView &v, uint64_t w0, tm_result &res,
                     Degenerate degenerate_windows)
 {
     int slot = -1;
@@ -778,11 +821,11 @@ void finish_answers(tm_ctx *ctx, const GroupPlan &g, const AnswerView &v, uint64
             if (b > a)
             {
                 TM_CUDA(cudaMemcpyAsync(rw.data(), v.d_win + a, sizeof(uint32_t) * (b - a), cudaMemcpyDeviceToHost,
-                                        ctx->stream));
+                                        L.stream));
                 TM_CUDA(cudaMemcpyAsync(rd.data(), v.d_dist + a, sizeof(float) * (b - a), cudaMemcpyDeviceToHost,
-                                        ctx->stream));
-                TM_CUDA(cudaStreamSynchronize(ctx->stream));
-                ctx->d2h_bytes += 8ull * (b - a);
+                                        L.stream));
+                TM_CUDA(cudaStreamSynchronize(L.stream));
+                L.d2h_bytes += 8ull * (b - a);
             }
             std::vector<Hit> finite, infinite;
             for (uint32_t i = 0; i < b - a; i++)
@@ -804,20 +847,20 @@ void finish_answers(tm_ctx *ctx, const GroupPlan &g, const AnswerView &v, uint64
     }
 }
 
-void add_span(tm_ctx *ctx, int phase, cudaEvent_t a, cudaEvent_t b)
+void add_span(Lane &L, int phase, cudaEvent_t a, cudaEvent_t b)
 {
     float ms = 0.0f;
     TM_CUDA(cudaEventElapsedTime(&ms, a, b));
-    ctx->phase_ms[phase] += ms;
+    L.phase_ms[phase] += ms;
 }
 
 // Exact re-scoring of a group's ncand candidates, answer order and kNN selection on the
 // device, one copy to a pinned block that the result keeps, canonical answers.
 template <class Degenerate>
-void rescore_and_answer(tm_ctx *ctx, const GroupPlan &g, uint32_t ncand, uint64_t w0, tm_result &res,
+void rescore_and_answer(tm_ctx *ctx, Lane &L, const GroupPlan &g, uint32_t ncand, uint64_t w0, tm_result &res,
                         Degenerate degenerate_windows)
 {
-    cudaStream_t s = ctx->stream;
+    cudaStream_t s = L.stream;
     const int T = g.T, nk = g.nk;
     int kcap = 1;
     for (int t = 0; t < T; t++)
@@ -825,61 +868,61 @@ void rescore_and_answer(tm_ctx *ctx, const GroupPlan &g, uint32_t ncand, uint64_
             kcap = std::max(kcap, g.k[t]);
     const bool device_knn = nk > 0 && kcap <= kMaxDeviceK;
     const size_t cn = std::max<uint32_t>(ncand, 1);
-    ctx->dist.reserve(sizeof(float) * cn);
-    ctx->akeys.reserve(2 * sizeof(unsigned long long) * cn);
-    ctx->avals.reserve(2 * sizeof(float) * cn);
+    L.dist.reserve(sizeof(float) * cn);
+    L.akeys.reserve(2 * sizeof(unsigned long long) * cn);
+    L.avals.reserve(2 * sizeof(float) * cn);
     if (nk > 0)
-        ctx->avals64.reserve(2 * sizeof(unsigned long long) * cn);
-    ctx->segs.reserve(sizeof(uint32_t) * (2 * static_cast<size_t>(std::max(T, 1)) +
+        L.avals64.reserve(2 * sizeof(unsigned long long) * cn);
+    L.segs.reserve(sizeof(uint32_t) * (2 * static_cast<size_t>(std::max(T, 1)) +
                                           (device_knn ? static_cast<size_t>(nk) * (1 + 2 * kcap) : 0)));
-    uint32_t *hc = ctx->h_counters.as<uint32_t>();
-    uint32_t *d_kept = ctx->counters.as<uint32_t>() + 3;
-    if (ctx->profile)
-        TM_CUDA(cudaEventRecord(ctx->ev2, s));
-    TM_CUDA(tmb::launch_rescore(ctx->cand.as<Candidate>(), ncand, g.tp.as<TemplParam>(), g.q.as<float>(),
-                                g.order.as<int>(), ctx->raw.as<float>(), w0, ctx->dist.as<float>(), s));
+    uint32_t *hc = L.h_counters.as<uint32_t>();
+    uint32_t *d_kept = L.counters.as<uint32_t>() + 3;
+    if (L.profile)
+        TM_CUDA(cudaEventRecord(L.ev2, s));
+    TM_CUDA(tmb::launch_rescore(L.cand.as<Candidate>(), ncand, g.tp.as<TemplParam>(), g.q.as<float>(),
+                                g.order.as<int>(), ctx->raw.as<float>(), w0, L.dist.as<float>(), s));
     if (ncand > 0)
-        count_launch(ctx);
-    if (ctx->profile)
-        TM_CUDA(cudaEventRecord(ctx->ev3, s));
-    unsigned long long *keys[2] = {ctx->akeys.as<unsigned long long>(), ctx->akeys.as<unsigned long long>() + cn};
-    float *vals32[2] = {ctx->avals.as<float>(), ctx->avals.as<float>() + cn};
-    unsigned long long *vals64[2] = {ctx->avals64.as<unsigned long long>(),
-                                     ctx->avals64.as<unsigned long long>() + (nk > 0 ? cn : 0)};
+        count_launch(L);
+    if (L.profile)
+        TM_CUDA(cudaEventRecord(L.ev3, s));
+    unsigned long long *keys[2] = {L.akeys.as<unsigned long long>(), L.akeys.as<unsigned long long>() + cn};
+    float *vals32[2] = {L.avals.as<float>(), L.avals.as<float>() + cn};
+    unsigned long long *vals64[2] = {L.avals64.as<unsigned long long>(),
+                                     L.avals64.as<unsigned long long>() + (nk > 0 ? cn : 0)};
     TM_CUDA(cudaMemsetAsync(d_kept, 0, 2 * sizeof(uint32_t), s));
-    TM_CUDA(tmb::launch_answer_keys(ctx->cand.as<Candidate>(), ctx->dist.as<float>(), ncand, g.tp.as<TemplParam>(),
+    TM_CUDA(tmb::launch_answer_keys(L.cand.as<Candidate>(), L.dist.as<float>(), ncand, g.tp.as<TemplParam>(),
                                     keys[0], vals32[0], d_kept, s));
     TM_CUDA(cudaMemcpyAsync(hc + 3, d_kept, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     TM_CUDA(cudaStreamSynchronize(s));
     if (ncand > 0)
-        count_launch(ctx);
+        count_launch(L);
     const uint32_t kept = hc[3], knn_kept = hc[4], thr_kept = kept - knn_kept;
     const size_t scratch = tmb::answer_sort_scratch(kept, T);
-    ctx->sort_tmp.reserve(scratch);
-    uint32_t *d_start = ctx->segs.as<uint32_t>(), *d_end = d_start + T;
+    L.sort_tmp.reserve(scratch);
+    uint32_t *d_start = L.segs.as<uint32_t>(), *d_end = d_start + T;
     uint32_t *d_knn_n = d_end + T, *d_knn_win = d_knn_n + nk;
     float *d_knn_dist = reinterpret_cast<float *>(d_knn_win + static_cast<size_t>(nk) * kcap);
-    uint32_t *d_win = reinterpret_cast<uint32_t *>(ctx->cand.p); // the candidates are consumed: reuse
-    float *d_dist = ctx->dist.as<float>();                       // likewise the re-scored distances
+    uint32_t *d_win = reinterpret_cast<uint32_t *>(L.cand.p); // the candidates are consumed: reuse
+    float *d_dist = L.dist.as<float>();                       // likewise the re-scored distances
     TM_CUDA(cudaMemsetAsync(d_start, 0, 2 * sizeof(uint32_t) * T, s));
-    TM_CUDA(tmb::launch_answer_order(keys, vals32, vals64, kept, knn_kept, g.tp.as<TemplParam>(), T, ctx->sort_tmp.p,
+    TM_CUDA(tmb::launch_answer_order(keys, vals32, vals64, kept, knn_kept, g.tp.as<TemplParam>(), T, L.sort_tmp.p,
                                      scratch, d_start, d_end, d_win, d_dist, s));
     if (kept > 0)
-        count_launch(ctx, knn_kept > 0 ? 4 : 2); // each radix sort counted as one launch
+        count_launch(L, knn_kept > 0 ? 4 : 2); // each radix sort counted as one launch
     if (device_knn)
     {
         TM_CUDA(tmb::launch_select_knn(g.slots.as<int>(), nk, g.tp.as<TemplParam>(), d_start, d_end, d_win, d_dist,
                                        kcap, d_knn_n, d_knn_win, d_knn_dist, s));
-        count_launch(ctx);
+        count_launch(L);
     }
-    if (ctx->profile)
-        TM_CUDA(cudaEventRecord(ctx->ev4, s));
+    if (L.profile)
+        TM_CUDA(cudaEventRecord(L.ev4, s));
 
     // block layout: win[thr_kept] | dist[thr_kept] | start[T] | end[T] | tkey[T] |
     //               knn_n[nk] | knn_win[nk * kcap] | knn_dist[nk * kcap]
     const size_t knn_words = device_knn ? static_cast<size_t>(nk) * (1 + 2 * kcap) : 0;
     std::shared_ptr<PinnedBlock> block = acquire_block(
-        ctx, sizeof(uint32_t) * (2 * static_cast<size_t>(thr_kept) + 3 * static_cast<size_t>(T) + knn_words) + 64);
+        L, sizeof(uint32_t) * (2 * static_cast<size_t>(thr_kept) + 3 * static_cast<size_t>(T) + knn_words) + 64);
     AnswerView v;
     v.win = static_cast<uint32_t *>(block->p);
     v.dist = reinterpret_cast<float *>(v.win + thr_kept);
@@ -893,24 +936,24 @@ void rescore_and_answer(tm_ctx *ctx, const GroupPlan &g, uint32_t ncand, uint64_
     }
     TM_CUDA(cudaMemcpyAsync(h_start, d_start, 2 * sizeof(uint32_t) * T, cudaMemcpyDeviceToHost, s));
     if (nk > 0)
-        TM_CUDA(cudaMemcpyAsync(h_tkey, ctx->tkey.p, sizeof(uint32_t) * T, cudaMemcpyDeviceToHost, s));
+        TM_CUDA(cudaMemcpyAsync(h_tkey, L.tkey.p, sizeof(uint32_t) * T, cudaMemcpyDeviceToHost, s));
     else
         std::fill(h_tkey, h_tkey + T, 0u);
     if (device_knn)
         TM_CUDA(cudaMemcpyAsync(h_knn, d_knn_n, sizeof(uint32_t) * knn_words, cudaMemcpyDeviceToHost, s));
-    if (ctx->profile)
-        TM_CUDA(cudaEventRecord(ctx->ev1, s));
+    if (L.profile)
+        TM_CUDA(cudaEventRecord(L.ev1, s));
     TM_CUDA(cudaStreamSynchronize(s));
-    ctx->last_candidates += ncand;
-    ctx->d2h_bytes += sizeof(uint32_t) * (2 * static_cast<uint64_t>(thr_kept) + 2 * static_cast<uint64_t>(T) +
+    L.last_candidates += ncand;
+    L.d2h_bytes += sizeof(uint32_t) * (2 * static_cast<uint64_t>(thr_kept) + 2 * static_cast<uint64_t>(T) +
                                           (nk > 0 ? T : 0) + knn_words) +
                       16;
     const auto t0 = std::chrono::steady_clock::now();
-    if (ctx->profile)
+    if (L.profile)
     {
-        add_span(ctx, 2, ctx->ev2, ctx->ev3);
-        add_span(ctx, 3, ctx->ev3, ctx->ev4);
-        add_span(ctx, 4, ctx->ev4, ctx->ev1);
+        add_span(L, 2, L.ev2, L.ev3);
+        add_span(L, 3, L.ev3, L.ev4);
+        add_span(L, 4, L.ev4, L.ev1);
     }
     v.start = h_start;
     v.end = h_start + T;
@@ -923,16 +966,16 @@ void rescore_and_answer(tm_ctx *ctx, const GroupPlan &g, uint32_t ncand, uint64_
     v.d_win = d_win;
     v.d_dist = d_dist;
     res.blocks.push_back(block);
-    finish_answers(ctx, g, v, w0, res, degenerate_windows);
-    if (ctx->profile)
-        ctx->phase_ms[5] += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    finish_answers(L, g, v, w0, res, degenerate_windows);
+    if (L.profile)
+        L.phase_ms[5] += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
 // Device pipeline and selection for one prepared group; writes answers[index].
-void execute_group(tm_ctx *ctx, GroupPlan &g, tm_result &res)
+void execute_group(tm_ctx *ctx, Lane &L, GroupPlan &g, tm_result &res)
 {
     const int m = g.m;
-    LengthStats &ls = ensure_length(ctx, m);
+    LengthStats &ls = ensure_length(ctx, L, m);
     const int T = g.T, T_pad = g.T_pad, m_pad = g.m_pad, nk = g.nk;
     const uint64_t w0 = ls.w0, W = ls.W;
     if (W == 0)
@@ -945,7 +988,7 @@ void execute_group(tm_ctx *ctx, GroupPlan &g, tm_result &res)
     }
     if (W >= (1ull << 32))
         throw Failure{TM_ERR_ARGUMENT, "more than 2^32 - 1 windows in one range; split the range"};
-    cudaStream_t s = ctx->stream;
+    cudaStream_t s = L.stream;
     const bool use_umma = ctx->kernel != TM_KERNEL_FP32 && g.t_rows > 0 && tmb::umma_supported(m, T, W);
     if (ctx->kernel == TM_KERNEL_SPLIT_BF16 && !use_umma)
         throw Failure{TM_ERR_STATE, "split-BF16 kernel not available for this request group"};
@@ -956,29 +999,29 @@ void execute_group(tm_ctx *ctx, GroupPlan &g, tm_result &res)
         TM_CUDA(cudaMemcpyAsync(g.tp.p, g.htp.data(), sizeof(TemplParam) * T_pad, cudaMemcpyHostToDevice, s));
         g.umma_constants = use_umma;
     }
-    ctx->tkey.reserve(sizeof(uint32_t) * T);
+    L.tkey.reserve(sizeof(uint32_t) * T);
 
     const uint32_t nb = static_cast<uint32_t>((W + tmb::kBucket - 1) / tmb::kBucket);
     if (nk > 0)
     {
-        ctx->bmin_u.reserve(sizeof(uint32_t) * static_cast<size_t>(T) * nb);
-        ctx->bmin_l.reserve(sizeof(uint32_t) * static_cast<size_t>(T) * nb);
+        L.bmin_u.reserve(sizeof(uint32_t) * static_cast<size_t>(T) * nb);
+        L.bmin_l.reserve(sizeof(uint32_t) * static_cast<size_t>(T) * nb);
     }
-    ctx->counters.reserve(8 * sizeof(uint32_t));
-    ctx->h_counters.reserve(8 * sizeof(uint32_t));
-    uint32_t *hc = ctx->h_counters.as<uint32_t>();
+    L.counters.reserve(8 * sizeof(uint32_t));
+    L.h_counters.reserve(8 * sizeof(uint32_t));
+    uint32_t *hc = L.h_counters.as<uint32_t>();
 
     uint32_t ncand = 0;
     for (int attempt = 0; attempt < 3; attempt++)
     {
-        ctx->cand.reserve(sizeof(Candidate) * static_cast<size_t>(ctx->cand_cap));
+        L.cand.reserve(sizeof(Candidate) * static_cast<size_t>(L.cand_cap));
         if (nk > 0)
         {
-            TM_CUDA(cudaMemsetAsync(ctx->bmin_u.p, 0xff, sizeof(uint32_t) * static_cast<size_t>(T) * nb, s));
-            TM_CUDA(cudaMemsetAsync(ctx->bmin_l.p, 0xff, sizeof(uint32_t) * static_cast<size_t>(T) * nb, s));
+            TM_CUDA(cudaMemsetAsync(L.bmin_u.p, 0xff, sizeof(uint32_t) * static_cast<size_t>(T) * nb, s));
+            TM_CUDA(cudaMemsetAsync(L.bmin_l.p, 0xff, sizeof(uint32_t) * static_cast<size_t>(T) * nb, s));
         }
-        TM_CUDA(cudaMemsetAsync(ctx->counters.p, 0, 4 * sizeof(uint32_t), s));
-        uint32_t *d_cand_count = ctx->counters.as<uint32_t>();
+        TM_CUDA(cudaMemsetAsync(L.counters.p, 0, 4 * sizeof(uint32_t), s));
+        uint32_t *d_cand_count = L.counters.as<uint32_t>();
         uint32_t *d_list_count = d_cand_count + 1;
 
         tmb::ScanArgs a{};
@@ -991,85 +1034,85 @@ void execute_group(tm_ctx *ctx, GroupPlan &g, tm_result &res)
         a.W = static_cast<uint32_t>(W);
         a.m_pad = m_pad;
         a.T = T;
-        a.bmin_u = ctx->bmin_u.as<uint32_t>();
-        a.bmin_l = ctx->bmin_l.as<uint32_t>();
+        a.bmin_u = L.bmin_u.as<uint32_t>();
+        a.bmin_l = L.bmin_l.as<uint32_t>();
         a.nb = nb;
-        a.cand = ctx->cand.as<Candidate>();
+        a.cand = L.cand.as<Candidate>();
         a.cand_count = d_cand_count;
-        a.cand_cap = ctx->cand_cap;
+        a.cand_cap = L.cand_cap;
         a.q_hi = g.q_hi.p;
         a.q_lo = g.q_lo.p;
         a.t_rows = g.t_rows;
         a.err = reinterpret_cast<int *>(d_cand_count + 2);
 
         // 2. contraction with fused epilogue
-        if (ctx->profile)
-            TM_CUDA(cudaEventRecord(ctx->ev0, s));
+        if (L.profile)
+            TM_CUDA(cudaEventRecord(L.ev0, s));
         if (use_umma)
             TM_CUDA(tmb::launch_scan_umma(a, s));
         else
             TM_CUDA(tmb::launch_scan_fp32(a, s));
-        count_launch(ctx);
-        if (ctx->profile)
+        count_launch(L);
+        if (L.profile)
         {
-            TM_CUDA(cudaEventRecord(ctx->ev1, s));
-            TM_CUDA(cudaEventSynchronize(ctx->ev1));
+            TM_CUDA(cudaEventRecord(L.ev1, s));
+            TM_CUDA(cudaEventSynchronize(L.ev1));
             float ms = 0.0f;
-            TM_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-            ctx->kname = use_umma ? "k_scan_umma" : "k_scan_fp32";
-            ctx->prof_launches++;
-            ctx->prof_ms += ms;
-            ctx->phase_ms[0] += ms;
-            ctx->prof_flops += 2.0 * m * static_cast<double>(W) * T;
+            TM_CUDA(cudaEventElapsedTime(&ms, L.ev0, L.ev1));
+            L.kname = use_umma ? "k_scan_umma" : "k_scan_fp32";
+            L.prof_launches++;
+            L.prof_ms += ms;
+            L.phase_ms[0] += ms;
+            L.prof_flops += 2.0 * m * static_cast<double>(W) * T;
         }
 
         // 3. kNN bound, bucket list, FP32 re-pass
         if (nk > 0)
         {
-            TM_CUDA(tmb::launch_bucket_select(ctx->bmin_u.as<uint32_t>(), nb, g.tp.as<TemplParam>(),
-                                              g.slots.as<int>(), nk, ctx->tkey.as<uint32_t>(), s));
+            TM_CUDA(tmb::launch_bucket_select(L.bmin_u.as<uint32_t>(), nb, g.tp.as<TemplParam>(),
+                                              g.slots.as<int>(), nk, L.tkey.as<uint32_t>(), s));
             for (int la = 0; la < 3; la++)
             {
-                ctx->list.reserve(sizeof(uint2) * static_cast<size_t>(ctx->list_cap));
+                L.list.reserve(sizeof(uint2) * static_cast<size_t>(L.list_cap));
                 TM_CUDA(cudaMemsetAsync(d_list_count, 0, sizeof(uint32_t), s));
-                TM_CUDA(tmb::launch_list_buckets(ctx->bmin_l.as<uint32_t>(), nb, g.slots.as<int>(), nk,
-                                                 ctx->tkey.as<uint32_t>(), ctx->list.as<uint2>(), d_list_count,
-                                                 ctx->list_cap, s));
+                TM_CUDA(tmb::launch_list_buckets(L.bmin_l.as<uint32_t>(), nb, g.slots.as<int>(), nk,
+                                                 L.tkey.as<uint32_t>(), L.list.as<uint2>(), d_list_count,
+                                                 L.list_cap, s));
                 TM_CUDA(cudaMemcpyAsync(hc + 1, d_list_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
                 TM_CUDA(cudaStreamSynchronize(s));
-                count_launch(ctx, 2);
-                if (hc[1] <= ctx->list_cap)
+                count_launch(L, 2);
+                if (hc[1] <= L.list_cap)
                     break;
-                ctx->list_cap = hc[1] + hc[1] / 2;
+                L.list_cap = hc[1] + hc[1] / 2;
             }
-            if (hc[1] > ctx->list_cap)
+            if (hc[1] > L.list_cap)
                 throw Failure{TM_ERR_NO_MEMORY, "bucket list overflow"};
-            TM_CUDA(tmb::launch_passb(ctx->list.as<uint2>(), hc[1], ctx->clean.as<float>(), g.q.as<float>(),
+            TM_CUDA(tmb::launch_passb(L.list.as<uint2>(), hc[1], ctx->clean.as<float>(), g.q.as<float>(),
                                       g.tp.as<TemplParam>(), ls.mean.as<float>(), ls.inv.as<float>(),
-                                      ctx->tkey.as<uint32_t>(), w0, static_cast<uint32_t>(W),
-                                      ctx->cand.as<Candidate>(), d_cand_count, ctx->cand_cap, s));
+                                      L.tkey.as<uint32_t>(), w0, static_cast<uint32_t>(W),
+                                      L.cand.as<Candidate>(), d_cand_count, L.cand_cap, s));
             if (hc[1] > 0)
-                count_launch(ctx);
+                count_launch(L);
         }
-        if (ctx->profile)
-            TM_CUDA(cudaEventRecord(ctx->ev2, s));
+        if (L.profile)
+            TM_CUDA(cudaEventRecord(L.ev2, s));
         TM_CUDA(cudaMemcpyAsync(hc, d_cand_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
         TM_CUDA(cudaMemcpyAsync(hc + 2, d_cand_count + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
         TM_CUDA(cudaStreamSynchronize(s));
-        if (ctx->profile)
-            add_span(ctx, 1, ctx->ev1, ctx->ev2);
+        if (L.profile)
+            add_span(L, 1, L.ev1, L.ev2);
         if (hc[2] != 0)
             throw Failure{TM_ERR_TIMEOUT, "contraction kernel gave up waiting (code " + std::to_string(hc[2]) + ")"};
         ncand = hc[0];
-        if (ncand <= ctx->cand_cap)
+        if (ncand <= L.cand_cap)
             break;
-        ctx->cand_cap = ncand + ncand / 2;
+        L.cand_cap = ncand + ncand / 2;
         if (attempt == 2)
             throw Failure{TM_ERR_NO_MEMORY, "candidate buffer overflow"};
     }
 
     std::vector<uint8_t> flags; // fetched only when some kNN bound is unbounded
-    rescore_and_answer(ctx, g, ncand, w0, res, [&](int, std::vector<Hit> &degenerate) {
+    rescore_and_answer(ctx, L, g, ncand, w0, res, [&](int, std::vector<Hit> &degenerate) {
         if (flags.empty())
         {
             flags.resize(W);
@@ -1082,11 +1125,11 @@ void execute_group(tm_ctx *ctx, GroupPlan &g, tm_result &res)
 }
 
 // Device pipeline for a mixed-length group (tensor-core kernel only).
-void execute_group_mixed(tm_ctx *ctx, GroupPlan &g, tm_result &res)
+void execute_group_mixed(tm_ctx *ctx, Lane &L, GroupPlan &g, tm_result &res)
 {
     if (ctx->kernel == TM_KERNEL_FP32)
         throw Failure{TM_ERR_STATE, "batch of several template lengths was prepared for the tensor-core kernel"};
-    ensure_prefix(ctx);
+    ensure_prefix(ctx, L);
     const int T = g.T, nk = g.nk;
     const uint64_t w0 = ctx->range_first, W = g.w_max;
     if (W == 0)
@@ -1100,17 +1143,17 @@ void execute_group_mixed(tm_ctx *ctx, GroupPlan &g, tm_result &res)
     }
     if (W >= (1ull << 32))
         throw Failure{TM_ERR_ARGUMENT, "more than 2^32 - 1 windows in one range; split the range"};
-    cudaStream_t s = ctx->stream;
-    ctx->tkey.reserve(sizeof(uint32_t) * T);
+    cudaStream_t s = L.stream;
+    L.tkey.reserve(sizeof(uint32_t) * T);
     const uint32_t nb = static_cast<uint32_t>((W + tmb::kBucket - 1) / tmb::kBucket);
     if (nk > 0)
     {
-        ctx->bmin_u.reserve(sizeof(uint32_t) * static_cast<size_t>(T) * nb);
-        ctx->bmin_l.reserve(sizeof(uint32_t) * static_cast<size_t>(T) * nb);
+        L.bmin_u.reserve(sizeof(uint32_t) * static_cast<size_t>(T) * nb);
+        L.bmin_l.reserve(sizeof(uint32_t) * static_cast<size_t>(T) * nb);
     }
-    ctx->counters.reserve(8 * sizeof(uint32_t));
-    ctx->h_counters.reserve(8 * sizeof(uint32_t));
-    uint32_t *hc = ctx->h_counters.as<uint32_t>();
+    L.counters.reserve(8 * sizeof(uint32_t));
+    L.h_counters.reserve(8 * sizeof(uint32_t));
+    uint32_t *hc = L.h_counters.as<uint32_t>();
     double flops = 0.0;
     for (int t = 0; t < T; t++)
         flops += 2.0 * g.htp[t].m * static_cast<double>(g.htp[t].wcount);
@@ -1118,14 +1161,14 @@ void execute_group_mixed(tm_ctx *ctx, GroupPlan &g, tm_result &res)
     uint32_t ncand = 0;
     for (int attempt = 0; attempt < 3; attempt++)
     {
-        ctx->cand.reserve(sizeof(Candidate) * static_cast<size_t>(ctx->cand_cap));
+        L.cand.reserve(sizeof(Candidate) * static_cast<size_t>(L.cand_cap));
         if (nk > 0)
         {
-            TM_CUDA(cudaMemsetAsync(ctx->bmin_u.p, 0xff, sizeof(uint32_t) * static_cast<size_t>(T) * nb, s));
-            TM_CUDA(cudaMemsetAsync(ctx->bmin_l.p, 0xff, sizeof(uint32_t) * static_cast<size_t>(T) * nb, s));
+            TM_CUDA(cudaMemsetAsync(L.bmin_u.p, 0xff, sizeof(uint32_t) * static_cast<size_t>(T) * nb, s));
+            TM_CUDA(cudaMemsetAsync(L.bmin_l.p, 0xff, sizeof(uint32_t) * static_cast<size_t>(T) * nb, s));
         }
-        TM_CUDA(cudaMemsetAsync(ctx->counters.p, 0, 4 * sizeof(uint32_t), s));
-        uint32_t *d_cand_count = ctx->counters.as<uint32_t>();
+        TM_CUDA(cudaMemsetAsync(L.counters.p, 0, 4 * sizeof(uint32_t), s));
+        uint32_t *d_cand_count = L.counters.as<uint32_t>();
         uint32_t *d_list_count = d_cand_count + 1;
         tmb::ScanArgs a{};
         a.x = ctx->clean.as<float>();
@@ -1135,12 +1178,12 @@ void execute_group_mixed(tm_ctx *ctx, GroupPlan &g, tm_result &res)
         a.W = static_cast<uint32_t>(W);
         a.m_pad = g.k_stride;
         a.T = T;
-        a.bmin_u = ctx->bmin_u.as<uint32_t>();
-        a.bmin_l = ctx->bmin_l.as<uint32_t>();
+        a.bmin_u = L.bmin_u.as<uint32_t>();
+        a.bmin_l = L.bmin_l.as<uint32_t>();
         a.nb = nb;
-        a.cand = ctx->cand.as<Candidate>();
+        a.cand = L.cand.as<Candidate>();
         a.cand_count = d_cand_count;
-        a.cand_cap = ctx->cand_cap;
+        a.cand_cap = L.cand_cap;
         a.q_hi = g.q_hi.p;
         a.q_lo = g.q_lo.p;
         a.t_rows = g.t_rows;
@@ -1152,69 +1195,69 @@ void execute_group_mixed(tm_ctx *ctx, GroupPlan &g, tm_result &res)
         a.tiles = g.d_tiles.as<tmb::TileInfo>();
         a.k_stride = g.k_stride;
         a.n = ctx->n;
-        if (ctx->profile)
-            TM_CUDA(cudaEventRecord(ctx->ev0, s));
+        if (L.profile)
+            TM_CUDA(cudaEventRecord(L.ev0, s));
         TM_CUDA(tmb::launch_scan_umma(a, s));
-        count_launch(ctx);
-        if (ctx->profile)
+        count_launch(L);
+        if (L.profile)
         {
-            TM_CUDA(cudaEventRecord(ctx->ev1, s));
-            TM_CUDA(cudaEventSynchronize(ctx->ev1));
+            TM_CUDA(cudaEventRecord(L.ev1, s));
+            TM_CUDA(cudaEventSynchronize(L.ev1));
             float ms = 0.0f;
-            TM_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-            ctx->kname = "k_scan_umma";
-            ctx->prof_launches++;
-            ctx->prof_ms += ms;
-            ctx->phase_ms[0] += ms;
-            ctx->prof_flops += flops;
+            TM_CUDA(cudaEventElapsedTime(&ms, L.ev0, L.ev1));
+            L.kname = "k_scan_umma";
+            L.prof_launches++;
+            L.prof_ms += ms;
+            L.phase_ms[0] += ms;
+            L.prof_flops += flops;
         }
         if (nk > 0)
         {
-            TM_CUDA(tmb::launch_bucket_select(ctx->bmin_u.as<uint32_t>(), nb, g.tp.as<TemplParam>(),
-                                              g.slots.as<int>(), nk, ctx->tkey.as<uint32_t>(), s));
+            TM_CUDA(tmb::launch_bucket_select(L.bmin_u.as<uint32_t>(), nb, g.tp.as<TemplParam>(),
+                                              g.slots.as<int>(), nk, L.tkey.as<uint32_t>(), s));
             for (int la = 0; la < 3; la++)
             {
-                ctx->list.reserve(sizeof(uint2) * static_cast<size_t>(ctx->list_cap));
+                L.list.reserve(sizeof(uint2) * static_cast<size_t>(L.list_cap));
                 TM_CUDA(cudaMemsetAsync(d_list_count, 0, sizeof(uint32_t), s));
-                TM_CUDA(tmb::launch_list_buckets(ctx->bmin_l.as<uint32_t>(), nb, g.slots.as<int>(), nk,
-                                                 ctx->tkey.as<uint32_t>(), ctx->list.as<uint2>(), d_list_count,
-                                                 ctx->list_cap, s));
+                TM_CUDA(tmb::launch_list_buckets(L.bmin_l.as<uint32_t>(), nb, g.slots.as<int>(), nk,
+                                                 L.tkey.as<uint32_t>(), L.list.as<uint2>(), d_list_count,
+                                                 L.list_cap, s));
                 TM_CUDA(cudaMemcpyAsync(hc + 1, d_list_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
                 TM_CUDA(cudaStreamSynchronize(s));
-                count_launch(ctx, 2);
-                if (hc[1] <= ctx->list_cap)
+                count_launch(L, 2);
+                if (hc[1] <= L.list_cap)
                     break;
-                ctx->list_cap = hc[1] + hc[1] / 2;
+                L.list_cap = hc[1] + hc[1] / 2;
             }
-            if (hc[1] > ctx->list_cap)
+            if (hc[1] > L.list_cap)
                 throw Failure{TM_ERR_NO_MEMORY, "bucket list overflow"};
-            TM_CUDA(tmb::launch_passb_mixed(ctx->list.as<uint2>(), hc[1], ctx->clean.as<float>(),
+            TM_CUDA(tmb::launch_passb_mixed(L.list.as<uint2>(), hc[1], ctx->clean.as<float>(),
                                             ctx->raw.as<float>(), ctx->prefix.as<double2>(), ctx->run.as<uint16_t>(),
                                             ctx->center, g.q.as<float>(), g.tp.as<TemplParam>(),
-                                            ctx->tkey.as<uint32_t>(), w0, ctx->cand.as<Candidate>(), d_cand_count,
-                                            ctx->cand_cap, s));
+                                            L.tkey.as<uint32_t>(), w0, L.cand.as<Candidate>(), d_cand_count,
+                                            L.cand_cap, s));
             if (hc[1] > 0)
-                count_launch(ctx);
+                count_launch(L);
         }
-        if (ctx->profile)
-            TM_CUDA(cudaEventRecord(ctx->ev2, s));
+        if (L.profile)
+            TM_CUDA(cudaEventRecord(L.ev2, s));
         TM_CUDA(cudaMemcpyAsync(hc, d_cand_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
         TM_CUDA(cudaMemcpyAsync(hc + 2, d_cand_count + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
         TM_CUDA(cudaStreamSynchronize(s));
-        if (ctx->profile)
-            add_span(ctx, 1, ctx->ev1, ctx->ev2);
+        if (L.profile)
+            add_span(L, 1, L.ev1, L.ev2);
         if (hc[2] != 0)
             throw Failure{TM_ERR_TIMEOUT, "contraction kernel gave up waiting (code " + std::to_string(hc[2]) + ")"};
         ncand = hc[0];
-        if (ncand <= ctx->cand_cap)
+        if (ncand <= L.cand_cap)
             break;
-        ctx->cand_cap = ncand + ncand / 2;
+        L.cand_cap = ncand + ncand / 2;
         if (attempt == 2)
             throw Failure{TM_ERR_NO_MEMORY, "candidate buffer overflow"};
     }
     std::vector<uint16_t> run;
     std::vector<float> raw;
-    rescore_and_answer(ctx, g, ncand, w0, res, [&](int t, std::vector<Hit> &degenerate) {
+    rescore_and_answer(ctx, L, g, ncand, w0, res, [&](int t, std::vector<Hit> &degenerate) {
         if (run.empty())
         {
             run.resize(W);
@@ -1232,9 +1275,19 @@ void execute_group_mixed(tm_ctx *ctx, GroupPlan &g, tm_result &res)
 // Groups of a batch. Lengths with a full 128-template tile (or any length, on the FP32
 // kernel) get their own group with per-length statistics; the remaining templates of
 // several lengths share one mixed-length group on the tensor cores.
-void create_batch(tm_ctx *ctx, const tm_request *requests, int count, tm_batch &b)
+void create_batch(tm_ctx *ctx, Lane &L, const tm_request *requests, int count, tm_batch &b, bool serving = false)
 {
     b.count = count;
+    if (serving) // one mixed-length group over the resident prefix sums, whatever the lengths
+    {
+        std::vector<int> all(static_cast<size_t>(count));
+        for (int i = 0; i < count; i++)
+            all[i] = i;
+        b.groups.resize(count > 0 ? 1 : 0);
+        if (count > 0)
+            prepare_group_mixed(ctx, L, all, requests, b.groups[0], b.h2d_bytes);
+        return;
+    }
     std::map<int, std::vector<int>> by_m;
     for (int i = 0; i < count; i++)
         by_m[requests[i].m].push_back(i);
@@ -1259,22 +1312,22 @@ void create_batch(tm_ctx *ctx, const tm_request *requests, int count, tm_batch &
     b.groups.resize(single.size() + (rest.empty() ? 0 : 1));
     size_t gi = 0;
     for (auto &kv : single)
-        prepare_group(ctx, kv.first, kv.second, requests, b.groups[gi++], b.h2d_bytes);
+        prepare_group(ctx, L, kv.first, kv.second, requests, b.groups[gi++], b.h2d_bytes);
     if (!rest.empty())
-        prepare_group_mixed(ctx, rest, requests, b.groups[gi++], b.h2d_bytes);
+        prepare_group_mixed(ctx, L, rest, requests, b.groups[gi++], b.h2d_bytes);
 }
 
-void run_batch(tm_ctx *ctx, tm_batch &b, tm_result &res)
+void run_batch(tm_ctx *ctx, Lane &L, tm_batch &b, tm_result &res)
 {
     res.answers.assign(static_cast<size_t>(b.count), Answer());
     res.blocks.clear();
-    ctx->last_candidates = 0;
+    L.last_candidates = 0;
     for (GroupPlan &g : b.groups)
     {
         if (g.mixed)
-            execute_group_mixed(ctx, g, res);
+            execute_group_mixed(ctx, L, g, res);
         else
-            execute_group(ctx, g, res);
+            execute_group(ctx, L, g, res);
     }
 }
 
@@ -1300,6 +1353,185 @@ int validate_requests(const tm_ctx *ctx, const tm_request *reqs, int count)
 
 } // namespace
 
+
+// ---- serving: continuous batching over the resident waveform ------------------------
+//
+// Requests are submitted one at a time from any thread and queue in arrival order.
+// Each worker owns a lane (stream + scratch) and loops: it admits the oldest pending
+// requests, as many as max_batch and the device-memory budget for requests in flight
+// allow (a request larger than the whole budget still runs, alone), prepares them as
+// one mixed-length group over the resident prefix sums, runs it and completes every
+// request of it. While one worker's batch is on the GPU, the others admit what arrived
+// meanwhile and prepare, launch or finish theirs, so batches overlap on the device and
+// with the host work around them. A request's answers are those of the same request
+// run alone: each (template, window) pair is scored, rescored and selected by itself.
+
+struct ServeItem
+{
+    uint64_t ticket = 0;
+    std::vector<float> templ; // owned copy
+    tm_request req{};
+    uint64_t bytes = 0; // admission estimate
+    double submit_ms = 0.0;
+};
+
+struct Server
+{
+    tm_ctx *ctx = nullptr;
+    tm_serve_config cfg{};
+    std::vector<std::unique_ptr<Lane>> lanes;
+    std::vector<std::thread> threads;
+    std::mutex mu;
+    std::condition_variable work_cv, done_cv;
+    std::deque<ServeItem> pending;
+    std::deque<tm_completion> done;
+    uint64_t next_ticket = 1, in_flight_bytes = 0, in_flight = 0, launches = 0;
+    bool stopping = false, stopped = false;
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+
+    double now_ms() const
+    {
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    ~Server()
+    {
+        for (tm_completion &c : done)
+            delete c.result;
+    }
+};
+
+// Device bytes a request holds while in flight: its template row (FP32, two BF16 halves,
+// block order) at up to the longest length a batch can have, plus its share of the
+// candidate, sort and answer buffers: kNN about 2k-1 buckets of windows, threshold a
+// fixed fraction of the windows (an estimate: the buffers grow when a batch needs more).
+static uint64_t serve_bytes(const tm_ctx *ctx, const tm_request &r)
+{
+    const uint64_t W = ctx->n - static_cast<uint64_t>(r.m) + 1;
+    const uint64_t row = 10ull * 16384 + sizeof(TemplParam);
+    const uint64_t cands = r.mode == TM_MODE_KNN ? std::min<uint64_t>(W, (2ull * r.k) * tmb::kBucket / 4)
+                                                 : std::max<uint64_t>(W / 512, 1024);
+    return row + 48ull * cands;
+}
+
+static void serve_worker(Server *sv, Lane *L)
+{
+    tm_ctx *ctx = sv->ctx;
+    cudaSetDevice(ctx->device);
+    // one batch object per worker, its device buffers grown and reused: freeing device
+    // memory would wait for the other lanes' kernels
+    tm_batch b;
+    for (;;)
+    {
+        std::vector<ServeItem> batch;
+        uint64_t bytes = 0;
+        {
+            std::unique_lock<std::mutex> lk(sv->mu);
+            for (;;)
+            {
+                if (sv->pending.empty() && sv->stopping)
+                    return;
+                while (!sv->pending.empty() && static_cast<int>(batch.size()) < sv->cfg.max_batch)
+                {
+                    const uint64_t b = sv->pending.front().bytes;
+                    const bool alone = sv->in_flight_bytes == 0 && batch.empty();
+                    if (!alone && sv->in_flight_bytes + bytes + b > sv->cfg.memory_budget)
+                        break;
+                    bytes += b;
+                    batch.push_back(std::move(sv->pending.front()));
+                    sv->pending.pop_front();
+                }
+                if (!batch.empty())
+                    break;
+                sv->work_cv.wait(lk); // nothing pending, or the budget is full: wait for either to change
+            }
+            sv->in_flight_bytes += bytes;
+            sv->in_flight += batch.size();
+        }
+        const double start = sv->now_ms();
+        std::vector<tm_request> reqs(batch.size());
+        for (size_t i = 0; i < batch.size(); i++)
+        {
+            reqs[i] = batch[i].req;
+            reqs[i].templ = batch[i].templ.data();
+        }
+        auto res = std::make_unique<tm_result>();
+        int code = TM_OK;
+        std::string what;
+        try
+        {
+            b.h2d_bytes = 0;
+            create_batch(ctx, *L, reqs.data(), static_cast<int>(reqs.size()), b, true);
+            run_batch(ctx, *L, b, *res);
+        }
+        catch (const Failure &f)
+        {
+            code = f.code;
+            what = f.what;
+        }
+        catch (const std::bad_alloc &)
+        {
+            code = TM_ERR_NO_MEMORY;
+        }
+        catch (const std::exception &e)
+        {
+            code = TM_ERR_STATE;
+            what = e.what();
+        }
+        const double end = sv->now_ms();
+        std::vector<tm_completion> out(batch.size());
+        for (size_t i = 0; i < batch.size(); i++)
+        {
+            tm_completion &c = out[i];
+            c.ticket = batch[i].ticket;
+            c.status = code;
+            c.result = nullptr;
+            c.submit_ms = batch[i].submit_ms;
+            c.start_ms = start;
+            c.done_ms = end;
+            c.batch_size = static_cast<int>(batch.size());
+            if (code == TM_OK)
+            {
+                // one result per request, sharing the batch's pinned answer blocks
+                auto r = std::make_unique<tm_result>();
+                r->answers.push_back(std::move(res->answers[i]));
+                r->blocks = res->blocks;
+                c.result = r.release();
+            }
+        }
+        {
+            std::lock_guard<std::mutex> lk(sv->mu);
+            sv->in_flight_bytes -= bytes;
+            sv->in_flight -= batch.size();
+            sv->launches += static_cast<uint64_t>(L->all_launches);
+            L->all_launches = 0;
+            for (tm_completion &c : out)
+                sv->done.push_back(c);
+        }
+        sv->done_cv.notify_all();
+        sv->work_cv.notify_all();
+    }
+}
+
+// Completes what was submitted, then joins the workers; completions stay pollable.
+static void stop_server(tm_ctx *ctx)
+{
+    Server *sv = ctx->server.get();
+    if (sv == nullptr || sv->stopped)
+        return;
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        sv->stopping = true;
+    }
+    sv->work_cv.notify_all();
+    for (std::thread &t : sv->threads)
+        t.join();
+    sv->threads.clear();
+    for (auto &L : sv->lanes)
+        L->close();
+    sv->lanes.clear();
+    sv->stopped = true;
+}
+
 // ---------------------------------------------------------------------------------
 extern "C" {
 
@@ -1319,19 +1551,14 @@ int tm_ctx_create(const float *raw, uint64_t n, int device, tm_ctx **out)
     ctx->n = n;
     const int rc = guarded(ctx.get(), [&] {
         TM_CUDA(cudaSetDevice(device));
-        TM_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
-        TM_CUDA(cudaEventCreate(&ctx->ev0));
-        TM_CUDA(cudaEventCreate(&ctx->ev1));
-        TM_CUDA(cudaEventCreate(&ctx->ev2));
-        TM_CUDA(cudaEventCreate(&ctx->ev3));
-        TM_CUDA(cudaEventCreate(&ctx->ev4));
+        ctx->main.open();
         const uint64_t total = n + tmb::kStagePad;
         ctx->raw.reserve(sizeof(float) * total);
         ctx->clean.reserve(sizeof(float) * total);
-        TM_CUDA(cudaMemsetAsync(ctx->raw.p, 0, sizeof(float) * total, ctx->stream));
-        TM_CUDA(cudaMemcpyAsync(ctx->raw.p, raw, sizeof(float) * n, cudaMemcpyHostToDevice, ctx->stream));
-        TM_CUDA(tmb::launch_clean(ctx->raw.as<float>(), ctx->clean.as<float>(), n, total, ctx->stream));
-        TM_CUDA(cudaStreamSynchronize(ctx->stream));
+        TM_CUDA(cudaMemsetAsync(ctx->raw.p, 0, sizeof(float) * total, ctx->main.stream));
+        TM_CUDA(cudaMemcpyAsync(ctx->raw.p, raw, sizeof(float) * n, cudaMemcpyHostToDevice, ctx->main.stream));
+        TM_CUDA(tmb::launch_clean(ctx->raw.as<float>(), ctx->clean.as<float>(), n, total, ctx->main.stream));
+        TM_CUDA(cudaStreamSynchronize(ctx->main.stream));
     });
     if (rc != TM_OK)
     {
@@ -1347,28 +1574,16 @@ int tm_ctx_destroy(tm_ctx *ctx)
     if (ctx == nullptr)
         return TM_OK;
     cudaSetDevice(ctx->device);
-    if (ctx->stream)
-        cudaStreamSynchronize(ctx->stream);
+    stop_server(ctx);
+    ctx->main.close();
     for (auto &kv : ctx->lengths)
     {
         kv.second->mean.release();
         kv.second->inv.release();
         kv.second->flags.release();
     }
-    for (DevBuf *b : {&ctx->prefix, &ctx->run, &ctx->raw, &ctx->clean, &ctx->suf, &ctx->tkey, &ctx->bmin_u,
-                      &ctx->bmin_l, &ctx->list, &ctx->counters, &ctx->cand, &ctx->dist, &ctx->akeys, &ctx->avals,
-                      &ctx->avals64, &ctx->sort_tmp, &ctx->segs})
+    for (DevBuf *b : {&ctx->prefix, &ctx->run, &ctx->raw, &ctx->clean, &ctx->suf})
         b->release();
-    for (HostBuf *b : {&ctx->h_split, &ctx->h_q, &ctx->h_order, &ctx->h_slots, &ctx->h_counters})
-        b->release();
-    ctx->pool.clear(); // blocks still held by results are freed with the last of them
-    if (ctx->ev0)
-        cudaEventDestroy(ctx->ev0);
-    for (cudaEvent_t e : {ctx->ev1, ctx->ev2, ctx->ev3, ctx->ev4})
-        if (e)
-            cudaEventDestroy(e);
-    if (ctx->stream)
-        cudaStreamDestroy(ctx->stream);
     delete ctx;
     return TM_OK;
 }
@@ -1379,6 +1594,8 @@ int tm_set_kernel(tm_ctx *ctx, int kernel)
 {
     if (ctx == nullptr || kernel < TM_KERNEL_AUTO || kernel > TM_KERNEL_SPLIT_BF16)
         return TM_ERR_ARGUMENT;
+    if (ctx->server && !ctx->server->stopped)
+        return TM_ERR_STATE;
     ctx->kernel = kernel;
     return TM_OK;
 }
@@ -1387,9 +1604,11 @@ int tm_set_window_range(tm_ctx *ctx, uint64_t first, uint64_t count)
 {
     if (ctx == nullptr || count == 0)
         return TM_ERR_ARGUMENT;
+    if (ctx->server && !ctx->server->stopped)
+        return TM_ERR_STATE;
     return guarded(ctx, [&] {
         TM_CUDA(cudaSetDevice(ctx->device));
-        TM_CUDA(cudaStreamSynchronize(ctx->stream));
+        TM_CUDA(cudaStreamSynchronize(ctx->main.stream));
         for (auto &kv : ctx->lengths)
         {
             kv.second->mean.release();
@@ -1408,8 +1627,8 @@ int tm_prepare_length(tm_ctx *ctx, int m)
         return TM_ERR_ARGUMENT;
     return guarded(ctx, [&] {
         TM_CUDA(cudaSetDevice(ctx->device));
-        ensure_length(ctx, m);
-        TM_CUDA(cudaStreamSynchronize(ctx->stream));
+        ensure_length(ctx, ctx->main, m);
+        TM_CUDA(cudaStreamSynchronize(ctx->main.stream));
     });
 }
 
@@ -1428,11 +1647,11 @@ int tm_window_stats(tm_ctx *ctx, int m, uint64_t first, uint64_t count, float *m
         dm.reserve(count * sizeof(float));
         ds.reserve(count * sizeof(float));
         TM_CUDA(tmb::launch_reference_stats(ctx->raw.as<float>(), m, first, count, dm.as<float>(), ds.as<float>(),
-                                           ctx->stream));
-        count_launch(ctx);
-        TM_CUDA(cudaMemcpyAsync(mean, dm.p, count * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
-        TM_CUDA(cudaMemcpyAsync(stddev, ds.p, count * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
-        TM_CUDA(cudaStreamSynchronize(ctx->stream));
+                                           ctx->main.stream));
+        count_launch(ctx->main);
+        TM_CUDA(cudaMemcpyAsync(mean, dm.p, count * sizeof(float), cudaMemcpyDeviceToHost, ctx->main.stream));
+        TM_CUDA(cudaMemcpyAsync(stddev, ds.p, count * sizeof(float), cudaMemcpyDeviceToHost, ctx->main.stream));
+        TM_CUDA(cudaStreamSynchronize(ctx->main.stream));
         dm.release();
         ds.release();
     });
@@ -1452,7 +1671,7 @@ int tm_batch_create(tm_ctx *ctx, const tm_request *requests, int count, tm_batch
     auto b = std::make_unique<tm_batch>();
     const int rc = guarded(ctx, [&] {
         TM_CUDA(cudaSetDevice(ctx->device));
-        create_batch(ctx, requests, count, *b);
+        create_batch(ctx, ctx->main, requests, count, *b);
     });
     if (rc == TM_OK)
         *out = b.release();
@@ -1467,7 +1686,7 @@ int tm_batch_run(tm_ctx *ctx, tm_batch *batch, tm_result **out)
     auto res = std::make_unique<tm_result>();
     const int rc = guarded(ctx, [&] {
         TM_CUDA(cudaSetDevice(ctx->device));
-        run_batch(ctx, *batch, *res);
+        run_batch(ctx, ctx->main, *batch, *res);
     });
     if (rc == TM_OK)
         *out = res.release();
@@ -1576,7 +1795,7 @@ int tm_profile_enable(tm_ctx *ctx, int enable)
 {
     if (ctx == nullptr)
         return TM_ERR_ARGUMENT;
-    ctx->profile = enable != 0;
+    ctx->main.profile = enable != 0;
     return TM_OK;
 }
 
@@ -1587,20 +1806,20 @@ int tm_profile_read(tm_ctx *ctx, char *name, size_t name_capacity, int64_t *laun
         return TM_ERR_ARGUMENT;
     if (name && name_capacity > 0)
     {
-        std::snprintf(name, name_capacity, "%s", ctx->kname.c_str());
+        std::snprintf(name, name_capacity, "%s", ctx->main.kname.c_str());
     }
     if (launches)
-        *launches = ctx->prof_launches;
+        *launches = ctx->main.prof_launches;
     if (milliseconds)
-        *milliseconds = ctx->prof_ms;
+        *milliseconds = ctx->main.prof_ms;
     if (flops)
-        *flops = ctx->prof_flops;
+        *flops = ctx->main.prof_flops;
     if (all_launches)
-        *all_launches = ctx->all_launches;
-    ctx->prof_launches = 0;
-    ctx->prof_ms = 0.0;
-    ctx->prof_flops = 0.0;
-    ctx->all_launches = 0;
+        *all_launches = ctx->main.all_launches;
+    ctx->main.prof_launches = 0;
+    ctx->main.prof_ms = 0.0;
+    ctx->main.prof_flops = 0.0;
+    ctx->main.all_launches = 0;
     return TM_OK;
 }
 
@@ -1611,8 +1830,8 @@ int tm_profile_phases(tm_ctx *ctx, double *milliseconds, int capacity)
     for (int i = 0; i < TM_PHASES; i++)
     {
         if (i < capacity)
-            milliseconds[i] = ctx->phase_ms[i];
-        ctx->phase_ms[i] = 0.0;
+            milliseconds[i] = ctx->main.phase_ms[i];
+        ctx->main.phase_ms[i] = 0.0;
     }
     return TM_PHASES;
 }
@@ -1633,8 +1852,8 @@ int tm_bound_diagnostics(tm_ctx *ctx, const float *queries, int count, int m, fl
         }
         GroupPlan g;
         uint64_t h2d = 0;
-        prepare_group(ctx, m, idx, reqs.data(), g, h2d);
-        LengthStats &ls = ensure_length(ctx, m);
+        prepare_group(ctx, ctx->main, m, idx, reqs.data(), g, h2d);
+        LengthStats &ls = ensure_length(ctx, ctx->main, m);
         const uint64_t W = ls.W;
         if (W == 0 || W * static_cast<uint64_t>(count) > (1ull << 31))
             throw Failure{TM_ERR_ARGUMENT, "diagnostics need 0 < windows x templates <= 2^31"};
@@ -1645,17 +1864,17 @@ int tm_bound_diagnostics(tm_ctx *ctx, const float *queries, int count, int m, fl
             if (use_umma)
                 g.htp[t].a1_main = g.a1_umma[t];
         }
-        cudaStream_t s = ctx->stream;
+        cudaStream_t s = ctx->main.stream;
         TM_CUDA(cudaMemcpyAsync(g.tp.p, g.htp.data(), sizeof(TemplParam) * g.T_pad, cudaMemcpyHostToDevice, s));
         const size_t pairs = W * static_cast<size_t>(count);
         DevBuf dd, de, dc;
         dd.reserve(pairs * sizeof(float));
         de.reserve(pairs * sizeof(float));
-        ctx->counters.reserve(4 * sizeof(uint32_t));
-        TM_CUDA(cudaMemsetAsync(ctx->counters.p, 0, 4 * sizeof(uint32_t), s));
+        ctx->main.counters.reserve(4 * sizeof(uint32_t));
+        TM_CUDA(cudaMemsetAsync(ctx->main.counters.p, 0, 4 * sizeof(uint32_t), s));
         TM_CUDA(cudaMemsetAsync(dd.p, 0xff, pairs * sizeof(float), s)); // NaN where nothing was written
         TM_CUDA(cudaMemsetAsync(de.p, 0xff, pairs * sizeof(float), s));
-        ctx->cand.reserve(sizeof(Candidate) * 16);
+        ctx->main.cand.reserve(sizeof(Candidate) * 16);
         tmb::ScanArgs a{};
         a.x = ctx->clean.as<float>();
         a.q = g.q.as<float>();
@@ -1667,17 +1886,17 @@ int tm_bound_diagnostics(tm_ctx *ctx, const float *queries, int count, int m, fl
         a.m_pad = g.m_pad;
         a.T = count;
         a.nb = 1;
-        a.cand = ctx->cand.as<Candidate>();
-        a.cand_count = ctx->counters.as<uint32_t>();
+        a.cand = ctx->main.cand.as<Candidate>();
+        a.cand_count = ctx->main.counters.as<uint32_t>();
         a.cand_cap = 0;
         a.q_hi = g.q_hi.p;
         a.q_lo = g.q_lo.p;
         a.t_rows = g.t_rows;
-        a.err = reinterpret_cast<int *>(ctx->counters.as<uint32_t>() + 2);
+        a.err = reinterpret_cast<int *>(ctx->main.counters.as<uint32_t>() + 2);
         a.dbg_d = dd.as<float>();
         a.dbg_e = de.as<float>();
         TM_CUDA(use_umma ? tmb::launch_scan_umma(a, s) : tmb::launch_scan_fp32(a, s));
-        count_launch(ctx);
+        count_launch(ctx->main);
         TM_CUDA(cudaMemcpyAsync(d, dd.p, pairs * sizeof(float), cudaMemcpyDeviceToHost, s));
         TM_CUDA(cudaMemcpyAsync(e, de.p, pairs * sizeof(float), cudaMemcpyDeviceToHost, s));
         if (exact != nullptr)
@@ -1693,13 +1912,13 @@ int tm_bound_diagnostics(tm_ctx *ctx, const float *queries, int count, int m, fl
             TM_CUDA(tmb::launch_rescore(dc.as<Candidate>(), static_cast<uint32_t>(pairs), g.tp.as<TemplParam>(),
                                         g.q.as<float>(), g.order.as<int>(), ctx->raw.as<float>(), ls.w0, dx.as<float>(),
                                         s));
-            count_launch(ctx);
+            count_launch(ctx->main);
             TM_CUDA(cudaMemcpyAsync(exact, dx.p, pairs * sizeof(float), cudaMemcpyDeviceToHost, s));
             TM_CUDA(cudaStreamSynchronize(s));
             dx.release();
         }
         uint32_t err = 0;
-        TM_CUDA(cudaMemcpyAsync(&err, ctx->counters.as<uint32_t>() + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        TM_CUDA(cudaMemcpyAsync(&err, ctx->main.counters.as<uint32_t>() + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
         TM_CUDA(cudaStreamSynchronize(s));
         dd.release();
         de.release();
@@ -1714,8 +1933,8 @@ int tm_d2h_bytes(tm_ctx *ctx, uint64_t *bytes)
 {
     if (ctx == nullptr || bytes == nullptr)
         return TM_ERR_ARGUMENT;
-    *bytes = ctx->d2h_bytes;
-    ctx->d2h_bytes = 0;
+    *bytes = ctx->main.d2h_bytes;
+    ctx->main.d2h_bytes = 0;
     return TM_OK;
 }
 
@@ -1723,7 +1942,7 @@ int tm_ctx_stream(tm_ctx *ctx, void **stream)
 {
     if (ctx == nullptr || stream == nullptr)
         return TM_ERR_ARGUMENT;
-    *stream = static_cast<void *>(ctx->stream);
+    *stream = static_cast<void *>(ctx->main.stream);
     return TM_OK;
 }
 
@@ -1731,7 +1950,139 @@ int tm_last_candidates(const tm_ctx *ctx, uint64_t *count)
 {
     if (ctx == nullptr || count == nullptr)
         return TM_ERR_ARGUMENT;
-    *count = ctx->last_candidates;
+    *count = ctx->main.last_candidates;
+    return TM_OK;
+}
+
+
+int tm_serve_start(tm_ctx *ctx, const tm_serve_config *config)
+{
+    if (ctx == nullptr)
+        return TM_ERR_ARGUMENT;
+    if (ctx->server && !ctx->server->stopped)
+        return TM_ERR_STATE;
+    tm_serve_config cfg{2, 256, 0};
+    if (config)
+        cfg = *config;
+    if (cfg.workers < 1 || cfg.workers > 8 || cfg.max_batch < 1)
+        return TM_ERR_ARGUMENT;
+    return guarded(ctx, [&] {
+        TM_CUDA(cudaSetDevice(ctx->device));
+        if (ctx->kernel == TM_KERNEL_FP32 || !tmb::umma_supported(0, 0, 0))
+            throw Failure{TM_ERR_STATE, "serving batches templates of several lengths on the tensor-core kernel"};
+        ensure_prefix(ctx, ctx->main);
+        if (cfg.memory_budget == 0)
+        {
+            size_t free_b = 0, total_b = 0;
+            TM_CUDA(cudaMemGetInfo(&free_b, &total_b));
+            cfg.memory_budget = free_b / 4;
+        }
+        ctx->server.reset();
+        auto sv = std::make_unique<Server>();
+        sv->ctx = ctx;
+        sv->cfg = cfg;
+        for (int i = 0; i < cfg.workers; i++)
+        {
+            sv->lanes.push_back(std::make_unique<Lane>());
+            sv->lanes.back()->open();
+        }
+        Server *p = sv.get();
+        ctx->server = std::move(sv);
+        for (int i = 0; i < cfg.workers; i++)
+            p->threads.emplace_back(serve_worker, p, p->lanes[i].get());
+    });
+}
+
+int tm_submit(tm_ctx *ctx, const tm_request *request, uint64_t *ticket)
+{
+    if (ctx == nullptr || request == nullptr || ticket == nullptr)
+        return TM_ERR_ARGUMENT;
+    Server *sv = ctx->server.get();
+    if (sv == nullptr || sv->stopped)
+        return TM_ERR_STATE;
+    const int rc = validate_requests(ctx, request, 1);
+    if (rc != TM_OK)
+        return rc;
+    if (request->m > 16384)
+        return TM_ERR_ARGUMENT;
+    ServeItem it;
+    try
+    {
+        it.templ.assign(request->templ, request->templ + request->m);
+    }
+    catch (const std::bad_alloc &)
+    {
+        return TM_ERR_NO_MEMORY;
+    }
+    it.req = *request;
+    it.bytes = serve_bytes(ctx, *request);
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        if (sv->stopping)
+            return TM_ERR_STATE;
+        it.ticket = sv->next_ticket++;
+        it.submit_ms = sv->now_ms();
+        *ticket = it.ticket;
+        sv->pending.push_back(std::move(it));
+    }
+    sv->work_cv.notify_one();
+    return TM_OK;
+}
+
+int tm_poll(tm_ctx *ctx, tm_completion *out, int capacity, int timeout_ms, int *count)
+{
+    if (ctx == nullptr || count == nullptr || capacity < 0 || (capacity > 0 && out == nullptr))
+        return TM_ERR_ARGUMENT;
+    *count = 0;
+    Server *sv = ctx->server.get();
+    if (sv == nullptr)
+        return TM_ERR_STATE;
+    std::unique_lock<std::mutex> lk(sv->mu);
+    if (sv->done.empty() && timeout_ms != 0)
+    {
+        auto ready = [&] { return !sv->done.empty(); };
+        if (timeout_ms < 0)
+            sv->done_cv.wait(lk, ready);
+        else
+            sv->done_cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready);
+    }
+    int n = 0;
+    while (n < capacity && !sv->done.empty())
+    {
+        out[n++] = sv->done.front();
+        sv->done.pop_front();
+    }
+    *count = n;
+    return TM_OK;
+}
+
+int tm_serve_stop(tm_ctx *ctx)
+{
+    if (ctx == nullptr)
+        return TM_ERR_ARGUMENT;
+    if (!ctx->server)
+        return TM_ERR_STATE;
+    stop_server(ctx);
+    return TM_OK;
+}
+
+int tm_serve_status(tm_ctx *ctx, uint64_t *pending, uint64_t *in_flight, uint64_t *in_flight_bytes,
+                    uint64_t *launches)
+{
+    if (ctx == nullptr)
+        return TM_ERR_ARGUMENT;
+    Server *sv = ctx->server.get();
+    if (sv == nullptr)
+        return TM_ERR_STATE;
+    std::lock_guard<std::mutex> lk(sv->mu);
+    if (pending)
+        *pending = sv->pending.size();
+    if (in_flight)
+        *in_flight = sv->in_flight;
+    if (in_flight_bytes)
+        *in_flight_bytes = sv->in_flight_bytes;
+    if (launches)
+        *launches = sv->launches;
     return TM_OK;
 }
 
