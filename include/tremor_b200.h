@@ -65,6 +65,17 @@ extern "C" {
 #define TM_KERNEL_FP32 1       /* plain FP32 sliding dot product (CUDA cores) */
 #define TM_KERNEL_SPLIT_BF16 2 /* tcgen05 split-BF16 Hankel contraction */
 
+/* Tile shapes of the tensor-core contraction for batches of templates of several lengths
+ * (tm_set_tiles). A tile's K extent is its longest template. Row tiles (k_scan_umma) hold
+ * 128 templates x 256 windows; column tiles (k_scan_wm) hold 128 windows x 32, 64 or 128
+ * templates, which wastes less when few templates share a length. AUTO picks the shape
+ * of least modelled time per group (tm_autotune measures the model's constants). */
+#define TM_TILES_AUTO 0
+#define TM_TILES_ROWS 1
+#define TM_TILES_COLS_128 2
+#define TM_TILES_COLS_64 3
+#define TM_TILES_COLS_32 4
+
 /* request flags */
 #define TM_FLAG_ZNORMALIZED 1u /* templ is already z-normalised (QaWorkerData::ts) */
 
@@ -93,6 +104,17 @@ int tm_ctx_destroy(tm_ctx *ctx);
 const char *tm_last_error(const tm_ctx *ctx);
 /* TM_KERNEL_*; default TM_KERNEL_AUTO. */
 int tm_set_kernel(tm_ctx *ctx, int kernel);
+/* Tile shape of mixed-length groups (TM_TILES_*); applies to batches created afterwards.
+ * No counterpart in the reference (its scan has no tiles). */
+int tm_set_tiles(tm_ctx *ctx, int tiles);
+/* Tiling model of the planner behind TM_TILES_AUTO: kernel milliseconds of 128 templates x
+ * 2^25 windows, [group kind: one length, several][shape: rows, columns 128, 64, 32]
+ * [K: 256, 1024, 4096, 16384], 32 doubles in that order. tm_autotune measures it on this
+ * device (a few seconds, its own synthetic record), stores it in the context and copies
+ * it to ms (up to capacity values); returns 32 or an error. tm_set_tile_model installs a
+ * saved one (count must be 32). No counterpart in the reference. */
+int tm_autotune(tm_ctx *ctx, double *ms, int capacity);
+int tm_set_tile_model(tm_ctx *ctx, const double *ms, int count);
 /* Restricts searches to windows [first, first + count) (a data partition as in
  * SkipSequential.cpp:218-226); default: every window of every length. */
 int tm_set_window_range(tm_ctx *ctx, uint64_t first, uint64_t count);

@@ -11,6 +11,10 @@ from tests import oracle_bindings as ob
 
 pytestmark = pytest.mark.gpu
 
+# every tile shape of the mixed-length contraction: 128-template row tiles (k_scan_umma),
+# column tiles of 128 / 64 / 32 templates (k_scan_wm)
+TILES = [tb.TILES_ROWS, tb.TILES_COLS_128, tb.TILES_COLS_64, tb.TILES_COLS_32]
+
 
 def _waveform(n, seed, offset=0.0):
     from tremor_b200 import synth
@@ -56,23 +60,27 @@ def _check(x, reqs, answers):
             assert np.array_equal(dist.view(np.uint32), d.view(np.uint32))
 
 
+@pytest.mark.parametrize('tiles', TILES)
 @pytest.mark.parametrize('offset', [0.0, 5000.0])
-def test_mixed_lengths_match_oracle(offset):
+def test_mixed_lengths_match_oracle(offset, tiles):
     x = _waveform(1 << 17, 5 + int(offset), offset)
     rng = np.random.default_rng(6)
     lengths = [int(v) for v in rng.choice([40, 64, 100, 128, 200, 333, 512, 1000, 2048], size=18)]
     reqs = _requests(x, rng, lengths)
     with tb.Context(x) as ctx:
+        ctx.set_tiles(tiles)
         answers = ctx.scan_batch(reqs)
     _check(x, reqs, answers)
 
 
-def test_mixed_lengths_window_range():
+@pytest.mark.parametrize('tiles', TILES)
+def test_mixed_lengths_window_range(tiles):
     x = _waveform(1 << 16, 8)
     rng = np.random.default_rng(9)
     reqs = _requests(x, rng, [64, 96, 150, 300, 64, 500])
     first, count = 7000, 40000
     with tb.Context(x) as ctx:
+        ctx.set_tiles(tiles)
         ctx.set_window_range(first, count)
         answers = ctx.scan_batch(reqs)
     for r, (pos, dist) in zip(reqs, answers):
@@ -88,7 +96,8 @@ def test_mixed_lengths_window_range():
             assert np.array_equal(dist.view(np.uint32), d.view(np.uint32))
 
 
-def test_mixed_lengths_sparse_unbounded():
+@pytest.mark.parametrize('tiles', TILES)
+def test_mixed_lengths_sparse_unbounded(tiles):
     """So few windows that no kNN bound exists: constant windows (distance FLT_MAX) fill
     the answers in position order, as the reference's unfilled queue makes them do."""
     rng = np.random.default_rng(10)
@@ -98,11 +107,13 @@ def test_mixed_lengths_sparse_unbounded():
             tb.Request(rng.normal(size=100).astype(np.float32), tb.MODE_KNN, k=9, merge_offset=30),
             tb.Request(rng.normal(size=48).astype(np.float32), tb.MODE_THRESHOLD, correlation=-0.2)]
     with tb.Context(x) as ctx:
+        ctx.set_tiles(tiles)
         answers = ctx.scan_batch(reqs)
     _check(x, reqs, answers)
 
 
-def test_constant_stretch_does_not_flood_candidates():
+@pytest.mark.parametrize('tiles', [tb.TILES_ROWS, tb.TILES_COLS_64])
+def test_constant_stretch_does_not_flood_candidates(tiles):
     """Windows inside a long constant stretch are recognised from the constant-run lengths,
     not handed one by one to the exact re-scoring."""
     from tremor_b200 import synth
@@ -112,11 +123,13 @@ def test_constant_stretch_does_not_flood_candidates():
     reqs = [tb.Request(synth.chirp_templates(1, m, rng)[0], tb.MODE_THRESHOLD, correlation=0.9)
             for m in [64, 128, 256, 512]]
     with tb.Context(x) as ctx:
+        ctx.set_tiles(tiles)
         ctx.scan_batch(reqs)
         assert ctx.last_candidates() < 5000
 
 
-def test_mixed_lengths_last_windows():
+@pytest.mark.parametrize('tiles', TILES)
+def test_mixed_lengths_last_windows(tiles):
     """A template planted in the last window of the waveform (or a few samples before it)
     is found with its exact distance while templates of other lengths share its tiles
     (the window-end prefix sums at the end of the record)."""
@@ -133,6 +146,7 @@ def test_mixed_lengths_last_windows():
             reqs.append(tb.Request(t, tb.MODE_KNN, k=1))
             reqs.append(tb.Request(t, tb.MODE_THRESHOLD, correlation=0.99))
         with tb.Context(x) as ctx:
+            ctx.set_tiles(tiles)
             answers = ctx.scan_batch(reqs)
         assert int(answers[2 * k][0][0]) == end - m
         assert end - m in set(int(p) for p in answers[2 * k + 1][0])

@@ -26,6 +26,7 @@ __all__ = ['Context', 'Batch', 'TremorError', 'Request', 'knn_rows', 'threshold_
 MODE_THRESHOLD = 0
 MODE_KNN = 1
 KERNEL_AUTO, KERNEL_FP32, KERNEL_SPLIT_BF16 = 0, 1, 2
+TILES_AUTO, TILES_ROWS, TILES_COLS_128, TILES_COLS_64, TILES_COLS_32 = 0, 1, 2, 3, 4
 FLAG_ZNORMALIZED = 1
 MISSING_VALUE = np.float32(-100000.0)
 FLT_MAX = float(np.finfo(np.float32).max)
@@ -73,6 +74,9 @@ def load_library():
         'tm_ctx_destroy': (i, [_vp]),
         'tm_last_error': (ctypes.c_char_p, [_vp]),
         'tm_set_kernel': (i, [_vp, i]),
+        'tm_set_tiles': (i, [_vp, i]),
+        'tm_autotune': (i, [_vp, _vp, i]),
+        'tm_set_tile_model': (i, [_vp, _vp, i]),
         'tm_set_window_range': (i, [_vp, u64, u64]),
         'tm_prepare_length': (i, [_vp, i]),
         'tm_window_stats': (i, [_vp, i, u64, u64, _vp, _vp]),
@@ -162,6 +166,23 @@ class Context:
 
     def set_kernel(self, kernel: int):
         self._check(self._lib.tm_set_kernel(self._h, kernel))
+
+    def set_tiles(self, tiles: int):
+        """Tile shape of mixed-length groups (TILES_*), for batches created afterwards."""
+        self._check(self._lib.tm_set_tiles(self._h, tiles))
+
+    def autotune(self) -> np.ndarray:
+        """Measures the tiling model on this device (tm_autotune): milliseconds of 128
+        templates x 2^25 windows, shape [kind (one length, several), tile shape (rows,
+        columns 128 / 64 / 32), K (256, 1024, 4096, 16384)]."""
+        out = np.zeros(32, np.float64)
+        rc = self._lib.tm_autotune(self._h, out.ctypes.data, 32)
+        self._check(min(rc, 0))
+        return out.reshape(2, 4, 4)
+
+    def set_tile_model(self, ms: np.ndarray):
+        arr = np.ascontiguousarray(ms, dtype=np.float64).reshape(-1)
+        self._check(self._lib.tm_set_tile_model(self._h, arr.ctypes.data, len(arr)))
 
     def set_window_range(self, first: int, count: int):
         self._check(self._lib.tm_set_window_range(self._h, first, count))

@@ -10,6 +10,7 @@
 //   4. device: every candidate re-scored with the reference's exact arithmetic;
 //   5. host: canonical exclusion selection / threshold merge on the exact distances.
 #include <algorithm>
+#include <functional>
 #include <condition_variable>
 #include <deque>
 #include <mutex>
@@ -38,6 +39,7 @@ cudaError_t launch_reference_stats(const float *raw, int m, uint64_t w0, uint64_
                                    cudaStream_t s);
 cudaError_t launch_scan_fp32(const ScanArgs &a, cudaStream_t s);
 cudaError_t launch_scan_umma(const ScanArgs &a, cudaStream_t s);
+cudaError_t launch_scan_wm(const ScanArgs &a, cudaStream_t s);
 bool umma_supported(int m, int T, uint64_t W);
 cudaError_t launch_bucket_select(const uint32_t *bmin_u, uint32_t nb, const TemplParam *tp, const int *knn_slots,
                                  int nk, uint32_t *tkey, cudaStream_t s);
@@ -277,6 +279,18 @@ struct tm_ctx
     DevBuf raw, clean;
     uint64_t range_first = 0, range_count = UINT64_MAX;
     int kernel = TM_KERNEL_AUTO;
+    int tiles = TM_TILES_AUTO;
+    // tiling cost model: kernel milliseconds for 128 templates x 2^25 windows, per group kind
+    // (one length / several), shape (row tiles; column tiles of 128, 64, 32) and K (256,
+    // 1024, 4096, 16384). Defaults: a B200 measurement; tm_autotune re-measures.
+    double tile_ms[2][4][4] = {{{17.5, 19.3, 68.8, 272.5},
+                                {29.9, 32.1, 90.9, 346.8},
+                                {31.8, 43.5, 157.4, 580.8},
+                                {36.7, 84.3, 308.9, 1129.8}},
+                               {{31.9, 35.9, 67.5, 261.8},
+                                {65.1, 70.5, 100.6, 351.7},
+                                {69.0, 78.3, 159.3, 580.5},
+                                {75.7, 92.5, 310.2, 1135.9}}};
     std::map<int, std::unique_ptr<LengthStats>> lengths;
     uint64_t use_clock = 0;
     DevBuf suf; // window-statistics scratch (per-length statistics)
@@ -404,11 +418,13 @@ struct GroupPlan
     std::vector<TemplParam> htp;
     DevBuf q, order, tp, slots, q_hi, q_lo;
     int t_rows = 0;
-    // templates of several lengths (sorted by length, longest first) in 128-row tiles
+    // templates of several lengths (sorted by length, longest first) in 128-row tiles of
+    // k_scan_umma or, when col_tile > 0, in column tiles of col_tile rows of k_scan_wm
     bool mixed = false;
+    int col_tile = 0;
     int k_stride = 0;            // row stride of the template arrays
     uint32_t w_max = 0;          // windows of the shortest template
-    std::vector<tmb::TileInfo> tiles; // per 128-row tile: K blocks, distinct lengths
+    std::vector<tmb::TileInfo> tiles; // per tile: K blocks (row tiles: and distinct lengths)
     DevBuf d_tiles;
     void release()
     {
@@ -441,9 +457,10 @@ namespace {
 // Host preparation of one group (bit-identical template z-normalisation and block
 // order, epilogue constants) and its upload.
 void prepare_group(tm_ctx *ctx, Lane &L, int m, const std::vector<int> &idx, const tm_request *reqs, GroupPlan &g,
-                   uint64_t &h2d)
+                   uint64_t &h2d, int col_tile = 0)
 {
     g.m = m;
+    g.col_tile = col_tile; // tensor cores: window-major column tiles (k_scan_wm) when > 0
     g.T = static_cast<int>(idx.size());
     g.T_pad = (g.T + 63) & ~63;
     g.m_pad = (m + 63) & ~63;
@@ -570,16 +587,18 @@ void ensure_prefix(tm_ctx *ctx, Lane &L)
     ctx->prefix_ready = true;
 }
 
-// Host preparation of a mixed-length group: templates sorted by length (longest first)
-// fill 128-row tiles, a tile closing early when a new length would be its 65th distinct
-// one (padding rows are inert); a tile's K extent is its longest template (shorter rows
-// are zero-padded, which leaves their dot products unchanged). Rows are the template
-// slots of the group: g.index[row] is the request (-1 for padding rows).
+// Host preparation of a mixed-length group: templates sorted by length (longest first).
+// Row tiles (col_tile 0, k_scan_umma): 128 rows, a tile closing early when a new length
+// would be its 65th distinct one. Column tiles (k_scan_wm): col_tile rows, any lengths.
+// Padding rows are inert; a tile's K extent is its longest template (shorter rows are
+// zero-padded, which leaves their dot products unchanged). Rows are the template slots of
+// the group: g.index[row] is the request (-1 for padding rows).
 void prepare_group_mixed(tm_ctx *ctx, Lane &L, const std::vector<int> &idx_in, const tm_request *reqs, GroupPlan &g,
-                         uint64_t &h2d)
+                         uint64_t &h2d, int col_tile = 0)
 {
     std::vector<int> idx = idx_in;
     std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return reqs[a].m > reqs[b].m; });
+    const size_t tile_rows = col_tile > 0 ? static_cast<size_t>(col_tile) : 128;
     // rows: request per row (-1 = padding)
     std::vector<int> rows;
     std::vector<tmb::TileInfo> tiles;
@@ -588,33 +607,39 @@ void prepare_group_mixed(tm_ctx *ctx, Lane &L, const std::vector<int> &idx_in, c
     {
         tmb::TileInfo ti{};
         const size_t start = rows.size();
-        while (i < idx.size() && rows.size() - start < 128)
+        const int longest = reqs[idx[i]].m;
+        while (i < idx.size() && rows.size() - start < tile_rows)
         {
             const int m = reqs[idx[i]].m;
             int d = 0;
-            while (d < ti.D && ti.len[d] != m)
-                d++;
-            if (d == ti.D)
+            if (col_tile == 0)
             {
-                if (ti.D == tmb::kTileLens)
-                    break;
-                ti.len[ti.D++] = m;
+                while (d < ti.D && ti.len[d] != m)
+                    d++;
+                if (d == ti.D)
+                {
+                    if (ti.D == tmb::kTileLens)
+                        break;
+                    ti.len[ti.D++] = m;
+                }
             }
             rows.push_back(idx[i]);
             didx_of_row.push_back(d);
             i++;
         }
-        ti.kb = (ti.len[0] + 63) / 64; // longest length first
-        while (rows.size() - start < 128)
+        ti.len[0] = longest;
+        ti.kb = (longest + 63) / 64;
+        while (rows.size() - start < tile_rows)
         {
             rows.push_back(-1);
             didx_of_row.push_back(0);
         }
         tiles.push_back(ti);
     }
-    const int R = static_cast<int>(rows.size()); // multiple of 128
+    const int R = static_cast<int>(rows.size()); // multiple of the tile rows
     const int m_max = reqs[idx[0]].m;
     g.mixed = true;
+    g.col_tile = col_tile;
     g.m = m_max;
     g.T = R;
     g.T_pad = R;
@@ -654,7 +679,7 @@ void prepare_group_mixed(tm_ctx *ctx, Lane &L, const std::vector<int> &idx_in, c
     for (int t = 0; t < R; t++)
     {
         TemplParam &p = g.htp[t];
-        const tmb::TileInfo &ti = tiles[t / 128];
+        const tmb::TileInfo &ti = tiles[static_cast<size_t>(t) / tile_rows];
         p.didx = didx_of_row[t];
         if (rows[t] < 0)
         {
@@ -1048,8 +1073,9 @@ void execute_group(tm_ctx *ctx, Lane &L, GroupPlan &g, tm_result &res)
         // 2. contraction with fused epilogue
         if (L.profile)
             TM_CUDA(cudaEventRecord(L.ev0, s));
+        a.col_tile = g.col_tile;
         if (use_umma)
-            TM_CUDA(tmb::launch_scan_umma(a, s));
+            TM_CUDA(g.col_tile > 0 ? tmb::launch_scan_wm(a, s) : tmb::launch_scan_umma(a, s));
         else
             TM_CUDA(tmb::launch_scan_fp32(a, s));
         count_launch(L);
@@ -1059,7 +1085,7 @@ void execute_group(tm_ctx *ctx, Lane &L, GroupPlan &g, tm_result &res)
             TM_CUDA(cudaEventSynchronize(L.ev1));
             float ms = 0.0f;
             TM_CUDA(cudaEventElapsedTime(&ms, L.ev0, L.ev1));
-            L.kname = use_umma ? "k_scan_umma" : "k_scan_fp32";
+            L.kname = use_umma ? (g.col_tile > 0 ? "k_scan_wm" : "k_scan_umma") : "k_scan_fp32";
             L.prof_launches++;
             L.prof_ms += ms;
             L.phase_ms[0] += ms;
@@ -1197,7 +1223,8 @@ void execute_group_mixed(tm_ctx *ctx, Lane &L, GroupPlan &g, tm_result &res)
         a.n = ctx->n;
         if (L.profile)
             TM_CUDA(cudaEventRecord(L.ev0, s));
-        TM_CUDA(tmb::launch_scan_umma(a, s));
+        a.col_tile = g.col_tile;
+        TM_CUDA(g.col_tile > 0 ? tmb::launch_scan_wm(a, s) : tmb::launch_scan_umma(a, s));
         count_launch(L);
         if (L.profile)
         {
@@ -1205,7 +1232,7 @@ void execute_group_mixed(tm_ctx *ctx, Lane &L, GroupPlan &g, tm_result &res)
             TM_CUDA(cudaEventSynchronize(L.ev1));
             float ms = 0.0f;
             TM_CUDA(cudaEventElapsedTime(&ms, L.ev0, L.ev1));
-            L.kname = "k_scan_umma";
+            L.kname = g.col_tile > 0 ? "k_scan_wm" : "k_scan_umma";
             L.prof_launches++;
             L.prof_ms += ms;
             L.phase_ms[0] += ms;
@@ -1272,6 +1299,64 @@ void execute_group_mixed(tm_ctx *ctx, Lane &L, GroupPlan &g, tm_result &res)
     });
 }
 
+// Modelled milliseconds of 128 template rows x 2^25 windows of shape v at K samples:
+// linear between the measured K, proportional to K above the largest, flat below the
+// smallest (epilogue-bound there).
+double tile_time(const tm_ctx *ctx, bool mixed, int v, double k)
+{
+    static const double ks[4] = {256.0, 1024.0, 4096.0, 16384.0};
+    const double *t = ctx->tile_ms[mixed ? 1 : 0][v];
+    if (k <= ks[0])
+        return t[0];
+    if (k >= ks[3])
+        return t[3] * k / ks[3];
+    int i = 0;
+    while (k > ks[i + 1])
+        i++;
+    return t[i] + (t[i + 1] - t[i]) * (k - ks[i]) / (ks[i + 1] - ks[i]);
+}
+
+// Tile shape of a group: 0 (row tiles of 128 templates, k_scan_umma) or the column-tile
+// size (k_scan_wm). Each shape's modelled time sums its tiles (consecutive in length
+// order; a tile costs its rows at its longest template's K); the least wins.
+int plan_col_tile(const tm_ctx *ctx, const tm_request *reqs, const std::vector<int> &idx)
+{
+    switch (ctx->tiles)
+    {
+    case TM_TILES_ROWS:
+        return 0;
+    case TM_TILES_COLS_128:
+        return 128;
+    case TM_TILES_COLS_64:
+        return 64;
+    case TM_TILES_COLS_32:
+        return 32;
+    default:
+        break;
+    }
+    std::vector<int> m(idx.size());
+    for (size_t i = 0; i < idx.size(); i++)
+        m[i] = reqs[idx[i]].m;
+    std::sort(m.begin(), m.end(), std::greater<int>());
+    const bool mixed = !m.empty() && m.front() != m.back();
+    const int shapes[4] = {128, 128, 64, 32};
+    double best = 0.0;
+    int choice = 0;
+    for (int v = 0; v < 4; v++)
+    {
+        const size_t rows = static_cast<size_t>(shapes[v]);
+        double cost = 0.0;
+        for (size_t i = 0; i < m.size(); i += rows) // row tiles may close early (65 lengths): ignored
+            cost += static_cast<double>(rows) / 128.0 * tile_time(ctx, mixed, v, static_cast<double>((m[i] + 63) & ~63));
+        if (v == 0 || cost < best)
+        {
+            best = cost;
+            choice = v == 0 ? 0 : shapes[v];
+        }
+    }
+    return choice;
+}
+
 // Groups of a batch. Lengths with a full 128-template tile (or any length, on the FP32
 // kernel) get their own group with per-length statistics; the remaining templates of
 // several lengths share one mixed-length group on the tensor cores.
@@ -1285,7 +1370,7 @@ void create_batch(tm_ctx *ctx, Lane &L, const tm_request *requests, int count, t
             all[i] = i;
         b.groups.resize(count > 0 ? 1 : 0);
         if (count > 0)
-            prepare_group_mixed(ctx, L, all, requests, b.groups[0], b.h2d_bytes);
+            prepare_group_mixed(ctx, L, all, requests, b.groups[0], b.h2d_bytes, plan_col_tile(ctx, requests, all));
         return;
     }
     std::map<int, std::vector<int>> by_m;
@@ -1312,9 +1397,10 @@ void create_batch(tm_ctx *ctx, Lane &L, const tm_request *requests, int count, t
     b.groups.resize(single.size() + (rest.empty() ? 0 : 1));
     size_t gi = 0;
     for (auto &kv : single)
-        prepare_group(ctx, L, kv.first, kv.second, requests, b.groups[gi++], b.h2d_bytes);
+        prepare_group(ctx, L, kv.first, kv.second, requests, b.groups[gi++], b.h2d_bytes,
+                      tensor && kv.first <= 16384 ? plan_col_tile(ctx, requests, kv.second) : 0);
     if (!rest.empty())
-        prepare_group_mixed(ctx, L, rest, requests, b.groups[gi++], b.h2d_bytes);
+        prepare_group_mixed(ctx, L, rest, requests, b.groups[gi++], b.h2d_bytes, plan_col_tile(ctx, requests, rest));
 }
 
 void run_batch(tm_ctx *ctx, Lane &L, tm_batch &b, tm_result &res)
@@ -1413,6 +1499,57 @@ static uint64_t serve_bytes(const tm_ctx *ctx, const tm_request &r)
     return row + 48ull * cands;
 }
 
+// Admission (under the server's lock). A batch is built a tile at a time: the 128 rows of
+// a contraction tile share one K extent, their longest template, so rows not longer than
+// that cost nothing extra. Each tile opens with the oldest pending request (so every batch
+// admits the oldest, and later arrivals never hold a request back indefinitely) and fills
+// with the longest pending requests not longer than it; with a long queue the tiles hold
+// similar lengths.
+// Stops at max_batch or at the memory budget (a first request alone is always admitted).
+static void admit(Server *sv, std::vector<ServeItem> &batch, uint64_t &bytes)
+{
+    auto fits = [&](uint64_t b) {
+        return (sv->in_flight_bytes == 0 && batch.empty()) || sv->in_flight_bytes + bytes + b <= sv->cfg.memory_budget;
+    };
+    std::vector<size_t> order;
+    std::vector<char> chosen;
+    while (!sv->pending.empty() && static_cast<int>(batch.size()) < sv->cfg.max_batch)
+    {
+        if (!fits(sv->pending.front().bytes))
+            return;
+        const int cap_m = sv->pending.front().req.m;
+        bytes += sv->pending.front().bytes;
+        batch.push_back(std::move(sv->pending.front()));
+        sv->pending.pop_front();
+        const size_t room = std::min<size_t>(127, static_cast<size_t>(sv->cfg.max_batch) - batch.size());
+        order.clear();
+        for (size_t i = 0; i < sv->pending.size(); i++)
+            if (sv->pending[i].req.m <= cap_m)
+                order.push_back(i);
+        std::stable_sort(order.begin(), order.end(),
+                         [&](size_t x, size_t y) { return sv->pending[x].req.m > sv->pending[y].req.m; });
+        chosen.assign(sv->pending.size(), 0);
+        size_t taken = 0;
+        for (size_t i : order)
+        {
+            if (taken == room || !fits(sv->pending[i].bytes))
+                break;
+            bytes += sv->pending[i].bytes;
+            batch.push_back(std::move(sv->pending[i]));
+            chosen[i] = 1;
+            taken++;
+        }
+        if (taken > 0)
+        {
+            std::deque<ServeItem> rest;
+            for (size_t i = 0; i < sv->pending.size(); i++)
+                if (!chosen[i])
+                    rest.push_back(std::move(sv->pending[i]));
+            sv->pending.swap(rest);
+        }
+    }
+}
+
 static void serve_worker(Server *sv, Lane *L)
 {
     tm_ctx *ctx = sv->ctx;
@@ -1430,16 +1567,7 @@ static void serve_worker(Server *sv, Lane *L)
             {
                 if (sv->pending.empty() && sv->stopping)
                     return;
-                while (!sv->pending.empty() && static_cast<int>(batch.size()) < sv->cfg.max_batch)
-                {
-                    const uint64_t b = sv->pending.front().bytes;
-                    const bool alone = sv->in_flight_bytes == 0 && batch.empty();
-                    if (!alone && sv->in_flight_bytes + bytes + b > sv->cfg.memory_budget)
-                        break;
-                    bytes += b;
-                    batch.push_back(std::move(sv->pending.front()));
-                    sv->pending.pop_front();
-                }
+                admit(sv, batch, bytes);
                 if (!batch.empty())
                     break;
                 sv->work_cv.wait(lk); // nothing pending, or the budget is full: wait for either to change
@@ -1532,6 +1660,90 @@ static void stop_server(tm_ctx *ctx)
     sv->stopped = true;
 }
 
+// tm_bound_diagnostics for the window-major kernel: the templates (all of length m) as one
+// group in column tiles of the context's shape, statistics from the prefix sums.
+static void bound_diagnostics_wm(tm_ctx *ctx, int m, const std::vector<int> &idx, const std::vector<tm_request> &reqs,
+                                 float *d, float *e, float *exact)
+{
+    Lane &L = ctx->main;
+    cudaStream_t s = L.stream;
+    const int count = static_cast<int>(idx.size());
+    ensure_prefix(ctx, L);
+    GroupPlan g;
+    uint64_t h2d = 0;
+    prepare_group_mixed(ctx, L, idx, reqs.data(), g, h2d, plan_col_tile(ctx, reqs.data(), idx));
+    const uint64_t W = g.w_max;
+    if (W == 0 || W * static_cast<uint64_t>(count) > (1ull << 31))
+        throw Failure{TM_ERR_ARGUMENT, "diagnostics need 0 < windows x templates <= 2^31"};
+    for (int t = 0; t < g.T; t++)
+        g.htp[t].thr_ed = -FLT_MAX; // emit nothing
+    TM_CUDA(cudaMemcpyAsync(g.tp.p, g.htp.data(), sizeof(TemplParam) * g.T, cudaMemcpyHostToDevice, s));
+    const size_t pairs = W * static_cast<size_t>(count);
+    DevBuf dd, de, dc, dx;
+    dd.reserve(pairs * sizeof(float));
+    de.reserve(pairs * sizeof(float));
+    L.counters.reserve(8 * sizeof(uint32_t));
+    TM_CUDA(cudaMemsetAsync(L.counters.p, 0, 8 * sizeof(uint32_t), s));
+    TM_CUDA(cudaMemsetAsync(dd.p, 0xff, pairs * sizeof(float), s)); // NaN where nothing was written
+    TM_CUDA(cudaMemsetAsync(de.p, 0xff, pairs * sizeof(float), s));
+    L.cand.reserve(sizeof(Candidate) * 16);
+    const uint32_t nb = static_cast<uint32_t>((W + tmb::kBucket - 1) / tmb::kBucket);
+    L.bmin_u.reserve(sizeof(uint32_t) * static_cast<size_t>(g.T) * nb);
+    L.bmin_l.reserve(sizeof(uint32_t) * static_cast<size_t>(g.T) * nb);
+    tmb::ScanArgs a{};
+    a.x = ctx->clean.as<float>();
+    a.q = g.q.as<float>();
+    a.tp = g.tp.as<TemplParam>();
+    a.w0 = ctx->range_first;
+    a.W = static_cast<uint32_t>(W);
+    a.T = g.T;
+    a.bmin_u = L.bmin_u.as<uint32_t>();
+    a.bmin_l = L.bmin_l.as<uint32_t>();
+    a.nb = nb;
+    a.cand = L.cand.as<Candidate>();
+    a.cand_count = L.counters.as<uint32_t>();
+    a.cand_cap = 0;
+    a.q_hi = g.q_hi.p;
+    a.q_lo = g.q_lo.p;
+    a.t_rows = g.t_rows;
+    a.err = reinterpret_cast<int *>(L.counters.as<uint32_t>() + 2);
+    a.dbg_d = dd.as<float>();
+    a.dbg_e = de.as<float>();
+    a.raw = ctx->raw.as<float>();
+    a.P = ctx->prefix.as<double2>();
+    a.run = ctx->run.as<uint16_t>();
+    a.center = ctx->center;
+    a.tiles = g.d_tiles.as<tmb::TileInfo>();
+    a.k_stride = g.k_stride;
+    a.n = ctx->n;
+    a.col_tile = g.col_tile;
+    TM_CUDA(g.col_tile > 0 ? tmb::launch_scan_wm(a, s) : tmb::launch_scan_umma(a, s));
+    count_launch(L);
+    TM_CUDA(cudaMemcpyAsync(d, dd.p, pairs * sizeof(float), cudaMemcpyDeviceToHost, s));
+    TM_CUDA(cudaMemcpyAsync(e, de.p, pairs * sizeof(float), cudaMemcpyDeviceToHost, s));
+    if (exact != nullptr)
+    {
+        std::vector<Candidate> all(pairs);
+        for (int t = 0; t < count; t++)
+            for (uint64_t j = 0; j < W; j++)
+                all[static_cast<size_t>(t) * W + j] = Candidate{static_cast<uint32_t>(t), static_cast<uint32_t>(j)};
+        dc.reserve(pairs * sizeof(Candidate));
+        dx.reserve(pairs * sizeof(float));
+        TM_CUDA(cudaMemcpyAsync(dc.p, all.data(), pairs * sizeof(Candidate), cudaMemcpyHostToDevice, s));
+        TM_CUDA(tmb::launch_rescore(dc.as<Candidate>(), static_cast<uint32_t>(pairs), g.tp.as<TemplParam>(),
+                                    g.q.as<float>(), g.order.as<int>(), ctx->raw.as<float>(), ctx->range_first,
+                                    dx.as<float>(), s));
+        count_launch(L);
+        TM_CUDA(cudaMemcpyAsync(exact, dx.p, pairs * sizeof(float), cudaMemcpyDeviceToHost, s));
+    }
+    uint32_t err = 0;
+    TM_CUDA(cudaMemcpyAsync(&err, L.counters.as<uint32_t>() + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    TM_CUDA(cudaStreamSynchronize(s));
+    g.release();
+    if (err != 0)
+        throw Failure{TM_ERR_TIMEOUT, "contraction kernel gave up waiting"};
+}
+
 // ---------------------------------------------------------------------------------
 extern "C" {
 
@@ -1597,6 +1809,95 @@ int tm_set_kernel(tm_ctx *ctx, int kernel)
     if (ctx->server && !ctx->server->stopped)
         return TM_ERR_STATE;
     ctx->kernel = kernel;
+    return TM_OK;
+}
+
+int tm_set_tiles(tm_ctx *ctx, int tiles)
+{
+    if (ctx == nullptr || tiles < TM_TILES_AUTO || tiles > TM_TILES_COLS_32)
+        return TM_ERR_ARGUMENT;
+    ctx->tiles = tiles;
+    return TM_OK;
+}
+
+int tm_autotune(tm_ctx *ctx, double *ms, int capacity)
+{
+    if (ctx == nullptr || capacity < 0 || (capacity > 0 && ms == nullptr))
+        return TM_ERR_ARGUMENT;
+    const int rc = guarded(ctx, [&] {
+        TM_CUDA(cudaSetDevice(ctx->device));
+        if (ctx->kernel == TM_KERNEL_FP32 || !tmb::umma_supported(0, 0, 0))
+            throw Failure{TM_ERR_STATE, "the tile shapes are those of the tensor-core kernel"};
+        // a synthetic record: a random walk of small steps plus noise (xorshift)
+        const uint64_t n = 1ull << 23;
+        std::vector<float> x(n);
+        uint64_t st = 0x9E3779B97F4A7C15ull;
+        auto rnd = [&] {
+            st ^= st << 13;
+            st ^= st >> 7;
+            st ^= st << 17;
+            return static_cast<float>((st >> 40) * (1.0 / 16777216.0)) - 0.5f;
+        };
+        float level = 0.0f;
+        for (uint64_t i = 0; i < n; i++)
+        {
+            level = 0.95f * level + rnd();
+            x[i] = level + 0.1f * rnd();
+        }
+        tm_ctx *tc = nullptr;
+        const int rc = tm_ctx_create(x.data(), n, ctx->device, &tc);
+        if (rc != TM_OK)
+            throw Failure{rc, "autotune context"};
+        std::unique_ptr<tm_ctx, int (*)(tm_ctx *)> hold(tc, tm_ctx_destroy);
+        const int ks[4] = {256, 1024, 4096, 16384};
+        std::vector<std::vector<float>> temps(128);
+        std::vector<tm_request> reqs(128);
+        double table[2][4][4];
+        for (int mixed = 0; mixed < 2; mixed++)
+            for (int ki = 0; ki < 4; ki++)
+            {
+                for (int t = 0; t < 128; t++)
+                {
+                    const int m = ks[ki] - (mixed && (t & 1) ? 16 : 0);
+                    temps[t].resize(static_cast<size_t>(m));
+                    for (int i = 0; i < m; i++)
+                        temps[t][i] = std::sin(0.003f * static_cast<float>(i) * (1.0f + 0.01f * t) +
+                                               1e-6f * static_cast<float>(i) * static_cast<float>(i));
+                    reqs[t] = tm_request{temps[t].data(), m, TM_MODE_THRESHOLD, 1, 0, 0.995f, 0u};
+                }
+                const double windows = static_cast<double>(n - static_cast<uint64_t>(ks[ki]) + 1);
+                for (int v = 0; v < 4; v++)
+                {
+                    tc->tiles = TM_TILES_ROWS + v;
+                    tm_batch b;
+                    create_batch(tc, tc->main, reqs.data(), 128, b);
+                    tm_result res;
+                    run_batch(tc, tc->main, b, res); // warm-up
+                    tc->main.profile = true;
+                    tc->main.prof_ms = 0.0;
+                    tc->main.prof_launches = 0;
+                    for (int r = 0; r < 2; r++)
+                        run_batch(tc, tc->main, b, res);
+                    tc->main.profile = false;
+                    const double per = tc->main.prof_ms / std::max<int64_t>(tc->main.prof_launches, 1);
+                    table[mixed][v][ki] = per * (33554432.0 / windows);
+                }
+            }
+        std::memcpy(ctx->tile_ms, table, sizeof(table));
+        for (int i = 0; i < std::min(capacity, 32); i++)
+            ms[i] = (&table[0][0][0])[i];
+    });
+    return rc == TM_OK ? 32 : rc;
+}
+
+int tm_set_tile_model(tm_ctx *ctx, const double *ms, int count)
+{
+    if (ctx == nullptr || ms == nullptr || count != 32)
+        return TM_ERR_ARGUMENT;
+    for (int i = 0; i < 32; i++)
+        if (!(ms[i] > 0.0) || !std::isfinite(ms[i]))
+            return TM_ERR_ARGUMENT;
+    std::memcpy(ctx->tile_ms, ms, sizeof(ctx->tile_ms));
     return TM_OK;
 }
 
@@ -1849,6 +2150,11 @@ int tm_bound_diagnostics(tm_ctx *ctx, const float *queries, int count, int m, fl
         {
             reqs[i] = tm_request{queries + static_cast<size_t>(i) * m, m, TM_MODE_THRESHOLD, 1, 0, 1.0f, 0u};
             idx[i] = i;
+        }
+        if (ctx->tiles >= TM_TILES_COLS_128 && ctx->kernel != TM_KERNEL_FP32 && tmb::umma_supported(m, count, 0))
+        {
+            bound_diagnostics_wm(ctx, m, idx, reqs, d, e, exact);
+            return;
         }
         GroupPlan g;
         uint64_t h2d = 0;

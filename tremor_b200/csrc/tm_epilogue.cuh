@@ -37,6 +37,7 @@ struct ScanArgs
     const TileInfo *tiles; // per 128-row tile: K blocks and distinct lengths
     int k_stride;          // row stride of the template arrays
     uint64_t n;            // samples of the waveform (P has n + 1 entries)
+    int col_tile;          // window-major kernel: templates per column tile (32, 64, 128); 0: row tiles
 };
 
 // Distance d of one (template, window) pair from its shifted dot product
@@ -114,6 +115,25 @@ __device__ __forceinline__ void stage_flush(Candidate *sbuf, uint32_t &n, int la
             cand[base + i] = sbuf[i];
     __syncwarp();
     n = 0;
+}
+
+// One candidate per lane (template t, window j) where `hit`, through the warp's staging
+// buffer (every lane must call it; kStageCap >= 32).
+template <uint32_t kStageCap>
+__device__ __forceinline__ void stage_emit_lane(bool hit, int lane, uint32_t t, uint32_t j, Candidate *sbuf,
+                                                uint32_t &n, Candidate *cand, uint32_t *count, uint32_t cap)
+{
+    static_assert(kStageCap >= 32, "a warp's hits must fit the staging buffer");
+    const unsigned b = __ballot_sync(0xffffffffu, hit);
+    if (b == 0u)
+        return;
+    const uint32_t total = (uint32_t)__popc(b);
+    if (n + total > kStageCap)
+        stage_flush(sbuf, n, lane, cand, count, cap);
+    if (hit)
+        sbuf[n + (uint32_t)__popc(b & ((1u << lane) - 1u))] = Candidate{t, j};
+    __syncwarp();
+    n += total;
 }
 
 // emit_candidates through the warp's staging buffer (every lane must call it).

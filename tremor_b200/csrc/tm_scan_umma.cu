@@ -639,30 +639,449 @@ done:
     }
 }
 
+
+// ---- window-major variant ----------------------------------------------------------
+//
+// The same split-BF16 contraction with the roles of the operands exchanged: 128 windows
+// on the MMA's M side (TMEM lanes) and NT templates on its N side (TMEM columns), for
+// groups whose templates are too few per length for 128-row template tiles (each tile's
+// K extent is its longest template, so a tile of mixed lengths wastes the difference).
+// Column tiles of NT = 32, 64 or 128 templates of similar length keep that waste small.
+//   A (windows): the Hankel strip, U[u][r][e] = split(x[j0 + k0 + 8u + r + e] - shift),
+//     u < 128/8 + 64/8, described with SBO = LBO = 128 bytes as for the B operand of
+//     k_scan_umma (the canonical K-major no-swizzle layout is the same for A and B).
+//   B (templates, K-major): TMA tiles of NT rows x 64 samples, SWIZZLE_128B, hi and lo.
+// Epilogue: a thread owns one window (its TMEM lane) and walks the tile's columns; the
+// column's template is warp-uniform, so its constants come from shared memory (staged
+// per tile) and mode branches do not diverge. Window statistics of each column's length
+// come from the resident prefix sums (prefix_stats), with the window-end sums of 8
+// columns loaded at once.
+
+struct ColParam // the epilogue's constants of one template column
+{
+    double inv_m;
+    float c_lin, s1, a1, a2, a3, a4, a5, a6, thr, qs;
+    int m, mode;
+    uint32_t wcount; // 0: padding column
+    int pad;
+};
+
+constexpr int WM_M = 128;                        // windows per tile
+constexpr int WM_STRIP = WM_M / 8 + KB / 8;      // 24 core matrices of 128 bytes
+constexpr int WM_A_BYTES = WM_STRIP * 128;
+
+template <int NT> struct SmemWM
+{
+    static constexpr int S = NT >= 128 ? 4 : (NT >= 64 ? 6 : 8);
+    static constexpr int B_BYTES_T = NT * KB * 2;
+    uint8_t b_hi[S][B_BYTES_T]; // 1024-byte aligned (swizzle atoms): NT * 128 is a multiple of 1024
+    uint8_t b_lo[S][B_BYTES_T];
+    uint8_t a_hi[S][WM_A_BYTES];
+    uint8_t a_lo[S][WM_A_BYTES];
+    ColParam cp[2][NT];
+    Candidate stage[8][64];
+    uint64_t full_a[S], full_b[S], empty[S];
+    uint64_t acc_full[2], acc_empty[2], par_ready[2], drain;
+    uint32_t tmem_base;
+    int abort;
+};
+
+static_assert(sizeof(SmemWM<128>) + 1024 <= 227 * 1024, "shared memory of k_scan_wm<128>");
+static_assert(sizeof(SmemWM<64>) + 1024 <= 227 * 1024, "shared memory of k_scan_wm<64>");
+static_assert(sizeof(SmemWM<32>) + 1024 <= 227 * 1024, "shared memory of k_scan_wm<32>");
+
+// Tile shift: the middle sample of the 128 windows (several lengths) or the mean of the
+// middle window (one length).
+template <bool MIXED> __device__ __forceinline__ float wm_shift(const ScanArgs &a, uint32_t j0)
+{
+    const uint32_t jm = min(j0 + WM_M / 2, a.W - 1);
+    return MIXED ? a.x[a.w0 + jm] : a.mean[jm];
+}
+
+// kind::f16 instruction descriptor: D F32, A and B BF16, both K-major, M = 128, N = n.
+__host__ __device__ constexpr uint32_t idesc_m128(int n)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(WM_M >> 4) << 24);
+}
+
+template <int NT>
+__device__ __forceinline__ void mma_n(uint32_t d, uint64_t a, uint64_t b, uint32_t accumulate)
+{
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "setp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
+                 "l"(a), "l"(b), "r"(idesc_m128(NT)), "r"(accumulate)
+                 : "memory");
+}
+
+struct WmArgs
+{
+    ScanArgs a;
+    int c_tiles, w_tiles, kblocks;
+    int *err;
+};
+
+// MIXED: templates of several lengths, statistics from the prefix sums, K blocks per
+// column tile (a.tiles); otherwise one length, the per-window statistics a.mean / a.inv
+// of that length and a.m_pad / 64 K blocks everywhere.
+template <int NT, bool MIXED>
+__global__ void __launch_bounds__(THREADS, 1)
+    k_scan_wm(const WmArgs wa, const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CUtensorMap map_lo)
+{
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    using Sm = SmemWM<NT>;
+    constexpr int STAGES = Sm::S;
+    constexpr uint32_t COLS = (NT < 32 ? 32 : NT);
+    Sm &sm = *reinterpret_cast<Sm *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const ScanArgs &a = wa.a;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long tiles = (long long)wa.c_tiles * wa.w_tiles;
+
+    if (threadIdx.x == 0)
+    {
+        for (int s = 0; s < STAGES; s++)
+        {
+            mbar_init(&sm.full_a[s], 1);
+            mbar_init(&sm.full_b[s], BUILDERS);
+            mbar_init(&sm.empty[s], 1);
+        }
+        for (int b = 0; b < 2; b++)
+        {
+            mbar_init(&sm.acc_full[b], 1);
+            mbar_init(&sm.acc_empty[b], EPI);
+            mbar_init(&sm.par_ready[b], EPI);
+        }
+        mbar_init(&sm.drain, 1);
+        sm.abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1)
+    {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(&sm.tmem_base)),
+                     "r"(2 * COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = sm.tmem_base;
+
+    if (warp == 0)
+    {
+        // ---- TMA producer: template column tiles (hi, lo) ----
+        if (lane == 0)
+        {
+            uint32_t it = 0;
+            for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x)
+            {
+                const int ct = (int)(tile / wa.w_tiles);
+                const int kblocks = MIXED ? a.tiles[ct].kb : wa.kblocks;
+                for (int kb = 0; kb < kblocks; kb++, it++)
+                {
+                    const int s = it % STAGES;
+                    if (!mbar_wait(&sm.empty[s], ((it / STAGES) & 1) ^ 1, sm.abort, wa.err, 21))
+                    {
+                        for (uint32_t i = it > STAGES ? it - STAGES : 0; i < it; i++)
+                            mbar_drain(&sm.full_a[i % STAGES], (i / STAGES) & 1);
+                        goto done;
+                    }
+                    mbar_expect_tx(&sm.full_a[s], 2 * Sm::B_BYTES_T);
+                    tma_load_2d(sm.b_hi[s], &map_hi, kb * KB, ct * NT, &sm.full_a[s]);
+                    tma_load_2d(sm.b_lo[s], &map_lo, kb * KB, ct * NT, &sm.full_a[s]);
+                }
+            }
+        }
+    }
+    else if (warp == 1)
+    {
+        // ---- MMA issuer ----
+        if (lane == 0)
+        {
+            uint32_t it = 0, tc = 0;
+            for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x, tc++)
+            {
+                const int buf = tc & 1;
+                if (!mbar_wait(&sm.acc_empty[buf], ((tc >> 1) & 1) ^ 1, sm.abort, wa.err, 22))
+                {
+                    mma_commit(&sm.drain);
+                    mbar_drain(&sm.drain, 0);
+                    goto done;
+                }
+                tc_fence_after();
+                const uint32_t d = tmem + (uint32_t)(buf * COLS);
+                const int kblocks = MIXED ? a.tiles[tile / wa.w_tiles].kb : wa.kblocks;
+                for (int kb = 0; kb < kblocks; kb++, it++)
+                {
+                    const int s = it % STAGES;
+                    const uint32_t ph = (it / STAGES) & 1;
+                    if (!mbar_wait(&sm.full_a[s], ph, sm.abort, wa.err, 23) ||
+                        !mbar_wait(&sm.full_b[s], ph, sm.abort, wa.err, 24))
+                    {
+                        mma_commit(&sm.drain);
+                        mbar_drain(&sm.drain, 0);
+                        goto done;
+                    }
+                    tc_fence_after();
+                    const uint32_t ah = saddr(sm.a_hi[s]), al = saddr(sm.a_lo[s]);
+                    const uint32_t bh = saddr(sm.b_hi[s]), bl = saddr(sm.b_lo[s]);
+#pragma unroll
+                    for (int kk = 0; kk < KB / 16; kk++)
+                    {
+                        const uint64_t dah = sdesc(ah + kk * 256, 128, 128, 0);
+                        const uint64_t dal = sdesc(al + kk * 256, 128, 128, 0);
+                        const uint64_t dbh = sdesc(bh + kk * 32, 16, 1024, 2);
+                        const uint64_t dbl = sdesc(bl + kk * 32, 16, 1024, 2);
+                        mma_n<NT>(d, dah, dbh, (kb | kk) != 0);
+                        mma_n<NT>(d, dah, dbl, 1);
+                        mma_n<NT>(d, dal, dbh, 1);
+                    }
+                    mma_commit(&sm.empty[s]);
+                }
+                mma_commit(&sm.acc_full[buf]);
+            }
+        }
+    }
+    else if (warp < 4)
+    {
+        // ---- strip builders (128 windows) ----
+        const int tid = threadIdx.x - 64;
+        uint32_t it = 0;
+        for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x)
+        {
+            const uint32_t j0 = (uint32_t)(tile % wa.w_tiles) * WM_M;
+            const float shift = wm_shift<MIXED>(a, j0);
+            const float *xw = a.x + a.w0 + j0;
+            const int kblocks = MIXED ? a.tiles[tile / wa.w_tiles].kb : wa.kblocks;
+            for (int kb = 0; kb < kblocks; kb++, it++)
+            {
+                const int s = it % STAGES;
+                if (!mbar_wait(&sm.empty[s], ((it / STAGES) & 1) ^ 1, sm.abort, wa.err, 25))
+                    goto done;
+                const float *xs = xw + kb * KB;
+                for (int row = tid; row < WM_STRIP * 8; row += BUILDERS)
+                {
+                    const int u = row >> 3, r = row & 7;
+                    float v[8], h[8], l[8];
+#pragma unroll
+                    for (int e = 0; e < 8; e++)
+                        v[e] = xs[8 * u + r + e] - shift;
+#pragma unroll
+                    for (int e = 0; e < 8; e++)
+                    {
+                        h[e] = __bfloat162float(__float2bfloat16_rn(v[e]));
+                        l[e] = v[e] - h[e];
+                    }
+                    uint4 hv, lv;
+                    hv.x = pack_bf16(h[0], h[1]);
+                    hv.y = pack_bf16(h[2], h[3]);
+                    hv.z = pack_bf16(h[4], h[5]);
+                    hv.w = pack_bf16(h[6], h[7]);
+                    lv.x = pack_bf16(l[0], l[1]);
+                    lv.y = pack_bf16(l[2], l[3]);
+                    lv.z = pack_bf16(l[4], l[5]);
+                    lv.w = pack_bf16(l[6], l[7]);
+                    *reinterpret_cast<uint4 *>(&sm.a_hi[s][u * 128 + r * 16]) = hv;
+                    *reinterpret_cast<uint4 *>(&sm.a_lo[s][u * 128 + r * 16]) = lv;
+                }
+                fence_proxy_async();
+                mbar_arrive(&sm.full_b[s]);
+            }
+        }
+    }
+    else
+    {
+        // ---- epilogue (8 warps): warp (quarter, half) holds windows 32 quarter + lane and
+        // the half of the tile's columns ----
+        const int quarter = warp & 3;
+        const int ew = warp - 4;
+        const int half = ew >> 2;
+        const int et = threadIdx.x - 128;
+        const float center_f = (float)a.center;
+        uint32_t tc = 0, staged = 0;
+        for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x, tc++)
+        {
+            const int buf = tc & 1;
+            const int ct = (int)(tile / wa.w_tiles);
+            const uint32_t j0 = (uint32_t)(tile % wa.w_tiles) * WM_M;
+            if (et < NT)
+            {
+                const int t = ct * NT + et;
+                ColParam c{};
+                if (t < a.T)
+                {
+                    const TemplParam &p = a.tp[t];
+                    c.inv_m = p.inv_m;
+                    c.c_lin = p.c_lin;
+                    c.s1 = p.s1;
+                    c.a1 = p.a1_main;
+                    c.a2 = p.a2;
+                    c.a3 = p.a3;
+                    c.a4 = p.a4;
+                    c.a5 = p.a5;
+                    c.a6 = p.a6;
+                    c.thr = p.thr_ed;
+                    c.qs = p.qs;
+                    c.m = p.m;
+                    c.mode = p.mode;
+                    c.wcount = MIXED ? p.wcount : 1u; // one length: every real row is searched
+                }
+                else
+                {
+                    c.m = 1;
+                    c.thr = -kFltMax;
+                }
+                sm.cp[buf][et] = c;
+            }
+            mbar_arrive(&sm.par_ready[buf]);
+            if (!mbar_wait_warp(&sm.par_ready[buf], (tc >> 1) & 1, sm.abort, wa.err, 27))
+                goto done;
+            const uint32_t j = j0 + (uint32_t)(quarter * 32 + lane);
+            const bool in = j < a.W;
+            double2 pj = make_double2(0.0, 0.0);
+            uint32_t runj = 0;
+            bool miss = !in;
+            float wmean = 0.0f, winv = 0.0f; // one length: the window's statistics (inv 0: not searched)
+            if (MIXED)
+            {
+                if (in)
+                {
+                    pj = a.P[a.w0 + j];
+                    runj = a.run[a.w0 + j];
+                    miss = a.raw[a.w0 + j] == kMissing;
+                }
+            }
+            else if (in)
+            {
+                wmean = a.mean[j];
+                winv = a.inv[j];
+                miss = winv == 0.0f;
+            }
+            const float a2 = (float)pj.y;
+            const float shift = wm_shift<MIXED>(a, j0);
+            const size_t bucket = j0 / kBucket;
+            if (!mbar_wait_warp(&sm.acc_full[buf], (tc >> 1) & 1, sm.abort, wa.err, 26))
+                goto done;
+            tc_fence_after();
+            const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(buf * COLS);
+            for (int g = half * (NT / 2); g < (half + 1) * (NT / 2); g += 8)
+            {
+                double2 pe[8];
+#pragma unroll
+                for (int i = 0; i < 8; i++)
+                {
+                    const ColParam &c = sm.cp[buf][g + i];
+                    const bool ok = MIXED && !miss && j < c.wcount && runj < (uint32_t)c.m;
+                    pe[i] = ok ? a.P[a.w0 + j + (uint32_t)c.m] : make_double2(0.0, 0.0);
+                }
+                float v[8];
+                tmem_ld8(taddr + g, v);
+#pragma unroll
+                for (int i = 0; i < 8; i++)
+                {
+                    const ColParam &c = sm.cp[buf][g + i];
+                    const uint32_t t = (uint32_t)(ct * NT + g + i);
+                    const bool ok = MIXED ? (!miss && j < c.wcount && runj < (uint32_t)c.m) : (!miss && c.wcount > 0);
+                    bool hit = false;
+                    float up = inf_f(), lo = inf_f();
+                    if (!MIXED && ok)
+                    {
+                        const float ms = wmean - shift;
+                        const float cross = (v[i] - ms * c.s1) * winv;
+                        const float dd = c.c_lin - 2.0f * cross;
+                        const float r = ms * winv, r0 = wmean * winv;
+                        const float e = c.a1 * sqrtf(1.0f + r * r) + c.a2 + c.a3 * fmaxf(dd, 0.0f) +
+                                        c.a4 * (1.0f + 2.0f * r0 * r0) + c.a5 * r0 * r0 +
+                                        c.a6 * (fabsf(wmean) + fabsf(shift)) * winv;
+                        if (a.dbg_d != nullptr)
+                        {
+                            a.dbg_d[(size_t)t * a.W + j] = dd;
+                            a.dbg_e[(size_t)t * a.W + j] = e;
+                        }
+                        up = dd + e;
+                        lo = dd - e;
+                        hit = lo <= c.thr;
+                    }
+                    else if (ok)
+                    {
+                        WindowStats ws;
+                        if (prefix_stats(pj, a2, pe[i], a.w0 + j, c.m, c.inv_m, center_f, ws) == 0)
+                        {
+                            const float ms = ws.mu - shift;
+                            const float cross = (v[i] - ms * c.s1) * ws.iv;
+                            const float dd = c.c_lin - 2.0f * cross;
+                            const float r = ms * ws.iv, r0 = ws.mu * ws.iv;
+                            const float e = c.a1 * sqrtf(1.0f + r * r) + c.a2 + c.a3 * fmaxf(dd, 0.0f) +
+                                            c.a5 * r0 * r0 + c.a6 * (fabsf(ws.mu) + fabsf(shift)) * ws.iv +
+                                            stats_error(ws, c.m, c.qs, c.s1);
+                            if (a.dbg_d != nullptr)
+                            {
+                                a.dbg_d[(size_t)t * a.W + j] = dd;
+                                a.dbg_e[(size_t)t * a.W + j] = e;
+                            }
+                            up = dd + e;
+                            lo = dd - e;
+                            hit = lo <= c.thr;
+                        }
+                        else
+                        {
+                            lo = -inf_f(); // statistics not trustworthy: exact re-scoring decides
+                            hit = true;
+                        }
+                    }
+                    if (c.mode == 1) // kNN: bucket minima over the warp's 32 windows
+                    {
+                        const uint32_t ku = __reduce_min_sync(0xffffffffu, float_key(up));
+                        const uint32_t kl = __reduce_min_sync(0xffffffffu, float_key(lo));
+                        if (lane == 0 && (ku != float_key(inf_f()) || kl != float_key(inf_f())))
+                        {
+                            atomicMin(&a.bmin_u[(size_t)t * a.nb + bucket], ku);
+                            atomicMin(&a.bmin_l[(size_t)t * a.nb + bucket], kl);
+                        }
+                    }
+                    else
+                        stage_emit_lane<64>(hit, lane, t, j, sm.stage[ew], staged, a.cand, a.cand_count, a.cand_cap);
+                }
+            }
+            tc_fence_before();
+            mbar_arrive(&sm.acc_empty[buf]);
+            stage_flush(sm.stage[ew], staged, lane, a.cand, a.cand_count, a.cand_cap);
+        }
+    }
+done:
+    __syncwarp();
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1)
+    {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * COLS));
+    }
+}
+
 // ---- host side -------------------------------------------------------------------
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
 {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    if (fn == nullptr)
-    {
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
         cudaDriverEntryPointQueryResult q;
         void *p = nullptr;
         if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    }
+            return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        return static_cast<PFN_cuTensorMapEncodeTiled_v12000>(nullptr);
+    }();
     return fn;
 }
 
-bool make_map(CUtensorMap *map, const void *base, int rows, int cols)
+// BF16 row-major [rows][cols] operand, boxes of 64 samples x box_rows rows, 128-byte swizzle.
+bool make_map(CUtensorMap *map, const void *base, int rows, int cols, int box_rows = TM)
 {
     auto fn = encode_fn();
     if (fn == nullptr)
         return false;
     const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
     const cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
-    const cuuint32_t box[2] = {(cuuint32_t)KB, (cuuint32_t)TM};
+    const cuuint32_t box[2] = {(cuuint32_t)KB, (cuuint32_t)box_rows};
     const cuuint32_t estr[2] = {1, 1};
     return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box, estr,
               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -706,18 +1125,16 @@ cudaError_t launch_scan_umma(const ScanArgs &a, cudaStream_t s)
     ua.kblocks = a.m_pad / KB;
     ua.err = a.err;
     const size_t smem = (mixed ? sizeof(SmemT<true>) : sizeof(SmemT<false>)) + 1024;
-    static bool attr = false;
-    if (!attr)
-    {
+    static const cudaError_t attr = [] {
         cudaError_t e = cudaFuncSetAttribute(k_scan_umma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)(sizeof(SmemT<false>) + 1024));
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(k_scan_umma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)(sizeof(SmemT<true>) + 1024));
-        if (e != cudaSuccess)
-            return e;
-        attr = true;
-    }
+        return e;
+    }();
+    if (attr != cudaSuccess)
+        return attr;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -727,6 +1144,75 @@ cudaError_t launch_scan_umma(const ScanArgs &a, cudaStream_t s)
         k_scan_umma<true><<<grid, THREADS, smem, s>>>(ua, mh, ml);
     else
         k_scan_umma<false><<<grid, THREADS, smem, s>>>(ua, mh, ml);
+    return cudaGetLastError();
+}
+
+// Window-major contraction in column tiles of a.col_tile templates: a mixed-length group
+// (a.tiles: one TileInfo per column tile, K blocks only; statistics from the prefix sums)
+// or, when a.tiles is null, one length (a.mean / a.inv, a.m_pad samples).
+template <int NT> static cudaError_t wm_attr()
+{
+    using namespace umma;
+    cudaError_t e = cudaFuncSetAttribute(k_scan_wm<NT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(sizeof(SmemWM<NT>) + 1024));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_scan_wm<NT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(sizeof(SmemWM<NT>) + 1024));
+    return e;
+}
+
+template <int NT>
+static void wm_launch(bool mixed, int grid, const umma::WmArgs &wa, const CUtensorMap &mh, const CUtensorMap &ml,
+                      cudaStream_t s)
+{
+    using namespace umma;
+    if (mixed)
+        k_scan_wm<NT, true><<<grid, THREADS, sizeof(SmemWM<NT>) + 1024, s>>>(wa, mh, ml);
+    else
+        k_scan_wm<NT, false><<<grid, THREADS, sizeof(SmemWM<NT>) + 1024, s>>>(wa, mh, ml);
+}
+
+cudaError_t launch_scan_wm(const ScanArgs &a, cudaStream_t s)
+{
+    using namespace umma;
+    const int NT = a.col_tile;
+    const bool mixed = a.tiles != nullptr;
+    if ((NT != 32 && NT != 64 && NT != 128) || a.q_hi == nullptr || a.q_lo == nullptr || a.err == nullptr ||
+        a.t_rows % NT != 0)
+        return cudaErrorInvalidValue;
+    if (mixed ? (a.P == nullptr || a.run == nullptr || a.raw == nullptr) : (a.mean == nullptr || a.inv == nullptr))
+        return cudaErrorInvalidValue;
+    const int stride = mixed ? a.k_stride : a.m_pad;
+    CUtensorMap mh, ml;
+    if (!make_map(&mh, a.q_hi, a.t_rows, stride, NT) || !make_map(&ml, a.q_lo, a.t_rows, stride, NT))
+        return cudaErrorInvalidValue;
+    WmArgs wa;
+    wa.a = a;
+    wa.c_tiles = a.t_rows / NT;
+    wa.w_tiles = (int)((a.W + WM_M - 1) / WM_M);
+    wa.kblocks = a.m_pad / KB;
+    wa.err = a.err;
+    static const cudaError_t attr = [] {
+        cudaError_t e = wm_attr<32>();
+        if (e == cudaSuccess)
+            e = wm_attr<64>();
+        if (e == cudaSuccess)
+            e = wm_attr<128>();
+        return e;
+    }();
+    if (attr != cudaSuccess)
+        return attr;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long long tiles = (long long)wa.c_tiles * wa.w_tiles;
+    const int grid = (int)std::min<long long>(tiles, sms);
+    if (NT == 32)
+        wm_launch<32>(mixed, grid, wa, mh, ml, s);
+    else if (NT == 64)
+        wm_launch<64>(mixed, grid, wa, mh, ml, s);
+    else
+        wm_launch<128>(mixed, grid, wa, mh, ml, s);
     return cudaGetLastError();
 }
 
