@@ -168,6 +168,15 @@ def peaks():
     return 1590.0, 6650.0, 'fallback'
 
 
+def peaks_sustained():
+    """The measured sustained BF16 figure (a seconds-long GEMM loop under the power cap),
+    or None."""
+    path = ROOT / 'MEASURED_PEAKS.json'
+    if path.exists():
+        return json.loads(path.read_text()).get('bf16_tflops_sustained')
+    return None
+
+
 def traffic_for(kernel, workload):
     """Per-launch DRAM bytes of the kernel from the committed ncu summary, or None."""
     path = ROOT / 'profiles' / 'traffic.txt'
@@ -464,6 +473,8 @@ def run_ours(args, w):
     kernel = {'auto': tb.KERNEL_AUTO, 'fp32': tb.KERNEL_FP32, 'bf16': tb.KERNEL_SPLIT_BF16}[args.kernel]
     ctx = tb.Context(x, device=local)
     ctx.set_kernel(kernel)
+    ctx.set_tiles({'auto': tb.TILES_AUTO, 'rows': tb.TILES_ROWS, 'cols128': tb.TILES_COLS_128,
+                   'cols64': tb.TILES_COLS_64, 'cols32': tb.TILES_COLS_32}[args.tiles])
     t0 = time.time()
     if w['mode'] != 'mixed':
         ctx.prepare_length(w['m'])
@@ -559,6 +570,11 @@ def run_ours(args, w):
             roof = {'bound': 'fp32', 'achieved': achieved, 'peak': nominal, 'unit': 'TFLOP/s',
                     'peak_note': 'nominal FP32 FMA peak (148 SMs x 128 lanes x 2 x 1.965 GHz); no measured FP32 figure'}
         roof['frac'] = achieved / roof['peak']
+        if kname != 'k_scan_fp32':
+            sustained = peaks_sustained()
+            if sustained:
+                roof['peak_sustained'] = sustained / 3.0
+                roof['frac_sustained'] = achieved / (sustained / 3.0)
         tb_bytes = traffic_for(kname, args.workload)
         roof['traffic'] = tb_bytes
         roof['kernel'] = kname
@@ -577,7 +593,7 @@ def run_ours(args, w):
                 'data': 'synthetic',
                 'config': {'workload': args.workload, 'n': w['n'], 'templates': w['q'], 'templates_per_step': per,
                            'm': w['m'], 'mode': w['mode'], 'k': w['k'], 'merge': w['merge'], 'corr': w['corr'],
-                           'events': w['events'], 'seed': w['seed'], 'kernel': args.kernel,
+                           'events': w['events'], 'seed': w['seed'], 'kernel': args.kernel, 'tiles': args.tiles,
                            'l2': 'inputs larger than L2 (waveform 4n bytes)', 'parallelism': f'replicas x{world}'},
                 'roofline': roof,
                 'cpu_baseline': {'value': cpu_v, 'unit': UNIT, **cpu_info},
@@ -603,6 +619,8 @@ def main():
     p.add_argument('--impl', choices=['ours', 'reference'], default='ours')
     p.add_argument('--workload', choices=sorted(WORKLOADS), default='precision')
     p.add_argument('--kernel', choices=['auto', 'fp32', 'bf16'], default='auto')
+    p.add_argument('--tiles', choices=['auto', 'rows', 'cols128', 'cols64', 'cols32'], default='auto',
+                   help='tile shape of mixed-length groups (TILES_*)')
     p.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline leg')
     p.add_argument('--rate', type=float, default=0.0, help='serving: Poisson arrival rate (req/s)')
     p.add_argument('--requests', type=int, default=0, help='serving: requests in the timed stream')
