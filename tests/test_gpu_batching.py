@@ -189,3 +189,36 @@ def test_large_k_selected_on_host():
     with tb.Context(x) as ctx:
         answers = ctx.scan_batch(reqs)
     _check(x, reqs, answers)
+
+
+def _block_waveform(seed):
+    """Three prefix blocks (65536 samples) and a bit: a level step at each block boundary,
+    a 1e5-fold loud stretch in block 0, missing samples; many windows cross a boundary."""
+    from tremor_b200 import synth
+    rng = np.random.default_rng(seed)
+    n = 3 * 65536 + 5000
+    x = synth.ar2_waveform(n, rng)
+    x[65536:131072] += np.float32(1000.0)
+    x[131072:] -= np.float32(500.0)
+    x[20000:24000] *= np.float32(1e5)
+    x[rng.integers(0, n, 40)] = tb.MISSING_VALUE
+    return x
+
+
+@pytest.mark.parametrize('tiles', [tb.TILES_ROWS, tb.TILES_COLS_64])
+def test_prefix_blocks_and_loud_event(tiles):
+    """Statistics from block-local prefix sums across block boundaries with level steps, and
+    after a loud event: answers equal the oracle's."""
+    x = _block_waveform(41)
+    rng = np.random.default_rng(42)
+    reqs = []
+    for i, m in enumerate([16384, 8000, 4096, 1000, 333, 64, 16384, 2048]):
+        p = int(rng.integers(60000, 140000))
+        t = x[p:p + m].copy()
+        t[t == tb.MISSING_VALUE] = 0.0
+        reqs.append(tb.Request(t, tb.MODE_KNN, k=3, merge_offset=m // 2) if i % 2 == 0
+                    else tb.Request(t, tb.MODE_THRESHOLD, correlation=0.7))
+    with tb.Context(x) as ctx:
+        ctx.set_tiles(tiles)
+        answers = ctx.scan_batch(reqs)
+    _check(x, reqs, answers)

@@ -51,3 +51,22 @@ def test_bound_holds_window_major(tiles, m):
     assert ok.sum() > 0.9 * ok.size * 0.5
     err = np.abs(d[ok].astype(np.float64) - exact[ok].astype(np.float64))
     assert np.all(err <= e[ok]), (m, float(np.max(err / e[ok])))
+
+
+@pytest.mark.parametrize('m', [100, 4096, 16384])
+def test_bound_holds_across_prefix_blocks(m):
+    """The window-major kernel's bound with block-local prefix sums, on a record with level
+    steps at the block boundaries and a 1e5-fold loud stretch in block 0: the bound holds,
+    and windows two blocks after the loud stretch keep trustworthy statistics (the prefix
+    sums' error bound is local)."""
+    from tests.test_gpu_batching import _block_waveform
+    x = _block_waveform(70 + m)
+    q = _templates(x, m, np.random.default_rng(m + 71), 4)
+    with tb.Context(x) as ctx:
+        ctx.set_tiles(tb.TILES_COLS_64)
+        d, e, exact = ctx.bound_diagnostics(q)
+    ok = np.isfinite(d) & (exact < np.float32(3.0e38))
+    err = np.abs(d[ok].astype(np.float64) - exact[ok].astype(np.float64))
+    assert np.all(err <= e[ok]), (m, float(np.max(err / e[ok])))
+    later = ok[:, 2 * 65536:2 * 65536 + 40000]
+    assert later.mean() > 0.95, float(later.mean())

@@ -30,6 +30,7 @@
 #include "tm_epilogue.cuh"
 #include "tm_host.h"
 #include "tm_internal.cuh"
+#include "tm_prefix.cuh"
 
 namespace tmb {
 cudaError_t launch_clean(const float *raw, float *clean, uint64_t n, uint64_t n_total, cudaStream_t s);
@@ -50,12 +51,16 @@ cudaError_t launch_passb(const uint2 *list, uint32_t items, const float *x, cons
                          Candidate *cand, uint32_t *cand_count, uint32_t cand_cap, cudaStream_t s);
 cudaError_t launch_rescore(const Candidate *cand, uint32_t count, const TemplParam *tp, const float *q,
                            const int *order, const float *raw, uint64_t w0, float *dist, cudaStream_t s);
-cudaError_t launch_prefix(const float *clean, uint64_t n, double c, double2 *totals, double2 *P, uint16_t *run,
-                          uint16_t *run_tmp, cudaStream_t s);
+uint32_t prefix_chunks(uint64_t n);
+cudaError_t launch_prefix_totals(const float *clean, uint64_t n, const double *centres, double2 *totals,
+                                 cudaStream_t s);
+cudaError_t launch_prefix_sums(const float *clean, uint64_t n, const double *centres, double2 *totals,
+                               double2 *block_totals, double2 *Q, cudaStream_t s);
+cudaError_t launch_runs(const float *clean, uint64_t n, uint16_t *run, uint16_t *run_tmp, cudaStream_t s);
 cudaError_t launch_passb_mixed(const uint2 *list, uint32_t items, const float *x, const float *raw, const double2 *P,
-                               const uint16_t *run, double center, const float *q, const TemplParam *tp,
-                               const uint32_t *tkey, uint64_t w0, Candidate *cand, uint32_t *cand_count,
-                               uint32_t cand_cap, cudaStream_t s);
+                               const double2 *PT, const double *PC, const uint16_t *run, const float *q,
+                               const TemplParam *tp, const uint32_t *tkey, uint64_t w0, Candidate *cand,
+                               uint32_t *cand_count, uint32_t cand_cap, cudaStream_t s);
 cudaError_t launch_answer_keys(const Candidate *cand, const float *dist, uint32_t count, const TemplParam *tp,
                                unsigned long long *keys, float *vals, uint32_t *kept, cudaStream_t s);
 size_t answer_sort_scratch(uint32_t count, int T);
@@ -294,9 +299,9 @@ struct tm_ctx
     std::map<int, std::unique_ptr<LengthStats>> lengths;
     uint64_t use_clock = 0;
     DevBuf suf; // window-statistics scratch (per-length statistics)
-    // length-independent statistics (mixed-length batches): FP64 prefix sums, constant runs
-    DevBuf prefix, run;
-    double center = 0.0;
+    // length-independent statistics (mixed-length batches): block-local FP64 prefix sums,
+    // their block totals and centres, constant runs
+    DevBuf prefix, ptot, pcen, run;
     bool prefix_ready = false;
     std::string err;
     Lane main;                      // the synchronous calls' lane
@@ -562,26 +567,42 @@ void ensure_prefix(tm_ctx *ctx, Lane &L)
         return;
     cudaStream_t s = L.stream;
     const uint64_t n = ctx->n;
-    const uint64_t chunks = (n + 8191) / 8192;
+    const uint32_t chunks = tmb::prefix_chunks(n);
+    const uint64_t blocks = (n + tmb::kPrefixBlock - 1) / tmb::kPrefixBlock;
     // zero tail: the contraction kernels read window-end sums in fixed-size chunks that may
     // run past n (values there belong to no window and are never used)
     ctx->prefix.reserve(sizeof(double2) * (n + 1 + tmb::kStagePad));
     TM_CUDA(cudaMemsetAsync(ctx->prefix.p, 0, sizeof(double2) * (n + 1 + tmb::kStagePad), s));
+    // one entry past the last block: a window ending at n = blocks x kPrefixBlock reads it
+    ctx->ptot.reserve(sizeof(double2) * (blocks + 1));
+    ctx->pcen.reserve(sizeof(double) * (blocks + 1));
+    TM_CUDA(cudaMemsetAsync(ctx->ptot.p, 0, sizeof(double2) * (blocks + 1), s));
     ctx->run.reserve(sizeof(uint16_t) * n);
     DevBuf totals, run_tmp;
     totals.reserve(sizeof(double2) * chunks);
     run_tmp.reserve(sizeof(uint16_t) * n);
-    // pass 1 without centring gives the mean; pass 2 centres on it
-    TM_CUDA(tmb::launch_prefix(ctx->clean.as<float>(), n, 0.0, totals.as<double2>(), ctx->prefix.as<double2>(),
-                               ctx->run.as<uint16_t>(), run_tmp.as<uint16_t>(), s));
-    double2 last;
-    TM_CUDA(cudaMemcpyAsync(&last, ctx->prefix.as<double2>() + n, sizeof(double2), cudaMemcpyDeviceToHost, s));
+    // centres: the mean of each block, from uncentred chunk sums
+    TM_CUDA(tmb::launch_prefix_totals(ctx->clean.as<float>(), n, nullptr, totals.as<double2>(), s));
+    std::vector<double2> ct(chunks);
+    TM_CUDA(cudaMemcpyAsync(ct.data(), totals.p, sizeof(double2) * chunks, cudaMemcpyDeviceToHost, s));
     TM_CUDA(cudaStreamSynchronize(s));
-    ctx->center = last.x / static_cast<double>(n);
-    TM_CUDA(tmb::launch_prefix(ctx->clean.as<float>(), n, ctx->center, totals.as<double2>(),
-                               ctx->prefix.as<double2>(), ctx->run.as<uint16_t>(), run_tmp.as<uint16_t>(), s));
+    const uint64_t per_block = tmb::kPrefixBlock / 8192;
+    std::vector<double> centres(blocks + 1, 0.0);
+    for (uint64_t b = 0; b < blocks; b++)
+    {
+        double sum = 0.0;
+        for (uint64_t c = b * per_block; c < std::min<uint64_t>(chunks, (b + 1) * per_block); c++)
+            sum += ct[c].x;
+        const uint64_t count = std::min<uint64_t>(tmb::kPrefixBlock, n - b * tmb::kPrefixBlock);
+        centres[b] = sum / static_cast<double>(count);
+    }
+    centres[blocks] = blocks > 0 ? centres[blocks - 1] : 0.0;
+    TM_CUDA(cudaMemcpyAsync(ctx->pcen.p, centres.data(), sizeof(double) * (blocks + 1), cudaMemcpyHostToDevice, s));
+    TM_CUDA(tmb::launch_prefix_sums(ctx->clean.as<float>(), n, ctx->pcen.as<double>(), totals.as<double2>(),
+                                    ctx->ptot.as<double2>(), ctx->prefix.as<double2>(), s));
+    TM_CUDA(tmb::launch_runs(ctx->clean.as<float>(), n, ctx->run.as<uint16_t>(), run_tmp.as<uint16_t>(), s));
     TM_CUDA(cudaStreamSynchronize(s));
-    count_launch(L, 2 * 16);
+    count_launch(L, 4 + 13);
     totals.release();
     run_tmp.release();
     ctx->prefix_ready = true;
@@ -1216,8 +1237,9 @@ void execute_group_mixed(tm_ctx *ctx, Lane &L, GroupPlan &g, tm_result &res)
         a.err = reinterpret_cast<int *>(d_cand_count + 2);
         a.raw = ctx->raw.as<float>();
         a.P = ctx->prefix.as<double2>();
+        a.PT = ctx->ptot.as<double2>();
+        a.PC = ctx->pcen.as<double>();
         a.run = ctx->run.as<uint16_t>();
-        a.center = ctx->center;
         a.tiles = g.d_tiles.as<tmb::TileInfo>();
         a.k_stride = g.k_stride;
         a.n = ctx->n;
@@ -1259,8 +1281,9 @@ void execute_group_mixed(tm_ctx *ctx, Lane &L, GroupPlan &g, tm_result &res)
             if (hc[1] > L.list_cap)
                 throw Failure{TM_ERR_NO_MEMORY, "bucket list overflow"};
             TM_CUDA(tmb::launch_passb_mixed(L.list.as<uint2>(), hc[1], ctx->clean.as<float>(),
-                                            ctx->raw.as<float>(), ctx->prefix.as<double2>(), ctx->run.as<uint16_t>(),
-                                            ctx->center, g.q.as<float>(), g.tp.as<TemplParam>(),
+                                            ctx->raw.as<float>(), ctx->prefix.as<double2>(), ctx->ptot.as<double2>(),
+                                            ctx->pcen.as<double>(), ctx->run.as<uint16_t>(), g.q.as<float>(),
+                                            g.tp.as<TemplParam>(),
                                             L.tkey.as<uint32_t>(), w0, L.cand.as<Candidate>(), d_cand_count,
                                             L.cand_cap, s));
             if (hc[1] > 0)
@@ -1711,8 +1734,9 @@ static void bound_diagnostics_wm(tm_ctx *ctx, int m, const std::vector<int> &idx
     a.dbg_e = de.as<float>();
     a.raw = ctx->raw.as<float>();
     a.P = ctx->prefix.as<double2>();
+    a.PT = ctx->ptot.as<double2>();
+    a.PC = ctx->pcen.as<double>();
     a.run = ctx->run.as<uint16_t>();
-    a.center = ctx->center;
     a.tiles = g.d_tiles.as<tmb::TileInfo>();
     a.k_stride = g.k_stride;
     a.n = ctx->n;
@@ -1794,7 +1818,7 @@ int tm_ctx_destroy(tm_ctx *ctx)
         kv.second->inv.release();
         kv.second->flags.release();
     }
-    for (DevBuf *b : {&ctx->prefix, &ctx->run, &ctx->raw, &ctx->clean, &ctx->suf})
+    for (DevBuf *b : {&ctx->prefix, &ctx->ptot, &ctx->pcen, &ctx->run, &ctx->raw, &ctx->clean, &ctx->suf})
         b->release();
     delete ctx;
     return TM_OK;

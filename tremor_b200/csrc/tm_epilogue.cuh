@@ -31,9 +31,10 @@ struct ScanArgs
     float *dbg_e;          //   [T][W]; null in searches
     // templates of several lengths in one tile (statistics from prefix sums, tm_prefix.cu)
     const float *raw;      // raw waveform (missing first samples)
-    const double2 *P;      // FP64 prefix sums of the centred waveform, n + 1
+    const double2 *P;      // block-local FP64 prefix sums Q, n + 1 (tm_prefix.cu)
+    const double2 *PT;     //   their block totals
+    const double *PC;      //   and block centres
     const uint16_t *run;   // constant-run lengths
-    double center;
     const TileInfo *tiles; // per 128-row tile: K blocks and distinct lengths
     int k_stride;          // row stride of the template arrays
     uint64_t n;            // samples of the waveform (P has n + 1 entries)

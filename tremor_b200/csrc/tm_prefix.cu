@@ -1,23 +1,27 @@
-// Length-independent window statistics: FP64 prefix sums of the waveform and the
-// length of the run of identical samples starting at every sample.
+// Length-independent window statistics: block-local FP64 prefix sums of the waveform and
+// the length of the run of identical samples starting at every sample.
 //
-// P[i] = (sum_{t<i} (x_t - c), sum_{t<i} (x_t - c)^2), i = 0..n, with c the mean of the
-// clean waveform (missing samples are 0) so that an offset does not inflate the sums.
-// A window [j, j+m) then has s1 = P1[j+m] - P1[j] and s2 = P2[j+m] - P2[j] for any m,
-// which is what lets templates of different lengths share one contraction tile. The
-// subtraction can cancel (a quiet window after loud samples); every use bounds that
-// error (window_stats_from_prefix in tm_prefix.cuh) and hands doubtful windows to the
-// exact re-scoring.
+// The record is cut into blocks of kPrefixBlock samples, each with its own centre c_b (the
+// block's mean, FP64). Within a block the sums restart:
+//   Q[i] = (sum (x_t - c_b), sum (x_t - c_b)^2) over t from the start of i's block to i - 1,
+// so Q[i] = 0 at every block start; T[b] holds block b's totals. A window [j, j + m) with
+// m <= kPrefixBlock lies in one block or in two adjacent ones, so its sums come from at
+// most one block total and two prefix values of those blocks (window_prefix_stats,
+// tm_prefix.cuh). Their rounding errors are bounded by the magnitudes of those blocks
+// alone: a loud stretch inflates the bounds of the windows near it, not of the rest of the
+// record, and a block's centre follows a drifting offset.
 //
 // run[i] = number of consecutive samples equal to clean[i] starting at i (capped at
 // 65535): a window is constant, hence not searchable (std 0 in the reference), exactly
 // when run[j] >= m. Constant stretches (gaps filled with zeros, clipped data) are
 // recognised without two-pass statistics.
-#include "tm_internal.cuh"
+#include "tm_prefix.cuh"
 
 namespace tmb {
 
 constexpr int PX_THREADS = 1024, PX_PER_THREAD = 8, PX_CHUNK = PX_THREADS * PX_PER_THREAD;
+constexpr int PX_CHUNKS_PER_BLOCK = kPrefixBlock / PX_CHUNK;
+static_assert(kPrefixBlock % PX_CHUNK == 0, "chunks tile the prefix blocks");
 
 __device__ __forceinline__ double2 add2(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 
@@ -53,9 +57,12 @@ __device__ double2 block_scan(double2 v, double2 *warp_tot)
     return v;
 }
 
-__device__ __forceinline__ double2 chunk_values(const float *__restrict__ clean, uint64_t n, double c, uint64_t base,
-                                                double2 *vals)
+// The centred values of one thread's 8 samples (centres: one per prefix block, or null
+// for 0) and their sum.
+__device__ __forceinline__ double2 chunk_values(const float *__restrict__ clean, uint64_t n,
+                                                const double *__restrict__ centres, uint64_t base, double2 *vals)
 {
+    const double c = centres ? centres[base >> kPrefixBlockLog] : 0.0; // 8 samples never straddle a block
     double2 s = make_double2(0.0, 0.0);
 #pragma unroll
     for (int k = 0; k < PX_PER_THREAD; k++)
@@ -69,60 +76,58 @@ __device__ __forceinline__ double2 chunk_values(const float *__restrict__ clean,
 }
 
 // Pass 1: per-chunk totals.
-__global__ void __launch_bounds__(PX_THREADS) k_prefix_totals(const float *__restrict__ clean, uint64_t n, double c,
+__global__ void __launch_bounds__(PX_THREADS) k_prefix_totals(const float *__restrict__ clean, uint64_t n,
+                                                              const double *__restrict__ centres,
                                                               double2 *__restrict__ totals)
 {
     __shared__ double2 warp_tot[32];
     double2 vals[PX_PER_THREAD];
     const uint64_t base = (uint64_t)blockIdx.x * PX_CHUNK + (uint64_t)threadIdx.x * PX_PER_THREAD;
-    const double2 s = block_scan(chunk_values(clean, n, c, base, vals), warp_tot);
+    const double2 s = block_scan(chunk_values(clean, n, centres, base, vals), warp_tot);
     if (threadIdx.x == blockDim.x - 1)
         totals[blockIdx.x] = s;
 }
 
-// Pass 2 (one block): exclusive scan of the chunk totals, in place.
-__global__ void __launch_bounds__(PX_THREADS) k_prefix_scan_totals(double2 *__restrict__ totals, uint32_t chunks)
+// Pass 2: within each prefix block, the exclusive scan of its chunks' totals (in place),
+// and the block's totals T[b]. One thread per prefix block (8 chunks each).
+__global__ void k_prefix_blocks(double2 *__restrict__ totals, uint32_t chunks, uint32_t blocks,
+                                double2 *__restrict__ block_totals)
 {
-    __shared__ double2 warp_tot[32];
-    __shared__ double2 carry;
-    if (threadIdx.x == 0)
-        carry = make_double2(0.0, 0.0);
-    __syncthreads();
-    for (uint32_t b = 0; b < chunks; b += PX_THREADS)
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= blocks)
+        return;
+    double2 run = make_double2(0.0, 0.0);
+    for (uint32_t c = b * PX_CHUNKS_PER_BLOCK; c < min(chunks, (b + 1) * PX_CHUNKS_PER_BLOCK); c++)
     {
-        const uint32_t i = b + threadIdx.x;
-        const double2 v = i < chunks ? totals[i] : make_double2(0.0, 0.0);
-        const double2 inc = block_scan(v, warp_tot);
-        const double2 c0 = carry;
-        if (i < chunks)
-            totals[i] = add2(c0, make_double2(inc.x - v.x, inc.y - v.y));
-        __syncthreads();
-        if (threadIdx.x == PX_THREADS - 1)
-            carry = add2(c0, inc);
-        __syncthreads();
+        const double2 t = totals[c];
+        totals[c] = run;
+        run = add2(run, t);
     }
+    block_totals[b] = run;
 }
 
-// Pass 3: P[i + 1] for every sample, P[0] = 0.
-__global__ void __launch_bounds__(PX_THREADS) k_prefix_apply(const float *__restrict__ clean, uint64_t n, double c,
+// Pass 3: Q[i + 1] for every sample (0 where i + 1 starts a block), Q[0] = 0.
+__global__ void __launch_bounds__(PX_THREADS) k_prefix_apply(const float *__restrict__ clean, uint64_t n,
+                                                             const double *__restrict__ centres,
                                                              const double2 *__restrict__ offsets,
-                                                             double2 *__restrict__ P)
+                                                             double2 *__restrict__ Q)
 {
     __shared__ double2 warp_tot[32];
     double2 vals[PX_PER_THREAD];
     const uint64_t base = (uint64_t)blockIdx.x * PX_CHUNK + (uint64_t)threadIdx.x * PX_PER_THREAD;
-    const double2 s = chunk_values(clean, n, c, base, vals);
+    const double2 s = chunk_values(clean, n, centres, base, vals);
     const double2 inc = block_scan(s, warp_tot);
     double2 run = add2(offsets[blockIdx.x], make_double2(inc.x - s.x, inc.y - s.y));
 #pragma unroll
     for (int k = 0; k < PX_PER_THREAD; k++)
     {
         run = add2(run, vals[k]);
-        if (base + k < n)
-            P[base + k + 1] = run;
+        const uint64_t i = base + k + 1;
+        if (i <= n)
+            Q[i] = (i & (kPrefixBlock - 1)) == 0 ? make_double2(0.0, 0.0) : run;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0)
-        P[0] = make_double2(0.0, 0.0);
+        Q[0] = make_double2(0.0, 0.0);
 }
 
 // run[i]: samples equal to clean[i] from i on, capped. Round 0 looks ahead up to 16
@@ -153,14 +158,32 @@ __global__ void k_run_double(const float *__restrict__ clean, uint64_t n, uint32
     }
 }
 
-// totals: ceil(n / 8192) double2; P: n + 1 double2; run and run_tmp: n uint16 each.
-cudaError_t launch_prefix(const float *clean, uint64_t n, double c, double2 *totals, double2 *P, uint16_t *run,
-                          uint16_t *run_tmp, cudaStream_t s)
+uint32_t prefix_chunks(uint64_t n) { return (uint32_t)((n + PX_CHUNK - 1) / PX_CHUNK); }
+
+// Chunk totals (centres per prefix block, or null for 0); chunks = prefix_chunks(n).
+cudaError_t launch_prefix_totals(const float *clean, uint64_t n, const double *centres, double2 *totals,
+                                 cudaStream_t s)
 {
-    const uint32_t chunks = (uint32_t)((n + PX_CHUNK - 1) / PX_CHUNK);
-    k_prefix_totals<<<chunks, PX_THREADS, 0, s>>>(clean, n, c, totals);
-    k_prefix_scan_totals<<<1, PX_THREADS, 0, s>>>(totals, chunks);
-    k_prefix_apply<<<chunks, PX_THREADS, 0, s>>>(clean, n, c, totals, P);
+    k_prefix_totals<<<prefix_chunks(n), PX_THREADS, 0, s>>>(clean, n, centres, totals);
+    return cudaGetLastError();
+}
+
+// Q (n + 1 entries) and T (blocks entries) with the given centres; totals: scratch of
+// prefix_chunks(n) entries.
+cudaError_t launch_prefix_sums(const float *clean, uint64_t n, const double *centres, double2 *totals,
+                               double2 *block_totals, double2 *Q, cudaStream_t s)
+{
+    const uint32_t chunks = prefix_chunks(n);
+    const uint32_t blocks = (uint32_t)((n + kPrefixBlock - 1) / kPrefixBlock);
+    k_prefix_totals<<<chunks, PX_THREADS, 0, s>>>(clean, n, centres, totals);
+    k_prefix_blocks<<<(blocks + 255) / 256, 256, 0, s>>>(totals, chunks, blocks, block_totals);
+    k_prefix_apply<<<chunks, PX_THREADS, 0, s>>>(clean, n, centres, totals, Q);
+    return cudaGetLastError();
+}
+
+// run and run_tmp: n uint16 each; the result ends in `run`.
+cudaError_t launch_runs(const float *clean, uint64_t n, uint16_t *run, uint16_t *run_tmp, cudaStream_t s)
+{
     // 16 -> 32 -> ... -> 65536: 12 doublings, an even number, so the result ends in `run`
     k_run_init<<<1184, 256, 0, s>>>(clean, n, run);
     uint16_t *a = run, *b = run_tmp;

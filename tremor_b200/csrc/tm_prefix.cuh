@@ -1,16 +1,30 @@
-// Window statistics of any length from the resident FP64 prefix sums (tm_prefix.cu),
-// with a bound on their error, for contraction tiles that mix template lengths.
+// Window statistics of any length from the resident block-local FP64 prefix sums
+// (tm_prefix.cu), with a bound on their error, for contraction tiles that mix template
+// lengths.
 #pragma once
 
 #include "tm_internal.cuh"
 
 namespace tmb {
 
+constexpr int kPrefixBlockLog = 16;
+constexpr uint64_t kPrefixBlock = 1ull << kPrefixBlockLog; // samples per prefix block (>= any mixed length)
+
 // Bound on the accumulated error of one prefix sum, relative to the sum of magnitudes
-// it covers: a sample passes through at most ~40 additions (8 per thread, 5 + 5 shuffle
-// levels, 5 + 5 + 5 levels for the chunk totals); doubled for margin.
+// it covers: a sample passes through at most ~25 additions (8 per thread, 5 + 5 shuffle
+// levels, the 8 chunk totals of its block) plus its own centring and squaring; 80 units
+// leave a wide margin.
 constexpr double kPrefixGamma = 80.0 * 1.1102230246251565e-16;
 constexpr double kEps64 = 1.1102230246251565e-16;
+
+// The resident prefix sums: Q[i] (block-local, n + 1 entries), T[b] and C[b] (block
+// totals and centres, one more entry than there are blocks).
+struct PrefixView
+{
+    const double2 *Q;
+    const double2 *T;
+    const double *C;
+};
 
 struct WindowStats
 {
@@ -27,36 +41,72 @@ __device__ __forceinline__ float stats_error(const WindowStats &w, int m, float 
     return 1.25f * ((4.0f * (float)m + 2.0f * qs) * w.rel_sd + 2.0f * fabsf(s1q) * w.e_mu * w.iv);
 }
 
-// Statistics of window j (global start index) of length m (independent of the template).
-// Returns 0 when the statistics are trustworthy, 2 when cancellation may have destroyed them (the window must then be
-// re-scored exactly, whatever its distance). Pa = P[j] (a2 = (float)Pa.y), Pb = P[j + m].
-//   prefix errors: gamma * (sum of |terms| up to each end); sum (x - c)^2 up to i is P2[i],
-//   and sum |x - c| up to i <= sqrt(i * P2[i]) <= sqrt((j + m) * P2[j + m]) for i <= j + m
+// Statistics of window [j, j + m) (global sample index, m <= kPrefixBlock) from its
+// block-local prefix sums Qa = Q[j], Qb = Q[j + m]. Returns 0 when they are trustworthy, 2
+// when cancellation may have destroyed them (the window must then be re-scored exactly,
+// whatever its distance).
+//   One block b:  s = Qb - Qa, centre c_b.
+//   Two blocks b, b + 1 (the window ends in b + 1 after n2 samples):
+//     s1 = (T1[b] - Qa1) + (Qb1 + n2 d),  s2 = (T2[b] - Qa2) + (Qb2 + 2 d Qb1 + n2 d^2),
+//     d = c_{b+1} - c_b: the second block's part re-centred on c_b.
+// Error bounds: a prefix value's error is at most gamma x the sum of |terms| it covers;
+// for the squares that is the value itself, for the first sums at most sqrt(count x the
+// squares); the re-centring adds the error of Qb1 times 2|d| and the roundings of its
+// products. The bounds are evaluated in float with margins (bounds, not values).
 //   var relative error  <= e_var / var
 //   std relative error  <= 0.5 e_var / var + rsqrtf's 2^-22 + float rounding
-// The error terms are evaluated in float with margins (they are bounds, not values).
-__device__ __forceinline__ int prefix_stats(double2 Pa, float a2, double2 Pb, uint64_t j, int m, double inv_m,
-                                            float center_f, WindowStats &w)
+__device__ __forceinline__ int window_prefix_stats(const PrefixView &pv, double2 Qa, double2 Qb, uint64_t j, int m,
+                                                   double inv_m, WindowStats &w)
 {
-    const double s1 = Pb.x - Pa.x, s2 = Pb.y - Pa.y;
+    const uint64_t e = j + (uint64_t)m;
+    const uint64_t b1 = j >> kPrefixBlockLog, be = e >> kPrefixBlockLog;
+    const float fg = (float)kPrefixGamma * 1.01f, fe = (float)kEps64 * 1.01f;
+    const float na = (float)(j - (b1 << kPrefixBlockLog)), qa = (float)Qa.y, qb = (float)Qb.y;
+    const double c = pv.C[b1];
+    double s1, s2;
+    float e_s1, e_s2;
+    if (be == b1)
+    {
+        s1 = Qb.x - Qa.x;
+        s2 = Qb.y - Qa.y;
+        const float nb = (float)(e - (b1 << kPrefixBlockLog));
+        e_s2 = fg * (qa + qb);
+        e_s1 = 1.001f * fg * (sqrtf(na * qa) + sqrtf(nb * qb));
+    }
+    else
+    {
+        const double2 t = pv.T[b1];
+        const double d = pv.C[be] - c;
+        const double n2 = (double)(e - (be << kPrefixBlockLog));
+        s1 = (t.x - Qa.x) + (Qb.x + n2 * d);
+        s2 = (t.y - Qa.y) + (Qb.y + (2.0 * d * Qb.x + n2 * d * d));
+        const float tq = (float)t.y, fd = fabsf((float)d), fn2 = (float)n2, q1b = fabsf((float)Qb.x);
+        const float nt = (float)kPrefixBlock;
+        const float eq1b = 1.001f * fg * sqrtf(fn2 * qb);
+        e_s2 = fg * (tq + qa + qb) + 2.0f * fd * eq1b + 8.0f * fe * (2.0f * fd * q1b + fn2 * fd * fd) +
+               4.0f * fe * fd * (q1b + fn2 * fd);
+        e_s1 = 1.001f * fg * (sqrtf(nt * tq) + sqrtf(na * qa)) + eq1b + 4.0f * fe * fn2 * fd +
+               4.0f * fe * (fabsf((float)t.x) + fabsf((float)Qa.x) + q1b + fn2 * fd);
+    }
     const double mu_c = s1 * inv_m;
     const double var = fma(-mu_c, mu_c, s2 * inv_m);
     // var < 1e-22 (std < 1e-11): near the reference's 1e-12 cut, decided by the exact path
     if (!(var > 1e-22) || !(var < 1e36))
         return 2;
-    const float fvar = (float)var, fmu = (float)mu_c, fb2 = (float)Pb.y;
+    const float fvar = (float)var, fmu = (float)mu_c;
     const float fm = (float)m, fim = 1.0f / fm;
-    const float fg = (float)kPrefixGamma * 1.01f, fe = (float)kEps64 * 1.01f;
     const float fs2 = fm * (fvar + fmu * fmu) * 1.0001f;
-    const float e_s2 = fg * (a2 + fb2) + 4.0f * fe * fs2;
-    const float e_s1 = 2.002f * fg * sqrtf((float)(j + (uint64_t)m) * fb2) + 4.0f * fe * fm * fabsf(fmu);
+    e_s2 += 4.0f * fe * fs2;
+    e_s1 += 4.0f * fe * fm * fabsf(fmu);
     const float e_var = (e_s2 + 2.0f * fabsf(fmu) * e_s1 + 8.0f * fe * fs2) * fim * 1.0001f;
-    if (e_var > 1e-4f * fvar)
+    if (!(e_var <= 1e-4f * fvar))
         return 2;
+    const float center_f = (float)c;
     w.iv = rsqrtf(fvar);
     w.mu = fmu + center_f;
     w.rel_sd = 0.5f * e_var * w.iv * w.iv * 1.001f + 6.0e-7f;
-    w.e_mu = e_s1 * fim + 1.2e-7f * (fabsf(w.mu) + fabsf(center_f)) + 4.0f * fe * fabsf(w.mu);
+    w.e_mu = e_s1 * fim + 1.2e-7f * (fabsf(w.mu) + fabsf(center_f)) + 4.0f * fe * fabsf(w.mu) +
+             6.0e-8f * fabsf(center_f);
     return 0;
 }
 

@@ -71,7 +71,6 @@ template <bool MIXED> struct SmemT
     double2 pend[R][MIXED ? kTileLens : 1][CH];  // P[j + len_d] per distinct length d
     float4 st[M2][CH][MIXED ? kTileLens : 1];    // (mean, 1/std or 0 / -1, rel. std error, mean error)
     double2 win_p[M2][TN];                       // mixed: prefix sums at each window start
-    float win_a2[M2][TN];                        //   their sums of squares as float
     uint16_t win_run[M2][TN];                    //   constant-run length at each window start
     uint8_t win_miss[M2][TN];                    //   first sample missing
     int lens[M2][kTileLens];                     //   distinct lengths of the tile
@@ -436,7 +435,6 @@ __global__ void __launch_bounds__(THREADS, 1)
                     const bool in = j < a.W;
                     const double2 pv = in ? a.P[a.w0 + j] : make_double2(0.0, 0.0);
                     sm.win_p[mb][i] = pv;
-                    sm.win_a2[mb][i] = (float)pv.y;
                     sm.win_run[mb][i] = in ? a.run[a.w0 + j] : (uint16_t)65535;
                     sm.win_miss[mb][i] = in ? (uint8_t)(a.raw[a.w0 + j] == kMissing) : (uint8_t)1;
                     if (et < kTileLens)
@@ -483,7 +481,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                 // Phase B: each lane's distances from its length's statistics.
                 const int D = a.tiles[tt].D;
                 constexpr uint32_t RING = Sm::R;
-                const float center_f = (float)a.center;
+                const PrefixView pv{a.P, a.PT, a.PC};
                 auto issue = [&](int cc, uint32_t k) {
                     const uint32_t slot = k % RING;
                     if (et < D)
@@ -520,8 +518,8 @@ __global__ void __launch_bounds__(THREADS, 1)
                         if (j < sm.lwc[mb][d] && !sm.win_miss[mb][ci] && sm.win_run[mb][ci] < len)
                         {
                             WindowStats ws;
-                            if (prefix_stats(sm.win_p[mb][ci], sm.win_a2[mb][ci], sm.pend[pend_it % RING][d][i],
-                                             a.w0 + j, len, sm.linv[mb][d], center_f, ws) == 0)
+                            if (window_prefix_stats(pv, sm.win_p[mb][ci], sm.pend[pend_it % RING][d][i], a.w0 + j,
+                                                    len, sm.linv[mb][d], ws) == 0)
                                 r = make_float4(ws.mu, ws.iv, ws.rel_sd, ws.e_mu);
                             else
                                 r.y = -1.0f; // statistics not trustworthy: exact re-scoring decides
@@ -654,7 +652,7 @@ done:
 // Epilogue: a thread owns one window (its TMEM lane) and walks the tile's columns; the
 // column's template is warp-uniform, so its constants come from shared memory (staged
 // per tile) and mode branches do not diverge. Window statistics of each column's length
-// come from the resident prefix sums (prefix_stats), with the window-end sums of 8
+// come from the resident prefix sums (window_prefix_stats), with the window-end sums of 8
 // columns loaded at once.
 
 struct ColParam // the epilogue's constants of one template column
@@ -896,7 +894,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         const int ew = warp - 4;
         const int half = ew >> 2;
         const int et = threadIdx.x - 128;
-        const float center_f = (float)a.center;
+        const PrefixView pv{a.P, a.PT, a.PC};
         uint32_t tc = 0, staged = 0;
         for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x, tc++)
         {
@@ -1004,7 +1002,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                     else if (ok)
                     {
                         WindowStats ws;
-                        if (prefix_stats(pj, a2, pe[i], a.w0 + j, c.m, c.inv_m, center_f, ws) == 0)
+                        if (window_prefix_stats(pv, pj, pe[i], a.w0 + j, c.m, c.inv_m, ws) == 0)
                         {
                             const float ms = ws.mu - shift;
                             const float cross = (v[i] - ms * c.s1) * ws.iv;
@@ -1112,7 +1110,7 @@ cudaError_t launch_scan_umma(const ScanArgs &a, cudaStream_t s)
     if (a.q_hi == nullptr || a.q_lo == nullptr || a.err == nullptr)
         return cudaErrorInvalidValue;
     const bool mixed = a.tiles != nullptr;
-    if (mixed && (a.P == nullptr || a.run == nullptr || a.raw == nullptr))
+    if (mixed && (a.P == nullptr || a.PT == nullptr || a.PC == nullptr || a.run == nullptr || a.raw == nullptr))
         return cudaErrorInvalidValue;
     const int stride = mixed ? a.k_stride : a.m_pad;
     CUtensorMap mh, ml;
@@ -1180,7 +1178,8 @@ cudaError_t launch_scan_wm(const ScanArgs &a, cudaStream_t s)
     if ((NT != 32 && NT != 64 && NT != 128) || a.q_hi == nullptr || a.q_lo == nullptr || a.err == nullptr ||
         a.t_rows % NT != 0)
         return cudaErrorInvalidValue;
-    if (mixed ? (a.P == nullptr || a.run == nullptr || a.raw == nullptr) : (a.mean == nullptr || a.inv == nullptr))
+    if (mixed ? (a.P == nullptr || a.PT == nullptr || a.PC == nullptr || a.run == nullptr || a.raw == nullptr)
+              : (a.mean == nullptr || a.inv == nullptr))
         return cudaErrorInvalidValue;
     const int stride = mixed ? a.k_stride : a.m_pad;
     CUtensorMap mh, ml;

@@ -197,8 +197,8 @@ __global__ void __launch_bounds__(B_THREADS) k_passb(const uint2 *__restrict__ l
 // k_passb for tiles of several template lengths: statistics from the prefix sums, and
 // windows whose statistics are not trustworthy are always emitted (re-scored exactly).
 __global__ void __launch_bounds__(B_THREADS) k_passb_mixed(const uint2 *__restrict__ list, const float *__restrict__ x,
-                                                           const float *__restrict__ raw, const double2 *__restrict__ P,
-                                                           const uint16_t *__restrict__ run, double center,
+                                                           const float *__restrict__ raw, const PrefixView pv,
+                                                           const uint16_t *__restrict__ run,
                                                            const float *__restrict__ q,
                                                            const TemplParam *__restrict__ tp,
                                                            const uint32_t *__restrict__ tkey, uint64_t w0,
@@ -257,8 +257,7 @@ __global__ void __launch_bounds__(B_THREADS) k_passb_mixed(const uint2 *__restri
         if (j >= p.wcount || raw[w0 + j] == kMissing || run[w0 + j] >= p.m)
             continue;
         WindowStats ws;
-        const double2 pa = P[w0 + j];
-        if (prefix_stats(pa, (float)pa.y, P[w0 + j + p.m], w0 + j, p.m, p.inv_m, (float)center, ws) != 0)
+        if (window_prefix_stats(pv, pv.Q[w0 + j], pv.Q[w0 + j + p.m], w0 + j, p.m, p.inv_m, ws) != 0)
         {
             mask |= 1u << w;
             continue;
@@ -315,12 +314,13 @@ cudaError_t launch_passb(const uint2 *list, uint32_t items, const float *x, cons
 }
 
 cudaError_t launch_passb_mixed(const uint2 *list, uint32_t items, const float *x, const float *raw, const double2 *P,
-                               const uint16_t *run, double center, const float *q, const TemplParam *tp,
+                               const double2 *PT, const double *PC, const uint16_t *run, const float *q,
+                               const TemplParam *tp,
                                const uint32_t *tkey, uint64_t w0, Candidate *cand, uint32_t *cand_count,
                                uint32_t cand_cap, cudaStream_t s)
 {
     if (items > 0)
-        k_passb_mixed<<<items, B_THREADS, 0, s>>>(list, x, raw, P, run, center, q, tp, tkey, w0, cand, cand_count,
+        k_passb_mixed<<<items, B_THREADS, 0, s>>>(list, x, raw, PrefixView{P, PT, PC}, run, q, tp, tkey, w0, cand, cand_count,
                                                   cand_cap);
     return cudaGetLastError();
 }
