@@ -59,6 +59,9 @@ WORKLOADS = {
                      per_step=4096, seed=2029),
     'batching_small': dict(n=1 << 25, q=512, m=(256, 8192), events=250, mode='mixed', k=0, merge=0, corr=0.0,
                            per_step=512, seed=2029),
+    # few long templates (the FFT branch's case): 2^28 samples, 8 chirps of 16384, kNN k=10
+    'long_templates': dict(n=1 << 28, q=8, m=16384, events=200, mode='knn', k=10, merge=8192, corr=0.0,
+                           per_step=8, seed=2031),
     # config 5: 2^29 samples resident with their prefix sums; a Poisson stream of requests
     # (lengths log-uniform in [128, 16384], 50/50 kNN / threshold as in config 4) served
     # with continuous batching; one step = one request

@@ -75,6 +75,11 @@ extern "C" {
 #define TM_TILES_COLS_128 2
 #define TM_TILES_COLS_64 3
 #define TM_TILES_COLS_32 4
+/* Not a tile shape: the FP64 FFT branch (overlap-save correlation of each template with
+ * the record, the same bounded epilogue and exact re-scoring), for few templates of up to
+ * 16384 samples; its cost does not grow with the length. AUTO chooses it when the model
+ * says it is faster than every tile shape. */
+#define TM_TILES_FFT 5
 
 /* request flags */
 #define TM_FLAG_ZNORMALIZED 1u /* templ is already z-normalised (QaWorkerData::ts) */
@@ -109,10 +114,11 @@ int tm_set_kernel(tm_ctx *ctx, int kernel);
 int tm_set_tiles(tm_ctx *ctx, int tiles);
 /* Tiling model of the planner behind TM_TILES_AUTO: kernel milliseconds of 128 templates x
  * 2^25 windows, [group kind: one length, several][shape: rows, columns 128, 64, 32]
- * [K: 256, 1024, 4096, 16384], 32 doubles in that order. tm_autotune measures it on this
- * device (a few seconds, its own synthetic record), stores it in the context and copies
- * it to ms (up to capacity values); returns 32 or an error. tm_set_tile_model installs a
- * saved one (count must be 32). No counterpart in the reference. */
+ * [K: 256, 1024, 4096, 16384], 32 doubles in that order, then the FFT branch's
+ * milliseconds per template per 2^25 samples. tm_autotune measures it on this device (a
+ * few seconds, its own synthetic record), stores it in the context and copies it to ms (up
+ * to capacity values); returns 33 or an error. tm_set_tile_model installs a saved one
+ * (count 33, or 32 to keep the FFT figure). No counterpart in the reference. */
 int tm_autotune(tm_ctx *ctx, double *ms, int capacity);
 int tm_set_tile_model(tm_ctx *ctx, const double *ms, int count);
 /* Restricts searches to windows [first, first + count) (a data partition as in

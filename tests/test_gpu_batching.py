@@ -11,9 +11,9 @@ from tests import oracle_bindings as ob
 
 pytestmark = pytest.mark.gpu
 
-# every tile shape of the mixed-length contraction: 128-template row tiles (k_scan_umma),
-# column tiles of 128 / 64 / 32 templates (k_scan_wm)
-TILES = [tb.TILES_ROWS, tb.TILES_COLS_128, tb.TILES_COLS_64, tb.TILES_COLS_32]
+# every branch of the mixed-length contraction: 128-template row tiles (k_scan_umma),
+# column tiles of 128 / 64 / 32 templates (k_scan_wm), the FP64 FFT branch (tm_fft.cu)
+TILES = [tb.TILES_ROWS, tb.TILES_COLS_128, tb.TILES_COLS_64, tb.TILES_COLS_32, tb.TILES_FFT]
 
 
 def _waveform(n, seed, offset=0.0):
@@ -112,7 +112,7 @@ def test_mixed_lengths_sparse_unbounded(tiles):
     _check(x, reqs, answers)
 
 
-@pytest.mark.parametrize('tiles', [tb.TILES_ROWS, tb.TILES_COLS_64])
+@pytest.mark.parametrize('tiles', [tb.TILES_ROWS, tb.TILES_COLS_64, tb.TILES_FFT])
 def test_constant_stretch_does_not_flood_candidates(tiles):
     """Windows inside a long constant stretch are recognised from the constant-run lengths,
     not handed one by one to the exact re-scoring."""
@@ -205,7 +205,7 @@ def _block_waveform(seed):
     return x
 
 
-@pytest.mark.parametrize('tiles', [tb.TILES_ROWS, tb.TILES_COLS_64])
+@pytest.mark.parametrize('tiles', [tb.TILES_ROWS, tb.TILES_COLS_64, tb.TILES_FFT])
 def test_prefix_blocks_and_loud_event(tiles):
     """Statistics from block-local prefix sums across block boundaries with level steps, and
     after a loud event: answers equal the oracle's."""

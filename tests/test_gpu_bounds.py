@@ -29,7 +29,7 @@ def test_bound_holds_everywhere(kernel, m):
     print(f'kernel={kernel} m={m}: max |d-exact|/e = {ratio:.3g}, median e/(2m) = {np.median(e[ok]) / (2 * m):.3g}')
 
 
-@pytest.mark.parametrize('tiles', [tb.TILES_COLS_128, tb.TILES_COLS_64, tb.TILES_COLS_32])
+@pytest.mark.parametrize('tiles', [tb.TILES_COLS_128, tb.TILES_COLS_64, tb.TILES_COLS_32, tb.TILES_FFT])
 @pytest.mark.parametrize('m', [48, 100, 1000, 4096])
 def test_bound_holds_window_major(tiles, m):
     """The same for the window-major kernel (templates in column tiles, window statistics
@@ -53,8 +53,9 @@ def test_bound_holds_window_major(tiles, m):
     assert np.all(err <= e[ok]), (m, float(np.max(err / e[ok])))
 
 
+@pytest.mark.parametrize('tiles', [tb.TILES_COLS_64, tb.TILES_FFT])
 @pytest.mark.parametrize('m', [100, 4096, 16384])
-def test_bound_holds_across_prefix_blocks(m):
+def test_bound_holds_across_prefix_blocks(m, tiles):
     """The window-major kernel's bound with block-local prefix sums, on a record with level
     steps at the block boundaries and a 1e5-fold loud stretch in block 0: the bound holds,
     and windows two blocks after the loud stretch keep trustworthy statistics (the prefix
@@ -63,7 +64,7 @@ def test_bound_holds_across_prefix_blocks(m):
     x = _block_waveform(70 + m)
     q = _templates(x, m, np.random.default_rng(m + 71), 4)
     with tb.Context(x) as ctx:
-        ctx.set_tiles(tb.TILES_COLS_64)
+        ctx.set_tiles(tiles)
         d, e, exact = ctx.bound_diagnostics(q)
     ok = np.isfinite(d) & (exact < np.float32(3.0e38))
     err = np.abs(d[ok].astype(np.float64) - exact[ok].astype(np.float64))

@@ -12,12 +12,13 @@ pytestmark = pytest.mark.gpu
 def test_autotune_model():
     x = _waveform(1 << 16, 31)
     with tb.Context(x) as ctx:
-        table = ctx.autotune()
+        table, fft_ms = ctx.autotune()
         assert table.shape == (2, 4, 4) and np.all(np.isfinite(table)) and np.all(table > 0)
+        assert np.isfinite(fft_ms) and fft_ms > 0
         # more samples per window cost more on every shape; long templates favour wide tiles
         assert np.all(np.diff(table[:, :, 1:], axis=2) > 0)
         assert np.all(table[:, 0, 3] < table[:, 3, 3])
-        ctx.set_tile_model(table)
+        ctx.set_tile_model(table, fft_ms)
         with pytest.raises(tb.TremorError):
             ctx.set_tile_model(np.zeros(32))
 
@@ -58,3 +59,23 @@ def test_planner_follows_the_model():
     for (p0, d0), (p1, d1) in zip(base, again):
         assert np.array_equal(p0, p1) and np.array_equal(d0.view(np.uint32), d1.view(np.uint32))
     _check(x, reqs, base)
+
+
+def test_planner_picks_fft_for_a_long_template():
+    """One long template: a 128-row tile would be mostly padding, the FFT branch's cost does
+    not grow with the length, so AUTO (default model) takes the FFT branch; the answers
+    equal the oracle's and the row tiles'."""
+    x = _waveform(1 << 17, 36)
+    t = x[40000:40000 + 8192].copy()
+    t[t == tb.MISSING_VALUE] = 0.0
+    reqs = [tb.Request(t, tb.MODE_KNN, k=4, merge_offset=4096)]
+    with tb.Context(x) as ctx:
+        ctx.profile_enable(True)
+        auto = ctx.scan_batch(reqs)
+        assert ctx.profile_read()[0] == 'fft'
+        ctx.set_tiles(tb.TILES_ROWS)
+        rows = ctx.scan_batch(reqs)
+        assert ctx.profile_read()[0] == 'k_scan_umma'
+    assert np.array_equal(auto[0][0], rows[0][0])
+    assert np.array_equal(auto[0][1].view(np.uint32), rows[0][1].view(np.uint32))
+    _check(x, reqs, auto)

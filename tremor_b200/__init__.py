@@ -26,7 +26,7 @@ __all__ = ['Context', 'Batch', 'TremorError', 'Request', 'knn_rows', 'threshold_
 MODE_THRESHOLD = 0
 MODE_KNN = 1
 KERNEL_AUTO, KERNEL_FP32, KERNEL_SPLIT_BF16 = 0, 1, 2
-TILES_AUTO, TILES_ROWS, TILES_COLS_128, TILES_COLS_64, TILES_COLS_32 = 0, 1, 2, 3, 4
+TILES_AUTO, TILES_ROWS, TILES_COLS_128, TILES_COLS_64, TILES_COLS_32, TILES_FFT = 0, 1, 2, 3, 4, 5
 FLAG_ZNORMALIZED = 1
 MISSING_VALUE = np.float32(-100000.0)
 FLT_MAX = float(np.finfo(np.float32).max)
@@ -171,17 +171,20 @@ class Context:
         """Tile shape of mixed-length groups (TILES_*), for batches created afterwards."""
         self._check(self._lib.tm_set_tiles(self._h, tiles))
 
-    def autotune(self) -> np.ndarray:
-        """Measures the tiling model on this device (tm_autotune): milliseconds of 128
-        templates x 2^25 windows, shape [kind (one length, several), tile shape (rows,
-        columns 128 / 64 / 32), K (256, 1024, 4096, 16384)]."""
-        out = np.zeros(32, np.float64)
-        rc = self._lib.tm_autotune(self._h, out.ctypes.data, 32)
+    def autotune(self):
+        """Measures the planner's model on this device (tm_autotune): (table, fft_ms). table:
+        milliseconds of 128 templates x 2^25 windows, shape [kind (one length, several),
+        tile shape (rows, columns 128 / 64 / 32), K (256, 1024, 4096, 16384)]; fft_ms: the FFT
+        branch's milliseconds per template per 2^25 samples."""
+        out = np.zeros(33, np.float64)
+        rc = self._lib.tm_autotune(self._h, out.ctypes.data, 33)
         self._check(min(rc, 0))
-        return out.reshape(2, 4, 4)
+        return out[:32].reshape(2, 4, 4), float(out[32])
 
-    def set_tile_model(self, ms: np.ndarray):
+    def set_tile_model(self, ms: np.ndarray, fft_ms: float = None):
         arr = np.ascontiguousarray(ms, dtype=np.float64).reshape(-1)
+        if fft_ms is not None:
+            arr = np.concatenate([arr, [float(fft_ms)]])
         self._check(self._lib.tm_set_tile_model(self._h, arr.ctypes.data, len(arr)))
 
     def set_window_range(self, first: int, count: int):

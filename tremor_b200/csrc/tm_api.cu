@@ -31,6 +31,9 @@
 #include "tm_host.h"
 #include "tm_internal.cuh"
 #include "tm_prefix.cuh"
+#include "tm_fft.cuh"
+
+#include <cufft.h>
 
 namespace tmb {
 cudaError_t launch_clean(const float *raw, float *clean, uint64_t n, uint64_t n_total, cudaStream_t s);
@@ -235,6 +238,10 @@ struct Lane
     std::vector<std::shared_ptr<PinnedBlock>> pool;
     HostBuf h_split, h_q, h_order, h_slots, h_counters;
     uint32_t cand_cap = 1u << 22, list_cap = 1u << 20;
+    // FFT branch: plans (one template; a batch of pieces) and buffers, created on first use
+    cufftHandle fft_plan1 = 0, fft_planB = 0;
+    bool fft_plans = false;
+    DevBuf fft_y, fft_Y, fft_Z, fft_out;
     // instrumentation
     bool profile = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr, ev4 = nullptr;
@@ -257,8 +264,14 @@ struct Lane
     {
         if (stream)
             cudaStreamSynchronize(stream);
+        if (fft_plans)
+        {
+            cufftDestroy(fft_plan1);
+            cufftDestroy(fft_planB);
+            fft_plans = false;
+        }
         for (DevBuf *b : {&tkey, &bmin_u, &bmin_l, &list, &counters, &cand, &dist, &akeys, &avals, &avals64, &sort_tmp,
-                          &segs})
+                          &segs, &fft_y, &fft_Y, &fft_Z, &fft_out})
             b->release();
         for (HostBuf *b : {&h_split, &h_q, &h_order, &h_slots, &h_counters})
             b->release();
@@ -303,6 +316,12 @@ struct tm_ctx
     // their block totals and centres, constant runs
     DevBuf prefix, ptot, pcen, run;
     bool prefix_ready = false;
+    // FFT branch: spectra of the record's pieces, their shifts and norms (built on first use)
+    DevBuf fft_X, fft_shift, fft_norm;
+    uint32_t fft_P = 0;
+    bool fft_ready = false;
+    std::mutex fft_mu;
+    double fft_ms = 1.4; // model: ms per template per 2^25 samples (B200; tm_autotune measures it)
     std::string err;
     Lane main;                      // the synchronous calls' lane
     std::unique_ptr<Server> server; // serving engine, while started
@@ -427,6 +446,7 @@ struct GroupPlan
     // k_scan_umma or, when col_tile > 0, in column tiles of col_tile rows of k_scan_wm
     bool mixed = false;
     int col_tile = 0;
+    bool fft = false; // FFT branch (tm_fft.cu) instead of a contraction kernel
     int k_stride = 0;            // row stride of the template arrays
     uint32_t w_max = 0;          // windows of the shortest template
     std::vector<tmb::TileInfo> tiles; // per tile: K blocks (row tiles: and distinct lengths)
@@ -661,6 +681,7 @@ void prepare_group_mixed(tm_ctx *ctx, Lane &L, const std::vector<int> &idx_in, c
     const int m_max = reqs[idx[0]].m;
     g.mixed = true;
     g.col_tile = col_tile;
+    g.fft = false;
     g.m = m_max;
     g.T = R;
     g.T_pad = R;
@@ -1171,10 +1192,139 @@ void execute_group(tm_ctx *ctx, Lane &L, GroupPlan &g, tm_result &res)
     });
 }
 
-// Device pipeline for a mixed-length group (tensor-core kernel only).
+#define TM_CUFFT(call)                                                                                            \
+    do                                                                                                            \
+    {                                                                                                             \
+        const cufftResult r_ = (call);                                                                            \
+        if (r_ != CUFFT_SUCCESS)                                                                                  \
+            throw Failure{r_ == CUFFT_ALLOC_FAILED ? TM_ERR_NO_MEMORY : TM_ERR_CUDA,                             \
+                          std::string(#call) + ": cuFFT error " + std::to_string(static_cast<int>(r_))};         \
+    } while (0)
+
+// Spectra of the record's overlapping pieces (tm_fft.cu), their shifts and norms: built
+// once per context (under a lock: serving workers may ask at once).
+void ensure_fft(tm_ctx *ctx, Lane &L)
+{
+    std::lock_guard<std::mutex> lk(ctx->fft_mu);
+    if (ctx->fft_ready)
+        return;
+    ensure_prefix(ctx, L);
+    cudaStream_t s = L.stream;
+    const uint32_t P = tmb::fft_pieces(ctx->n);
+    const uint32_t B = tmb::kFftBatch;
+    const uint64_t Ppad = (static_cast<uint64_t>(P) + B - 1) / B * B; // whole batches; extra pieces stay zero
+    ctx->fft_X.reserve(sizeof(double2) * Ppad * tmb::kFftH);
+    ctx->fft_shift.reserve(sizeof(double) * Ppad);
+    ctx->fft_norm.reserve(sizeof(double) * Ppad);
+    TM_CUDA(cudaMemsetAsync(ctx->fft_X.p, 0, sizeof(double2) * Ppad * tmb::kFftH, s));
+    TM_CUDA(cudaMemsetAsync(ctx->fft_shift.p, 0, sizeof(double) * Ppad, s));
+    TM_CUDA(cudaMemsetAsync(ctx->fft_norm.p, 0, sizeof(double) * Ppad, s));
+    DevBuf pieces;
+    pieces.reserve(sizeof(double) * static_cast<size_t>(B) * tmb::kFftL);
+    cufftHandle plan;
+    int len = tmb::kFftL;
+    TM_CUFFT(cufftPlanMany(&plan, 1, &len, nullptr, 1, tmb::kFftL, nullptr, 1, tmb::kFftH, CUFFT_D2Z,
+                           static_cast<int>(B)));
+    std::unique_ptr<cufftHandle, void (*)(cufftHandle *)> hold(&plan, [](cufftHandle *h) { cufftDestroy(*h); });
+    TM_CUFFT(cufftSetStream(plan, s));
+    for (uint32_t p0 = 0; p0 < P; p0 += B)
+    {
+        const uint32_t cnt = std::min<uint32_t>(B, P - p0);
+        if (cnt < B)
+            TM_CUDA(cudaMemsetAsync(pieces.p, 0, sizeof(double) * static_cast<size_t>(B) * tmb::kFftL, s));
+        TM_CUDA(tmb::launch_fft_gather(ctx->clean.as<float>(), ctx->n, ctx->pcen.as<double>(), p0, cnt,
+                                       pieces.as<double>(), ctx->fft_shift.as<double>(), ctx->fft_norm.as<double>(),
+                                       s));
+        TM_CUFFT(cufftExecD2Z(plan, pieces.as<cufftDoubleReal>(),
+                              reinterpret_cast<cufftDoubleComplex *>(ctx->fft_X.as<double2>() +
+                                                                     static_cast<size_t>(p0) * tmb::kFftH)));
+        count_launch(L, 2);
+    }
+    TM_CUDA(cudaStreamSynchronize(s));
+    pieces.release();
+    ctx->fft_P = P;
+    ctx->fft_ready = true;
+}
+
+// The lane's FFT plans and buffers.
+void ensure_lane_fft(Lane &L)
+{
+    if (L.fft_plans)
+        return;
+    int len = tmb::kFftL;
+    TM_CUFFT(cufftPlan1d(&L.fft_plan1, tmb::kFftL, CUFFT_D2Z, 1));
+    if (cufftPlanMany(&L.fft_planB, 1, &len, nullptr, 1, tmb::kFftH, nullptr, 1, tmb::kFftL, CUFFT_Z2D,
+                      static_cast<int>(tmb::kFftBatch)) != CUFFT_SUCCESS)
+    {
+        cufftDestroy(L.fft_plan1);
+        throw Failure{TM_ERR_CUDA, "cufftPlanMany (inverse FFT batch) failed"};
+    }
+    L.fft_plans = true;
+    TM_CUFFT(cufftSetStream(L.fft_plan1, L.stream));
+    TM_CUFFT(cufftSetStream(L.fft_planB, L.stream));
+    L.fft_y.reserve(sizeof(double) * tmb::kFftL);
+    L.fft_Y.reserve(sizeof(double2) * tmb::kFftH);
+    L.fft_Z.reserve(sizeof(double2) * static_cast<size_t>(tmb::kFftBatch) * tmb::kFftH);
+    L.fft_out.reserve(sizeof(double) * static_cast<size_t>(tmb::kFftBatch) * tmb::kFftL);
+}
+
+// FFT branch of a prepared mixed-length group: each template's correlation with every
+// piece its windows touch, batch by batch, into the same bucket minima and candidate
+// list as the contraction kernels (a: the launch arguments those would get).
+void fft_contract(tm_ctx *ctx, Lane &L, const GroupPlan &g, const tmb::ScanArgs &a)
+{
+    ensure_fft(ctx, L);
+    ensure_lane_fft(L);
+    cudaStream_t s = L.stream;
+    const uint32_t B = tmb::kFftBatch, P = ctx->fft_P;
+    for (int t = 0; t < g.T; t++)
+    {
+        const TemplParam &p = g.htp[t];
+        if (g.index[t] < 0 || p.wcount == 0)
+            continue;
+        TM_CUDA(tmb::launch_fft_template(g.q.as<float>() + p.q_offset, p.m, L.fft_y.as<double>(), s));
+        TM_CUFFT(cufftExecD2Z(L.fft_plan1, L.fft_y.as<cufftDoubleReal>(),
+                              reinterpret_cast<cufftDoubleComplex *>(L.fft_Y.p)));
+        const uint64_t first = a.w0, last = a.w0 + p.wcount - 1;
+        const uint32_t pa = static_cast<uint32_t>(first / tmb::kFftS), pb = static_cast<uint32_t>(last / tmb::kFftS);
+        for (uint32_t p0 = pa / B * B; p0 <= pb && p0 < P; p0 += B)
+        {
+            TM_CUDA(tmb::launch_fft_mul(ctx->fft_X.as<double2>() + static_cast<size_t>(p0) * tmb::kFftH,
+                                        L.fft_Y.as<double2>(), L.fft_Z.as<double2>(), B, s));
+            TM_CUFFT(cufftExecZ2D(L.fft_planB, reinterpret_cast<cufftDoubleComplex *>(L.fft_Z.p),
+                                  L.fft_out.as<cufftDoubleReal>()));
+            tmb::FftEpiArgs f{};
+            f.out = L.fft_out.as<double>();
+            f.p0 = p0;
+            f.count = std::min<uint32_t>(B, P - p0);
+            f.t = static_cast<uint32_t>(t);
+            f.tp = g.tp.as<TemplParam>();
+            f.w0 = a.w0;
+            f.pv = tmb::PrefixView{a.P, a.PT, a.PC};
+            f.run = a.run;
+            f.raw = a.raw;
+            f.shifts = ctx->fft_shift.as<double>();
+            f.norms = ctx->fft_norm.as<double>();
+            f.bmin_u = a.bmin_u;
+            f.bmin_l = a.bmin_l;
+            f.nb = a.nb;
+            f.cand = a.cand;
+            f.cand_count = a.cand_count;
+            f.cand_cap = a.cand_cap;
+            f.dbg_d = a.dbg_d;
+            f.dbg_e = a.dbg_e;
+            f.W = a.W;
+            TM_CUDA(tmb::launch_fft_epilogue(f, s));
+            count_launch(L, 3);
+        }
+        count_launch(L, 2);
+    }
+}
+
+// Device pipeline for a mixed-length group (tensor-core kernels or the FFT branch).
 void execute_group_mixed(tm_ctx *ctx, Lane &L, GroupPlan &g, tm_result &res)
 {
-    if (ctx->kernel == TM_KERNEL_FP32)
+    if (ctx->kernel == TM_KERNEL_FP32 && !g.fft)
         throw Failure{TM_ERR_STATE, "batch of several template lengths was prepared for the tensor-core kernel"};
     ensure_prefix(ctx, L);
     const int T = g.T, nk = g.nk;
@@ -1246,15 +1396,20 @@ void execute_group_mixed(tm_ctx *ctx, Lane &L, GroupPlan &g, tm_result &res)
         if (L.profile)
             TM_CUDA(cudaEventRecord(L.ev0, s));
         a.col_tile = g.col_tile;
-        TM_CUDA(g.col_tile > 0 ? tmb::launch_scan_wm(a, s) : tmb::launch_scan_umma(a, s));
-        count_launch(L);
+        if (g.fft)
+            fft_contract(ctx, L, g, a);
+        else
+        {
+            TM_CUDA(g.col_tile > 0 ? tmb::launch_scan_wm(a, s) : tmb::launch_scan_umma(a, s));
+            count_launch(L);
+        }
         if (L.profile)
         {
             TM_CUDA(cudaEventRecord(L.ev1, s));
             TM_CUDA(cudaEventSynchronize(L.ev1));
             float ms = 0.0f;
             TM_CUDA(cudaEventElapsedTime(&ms, L.ev0, L.ev1));
-            L.kname = g.col_tile > 0 ? "k_scan_wm" : "k_scan_umma";
+            L.kname = g.fft ? "fft" : (g.col_tile > 0 ? "k_scan_wm" : "k_scan_umma");
             L.prof_launches++;
             L.prof_ms += ms;
             L.phase_ms[0] += ms;
@@ -1341,43 +1496,67 @@ double tile_time(const tm_ctx *ctx, bool mixed, int v, double k)
 
 // Tile shape of a group: 0 (row tiles of 128 templates, k_scan_umma) or the column-tile
 // size (k_scan_wm). Each shape's modelled time sums its tiles (consecutive in length
-// order; a tile costs its rows at its longest template's K); the least wins.
-int plan_col_tile(const tm_ctx *ctx, const tm_request *reqs, const std::vector<int> &idx)
+// order; a tile costs its rows at its longest template's K); the least wins. *cost gets
+// the winner's modelled milliseconds per 2^25 windows.
+int plan_col_tile(const tm_ctx *ctx, const tm_request *reqs, const std::vector<int> &idx, double *cost = nullptr)
 {
-    switch (ctx->tiles)
-    {
-    case TM_TILES_ROWS:
-        return 0;
-    case TM_TILES_COLS_128:
-        return 128;
-    case TM_TILES_COLS_64:
-        return 64;
-    case TM_TILES_COLS_32:
-        return 32;
-    default:
-        break;
-    }
     std::vector<int> m(idx.size());
     for (size_t i = 0; i < idx.size(); i++)
         m[i] = reqs[idx[i]].m;
     std::sort(m.begin(), m.end(), std::greater<int>());
     const bool mixed = !m.empty() && m.front() != m.back();
     const int shapes[4] = {128, 128, 64, 32};
-    double best = 0.0;
-    int choice = 0;
+    double costs[4];
     for (int v = 0; v < 4; v++)
     {
         const size_t rows = static_cast<size_t>(shapes[v]);
-        double cost = 0.0;
+        costs[v] = 0.0;
         for (size_t i = 0; i < m.size(); i += rows) // row tiles may close early (65 lengths): ignored
-            cost += static_cast<double>(rows) / 128.0 * tile_time(ctx, mixed, v, static_cast<double>((m[i] + 63) & ~63));
-        if (v == 0 || cost < best)
-        {
-            best = cost;
-            choice = v == 0 ? 0 : shapes[v];
-        }
+            costs[v] += static_cast<double>(rows) / 128.0 *
+                        tile_time(ctx, mixed, v, static_cast<double>((m[i] + 63) & ~63));
     }
-    return choice;
+    int v = 0;
+    switch (ctx->tiles)
+    {
+    case TM_TILES_ROWS:
+        v = 0;
+        break;
+    case TM_TILES_COLS_128:
+        v = 1;
+        break;
+    case TM_TILES_COLS_64:
+        v = 2;
+        break;
+    case TM_TILES_COLS_32:
+        v = 3;
+        break;
+    default:
+        for (int u = 1; u < 4; u++)
+            if (costs[u] < costs[v])
+                v = u;
+    }
+    if (cost)
+        *cost = costs[v];
+    return v == 0 ? 0 : shapes[v];
+}
+
+// FFT branch for a group: forced (TM_TILES_FFT), or under TM_TILES_AUTO with the
+// automatic kernel when its modelled time (templates x the measured per-template time)
+// is below the best tile shape's. Lengths up to 16384 (the FFT pieces' step).
+bool plan_fft(const tm_ctx *ctx, const tm_request *reqs, const std::vector<int> &idx)
+{
+    if (idx.empty() || ctx->kernel == TM_KERNEL_FP32 || !tmb::umma_supported(0, 0, 0))
+        return false;
+    for (int i : idx)
+        if (reqs[i].m > tmb::kFftS)
+            return false;
+    if (ctx->tiles == TM_TILES_FFT)
+        return true;
+    if (ctx->tiles != TM_TILES_AUTO || ctx->kernel != TM_KERNEL_AUTO)
+        return false;
+    double tensor = 0.0;
+    plan_col_tile(ctx, reqs, idx, &tensor);
+    return static_cast<double>(idx.size()) * ctx->fft_ms < tensor;
 }
 
 // Groups of a batch. Lengths with a full 128-template tile (or any length, on the FP32
@@ -1393,7 +1572,12 @@ void create_batch(tm_ctx *ctx, Lane &L, const tm_request *requests, int count, t
             all[i] = i;
         b.groups.resize(count > 0 ? 1 : 0);
         if (count > 0)
-            prepare_group_mixed(ctx, L, all, requests, b.groups[0], b.h2d_bytes, plan_col_tile(ctx, requests, all));
+        {
+            const bool fft = plan_fft(ctx, requests, all);
+            prepare_group_mixed(ctx, L, all, requests, b.groups[0], b.h2d_bytes,
+                                fft ? 0 : plan_col_tile(ctx, requests, all));
+            b.groups[0].fft = fft;
+        }
         return;
     }
     std::map<int, std::vector<int>> by_m;
@@ -1420,10 +1604,24 @@ void create_batch(tm_ctx *ctx, Lane &L, const tm_request *requests, int count, t
     b.groups.resize(single.size() + (rest.empty() ? 0 : 1));
     size_t gi = 0;
     for (auto &kv : single)
-        prepare_group(ctx, L, kv.first, kv.second, requests, b.groups[gi++], b.h2d_bytes,
-                      tensor && kv.first <= 16384 ? plan_col_tile(ctx, requests, kv.second) : 0);
+    {
+        GroupPlan &g = b.groups[gi++];
+        if (tensor && plan_fft(ctx, requests, kv.second))
+        {
+            prepare_group_mixed(ctx, L, kv.second, requests, g, b.h2d_bytes, 0);
+            g.fft = true;
+        }
+        else
+            prepare_group(ctx, L, kv.first, kv.second, requests, g, b.h2d_bytes,
+                          tensor && kv.first <= 16384 ? plan_col_tile(ctx, requests, kv.second) : 0);
+    }
     if (!rest.empty())
-        prepare_group_mixed(ctx, L, rest, requests, b.groups[gi++], b.h2d_bytes, plan_col_tile(ctx, requests, rest));
+    {
+        GroupPlan &g = b.groups[gi++];
+        const bool fft = plan_fft(ctx, requests, rest);
+        prepare_group_mixed(ctx, L, rest, requests, g, b.h2d_bytes, fft ? 0 : plan_col_tile(ctx, requests, rest));
+        g.fft = fft;
+    }
 }
 
 void run_batch(tm_ctx *ctx, Lane &L, tm_batch &b, tm_result &res)
@@ -1683,8 +1881,9 @@ static void stop_server(tm_ctx *ctx)
     sv->stopped = true;
 }
 
-// tm_bound_diagnostics for the window-major kernel: the templates (all of length m) as one
-// group in column tiles of the context's shape, statistics from the prefix sums.
+// tm_bound_diagnostics for the window-major kernel or the FFT branch: the templates (all of
+// length m) as one group in column tiles of the context's shape (or through the FFT
+// branch), statistics from the prefix sums.
 static void bound_diagnostics_wm(tm_ctx *ctx, int m, const std::vector<int> &idx, const std::vector<tm_request> &reqs,
                                  float *d, float *e, float *exact)
 {
@@ -1741,8 +1940,13 @@ static void bound_diagnostics_wm(tm_ctx *ctx, int m, const std::vector<int> &idx
     a.k_stride = g.k_stride;
     a.n = ctx->n;
     a.col_tile = g.col_tile;
-    TM_CUDA(g.col_tile > 0 ? tmb::launch_scan_wm(a, s) : tmb::launch_scan_umma(a, s));
-    count_launch(L);
+    if (ctx->tiles == TM_TILES_FFT)
+        fft_contract(ctx, L, g, a);
+    else
+    {
+        TM_CUDA(g.col_tile > 0 ? tmb::launch_scan_wm(a, s) : tmb::launch_scan_umma(a, s));
+        count_launch(L);
+    }
     TM_CUDA(cudaMemcpyAsync(d, dd.p, pairs * sizeof(float), cudaMemcpyDeviceToHost, s));
     TM_CUDA(cudaMemcpyAsync(e, de.p, pairs * sizeof(float), cudaMemcpyDeviceToHost, s));
     if (exact != nullptr)
@@ -1818,7 +2022,8 @@ int tm_ctx_destroy(tm_ctx *ctx)
         kv.second->inv.release();
         kv.second->flags.release();
     }
-    for (DevBuf *b : {&ctx->prefix, &ctx->ptot, &ctx->pcen, &ctx->run, &ctx->raw, &ctx->clean, &ctx->suf})
+    for (DevBuf *b : {&ctx->prefix, &ctx->ptot, &ctx->pcen, &ctx->run, &ctx->raw, &ctx->clean, &ctx->suf,
+                      &ctx->fft_X, &ctx->fft_shift, &ctx->fft_norm})
         b->release();
     delete ctx;
     return TM_OK;
@@ -1838,7 +2043,7 @@ int tm_set_kernel(tm_ctx *ctx, int kernel)
 
 int tm_set_tiles(tm_ctx *ctx, int tiles)
 {
-    if (ctx == nullptr || tiles < TM_TILES_AUTO || tiles > TM_TILES_COLS_32)
+    if (ctx == nullptr || tiles < TM_TILES_AUTO || tiles > TM_TILES_FFT)
         return TM_ERR_ARGUMENT;
     ctx->tiles = tiles;
     return TM_OK;
@@ -1907,21 +2112,38 @@ int tm_autotune(tm_ctx *ctx, double *ms, int capacity)
                     table[mixed][v][ki] = per * (33554432.0 / windows);
                 }
             }
+        // the FFT branch: 8 of the last templates (its time does not depend on the length)
+        tc->tiles = TM_TILES_FFT;
+        {
+            tm_batch b;
+            create_batch(tc, tc->main, reqs.data(), 8, b);
+            tm_result res;
+            run_batch(tc, tc->main, b, res);
+            tc->main.profile = true;
+            tc->main.prof_ms = 0.0;
+            tc->main.prof_launches = 0;
+            run_batch(tc, tc->main, b, res);
+            tc->main.profile = false;
+        }
+        const double fft_ms = tc->main.prof_ms / 8.0 * (33554432.0 / static_cast<double>(n));
         std::memcpy(ctx->tile_ms, table, sizeof(table));
-        for (int i = 0; i < std::min(capacity, 32); i++)
-            ms[i] = (&table[0][0][0])[i];
+        ctx->fft_ms = fft_ms;
+        for (int i = 0; i < std::min(capacity, 33); i++)
+            ms[i] = i < 32 ? (&table[0][0][0])[i] : fft_ms;
     });
-    return rc == TM_OK ? 32 : rc;
+    return rc == TM_OK ? 33 : rc;
 }
 
 int tm_set_tile_model(tm_ctx *ctx, const double *ms, int count)
 {
-    if (ctx == nullptr || ms == nullptr || count != 32)
+    if (ctx == nullptr || ms == nullptr || (count != 32 && count != 33))
         return TM_ERR_ARGUMENT;
-    for (int i = 0; i < 32; i++)
+    for (int i = 0; i < count; i++)
         if (!(ms[i] > 0.0) || !std::isfinite(ms[i]))
             return TM_ERR_ARGUMENT;
     std::memcpy(ctx->tile_ms, ms, sizeof(ctx->tile_ms));
+    if (count == 33)
+        ctx->fft_ms = ms[32];
     return TM_OK;
 }
 
@@ -2175,7 +2397,8 @@ int tm_bound_diagnostics(tm_ctx *ctx, const float *queries, int count, int m, fl
             reqs[i] = tm_request{queries + static_cast<size_t>(i) * m, m, TM_MODE_THRESHOLD, 1, 0, 1.0f, 0u};
             idx[i] = i;
         }
-        if (ctx->tiles >= TM_TILES_COLS_128 && ctx->kernel != TM_KERNEL_FP32 && tmb::umma_supported(m, count, 0))
+        if (ctx->tiles >= TM_TILES_COLS_128 && ctx->kernel != TM_KERNEL_FP32 && tmb::umma_supported(m, count, 0) &&
+            (ctx->tiles != TM_TILES_FFT || m <= tmb::kFftS))
         {
             bound_diagnostics_wm(ctx, m, idx, reqs, d, e, exact);
             return;
