@@ -6,7 +6,8 @@
 The model is the kernel time in milliseconds of 128 templates against 2^25 windows, per
 group kind (one length, several lengths), tile shape (128-template row tiles; window-major
 column tiles of 128, 64 and 32 templates) and template length K; TILES_AUTO picks the
-shape of least modelled time from it."""
+shape (or the FFT branch, whose per-template time is measured too) of least modelled
+time from it."""
 from __future__ import annotations
 
 import argparse
@@ -26,16 +27,17 @@ def main():
     p.add_argument('--device', type=int, default=0)
     args = p.parse_args()
     with tb.Context(np.random.default_rng(0).normal(size=1 << 16).astype(np.float32), device=args.device) as ctx:
-        table = ctx.autotune()
+        table, fft_ms = ctx.autotune()
     for kind, name in enumerate(('one length', 'several lengths')):
         print(f'{name}: ms per 128 templates x 2^25 windows, K = {KS}')
         for v, shape in enumerate(SHAPES):
             tf = [2.0 * 128 * (1 << 25) * k / (table[kind, v, i] * 1e-3) / 1e12 for i, k in enumerate(KS)]
             print(f'  {shape:26s} ' + '  '.join(f'{table[kind, v, i]:8.1f} ms ({t:5.0f} TF)' for i, t in
                                                   enumerate(tf)))
+    print(f'FFT branch: {fft_ms:.2f} ms per template per 2^25 samples (any length up to 16384)')
     if args.out:
         with open(args.out, 'w') as f:
-            json.dump({'k': KS, 'shapes': SHAPES, 'ms': table.tolist()}, f, indent=1)
+            json.dump({'k': KS, 'shapes': SHAPES, 'ms': table.tolist(), 'fft_ms': fft_ms}, f, indent=1)
 
 
 if __name__ == '__main__':
