@@ -79,3 +79,22 @@ def test_planner_picks_fft_for_a_long_template():
     assert np.array_equal(auto[0][0], rows[0][0])
     assert np.array_equal(auto[0][1].view(np.uint32), rows[0][1].view(np.uint32))
     _check(x, reqs, auto)
+
+
+def test_planner_splits_long_tail_to_fft():
+    """A batch with a few very long templates and many short ones: under the default model
+    the longest go to the FFT branch and the rest to row tiles (two groups, both kernels
+    run); the answers equal the oracle's and those of row tiles alone."""
+    x = _waveform(1 << 17, 37)
+    rng = np.random.default_rng(38)
+    reqs = _requests(x, rng, [16384, 12000] + [int(v) for v in rng.choice([64, 96, 128, 200], size=130)])
+    with tb.Context(x) as ctx:
+        ctx.profile_enable(True)
+        ctx.profile_phases()
+        auto = ctx.scan_batch(reqs)
+        ctx.profile_read()
+        ctx.set_tiles(tb.TILES_ROWS)
+        rows = ctx.scan_batch(reqs)
+    for (p0, d0), (p1, d1) in zip(auto, rows):
+        assert np.array_equal(p0, p1) and np.array_equal(d0.view(np.uint32), d1.view(np.uint32))
+    _check(x, reqs, auto)

@@ -485,6 +485,8 @@ void prepare_group(tm_ctx *ctx, Lane &L, int m, const std::vector<int> &idx, con
                    uint64_t &h2d, int col_tile = 0)
 {
     g.m = m;
+    g.mixed = false; // a reused plan may have held another kind of group
+    g.fft = false;
     g.col_tile = col_tile; // tensor cores: window-major column tiles (k_scan_wm) when > 0
     g.T = static_cast<int>(idx.size());
     g.T_pad = (g.T + 63) & ~63;
@@ -1540,23 +1542,62 @@ int plan_col_tile(const tm_ctx *ctx, const tm_request *reqs, const std::vector<i
     return v == 0 ? 0 : shapes[v];
 }
 
-// FFT branch for a group: forced (TM_TILES_FFT), or under TM_TILES_AUTO with the
-// automatic kernel when its modelled time (templates x the measured per-template time)
-// is below the best tile shape's. Lengths up to 16384 (the FFT pieces' step).
-bool plan_fft(const tm_ctx *ctx, const tm_request *reqs, const std::vector<int> &idx)
+// Modelled milliseconds per 2^25 windows of templates with lengths m[0..n) (sorted,
+// longest first) in the tile shape TM_TILES_AUTO would pick (or the forced one).
+double tensor_cost_sorted(const tm_ctx *ctx, const int *m, size_t n)
 {
-    if (idx.empty() || ctx->kernel == TM_KERNEL_FP32 || !tmb::umma_supported(0, 0, 0))
-        return false;
-    for (int i : idx)
+    if (n == 0)
+        return 0.0;
+    const bool mixed = m[0] != m[n - 1];
+    const int shapes[4] = {128, 128, 64, 32};
+    double best = 0.0;
+    for (int v = 0; v < 4; v++)
+    {
+        if ((ctx->tiles == TM_TILES_ROWS && v != 0) || (ctx->tiles == TM_TILES_COLS_128 && v != 1) ||
+            (ctx->tiles == TM_TILES_COLS_64 && v != 2) || (ctx->tiles == TM_TILES_COLS_32 && v != 3))
+            continue;
+        double c = 0.0;
+        for (size_t i = 0; i < n; i += static_cast<size_t>(shapes[v]))
+            c += shapes[v] / 128.0 * tile_time(ctx, mixed, v, static_cast<double>((m[i] + 63) & ~63));
+        if (best == 0.0 || c < best)
+            best = c;
+    }
+    return best;
+}
+
+// How many of a group's templates (ordered longest first) go to the FFT branch: all of
+// them when it is forced (TM_TILES_FFT); under TM_TILES_AUTO with the automatic kernel,
+// the f minimising f x (the FFT's per-template time) + the tensor cost of the other
+// templates: the longest templates set a tile's K extent, so moving a few of them to the
+// FFT (whose cost does not grow with the length) can shorten every tile they would have
+// padded. Lengths up to 16384 (the FFT pieces' step); otherwise none.
+size_t plan_fft_split(const tm_ctx *ctx, const tm_request *reqs, const std::vector<int> &sorted_idx)
+{
+    const size_t n = sorted_idx.size();
+    if (n == 0 || ctx->kernel == TM_KERNEL_FP32 || !tmb::umma_supported(0, 0, 0))
+        return 0;
+    for (int i : sorted_idx)
         if (reqs[i].m > tmb::kFftS)
-            return false;
+            return 0;
     if (ctx->tiles == TM_TILES_FFT)
-        return true;
+        return n;
     if (ctx->tiles != TM_TILES_AUTO || ctx->kernel != TM_KERNEL_AUTO)
-        return false;
-    double tensor = 0.0;
-    plan_col_tile(ctx, reqs, idx, &tensor);
-    return static_cast<double>(idx.size()) * ctx->fft_ms < tensor;
+        return 0;
+    std::vector<int> m(n);
+    for (size_t i = 0; i < n; i++)
+        m[i] = reqs[sorted_idx[i]].m;
+    size_t best_f = 0;
+    double best = tensor_cost_sorted(ctx, m.data(), n);
+    for (size_t f = 1; f <= n; f++)
+    {
+        const double c = static_cast<double>(f) * ctx->fft_ms + tensor_cost_sorted(ctx, m.data() + f, n - f);
+        if (c < best)
+        {
+            best = c;
+            best_f = f;
+        }
+    }
+    return best_f;
 }
 
 // Groups of a batch. Lengths with a full 128-template tile (or any length, on the FP32
@@ -1565,62 +1606,67 @@ bool plan_fft(const tm_ctx *ctx, const tm_request *reqs, const std::vector<int> 
 void create_batch(tm_ctx *ctx, Lane &L, const tm_request *requests, int count, tm_batch &b, bool serving = false)
 {
     b.count = count;
-    if (serving) // one mixed-length group over the resident prefix sums, whatever the lengths
-    {
-        std::vector<int> all(static_cast<size_t>(count));
-        for (int i = 0; i < count; i++)
-            all[i] = i;
-        b.groups.resize(count > 0 ? 1 : 0);
-        if (count > 0)
-        {
-            const bool fft = plan_fft(ctx, requests, all);
-            prepare_group_mixed(ctx, L, all, requests, b.groups[0], b.h2d_bytes,
-                                fft ? 0 : plan_col_tile(ctx, requests, all));
-            b.groups[0].fft = fft;
-        }
-        return;
-    }
-    std::map<int, std::vector<int>> by_m;
-    for (int i = 0; i < count; i++)
-        by_m[requests[i].m].push_back(i);
     const bool tensor = ctx->kernel != TM_KERNEL_FP32 && tmb::umma_supported(0, 0, 0);
-    std::vector<int> rest;
-    std::vector<std::pair<int, std::vector<int>>> single;
-    for (auto &kv : by_m)
+    // candidate groups (lists of requests); each is then split between the FFT branch and
+    // the contraction (plan_fft_split)
+    std::vector<std::vector<int>> lists;
+    if (serving) // one list over the resident prefix sums, whatever the lengths
     {
-        if (!tensor || kv.second.size() >= 128 || kv.first > 16384)
-            single.emplace_back(kv.first, kv.second);
-        else
-            rest.insert(rest.end(), kv.second.begin(), kv.second.end());
+        lists.emplace_back(static_cast<size_t>(count));
+        for (int i = 0; i < count; i++)
+            lists[0][i] = i;
     }
-    std::map<int, int> rest_lengths;
-    for (int i : rest)
-        rest_lengths[requests[i].m]++;
-    if (rest_lengths.size() == 1)
+    else
     {
-        single.emplace_back(rest_lengths.begin()->first, rest);
-        rest.clear();
-    }
-    b.groups.resize(single.size() + (rest.empty() ? 0 : 1));
-    size_t gi = 0;
-    for (auto &kv : single)
-    {
-        GroupPlan &g = b.groups[gi++];
-        if (tensor && plan_fft(ctx, requests, kv.second))
+        std::map<int, std::vector<int>> by_m;
+        for (int i = 0; i < count; i++)
+            by_m[requests[i].m].push_back(i);
+        std::vector<int> rest;
+        for (auto &kv : by_m)
         {
-            prepare_group_mixed(ctx, L, kv.second, requests, g, b.h2d_bytes, 0);
+            if (!tensor || kv.second.size() >= 128 || kv.first > 16384)
+                lists.push_back(kv.second);
+            else
+                rest.insert(rest.end(), kv.second.begin(), kv.second.end());
+        }
+        if (!rest.empty())
+            lists.push_back(rest);
+    }
+    struct Spec
+    {
+        std::vector<int> idx;
+        int kind; // 0: one length, per-length statistics; 1: prefix statistics, tiles; 2: FFT branch
+    };
+    std::vector<Spec> specs;
+    for (std::vector<int> &list : lists)
+    {
+        std::stable_sort(list.begin(), list.end(), [&](int a, int c) { return requests[a].m > requests[c].m; });
+        const size_t f = tensor ? plan_fft_split(ctx, requests, list) : 0;
+        if (f > 0)
+            specs.push_back(Spec{std::vector<int>(list.begin(), list.begin() + f), 2});
+        if (f < list.size())
+        {
+            std::vector<int> part(list.begin() + f, list.end());
+            const bool one_length = requests[part.front()].m == requests[part.back()].m;
+            specs.push_back(Spec{part, one_length && !serving ? 0 : 1});
+        }
+    }
+    b.groups.resize(specs.size());
+    for (size_t gi = 0; gi < specs.size(); gi++)
+    {
+        GroupPlan &g = b.groups[gi];
+        const std::vector<int> &idx = specs[gi].idx;
+        const int m = requests[idx.front()].m;
+        if (specs[gi].kind == 2)
+        {
+            prepare_group_mixed(ctx, L, idx, requests, g, b.h2d_bytes, 0);
             g.fft = true;
         }
+        else if (specs[gi].kind == 0)
+            prepare_group(ctx, L, m, idx, requests, g, b.h2d_bytes,
+                          tensor && m <= 16384 ? plan_col_tile(ctx, requests, idx) : 0);
         else
-            prepare_group(ctx, L, kv.first, kv.second, requests, g, b.h2d_bytes,
-                          tensor && kv.first <= 16384 ? plan_col_tile(ctx, requests, kv.second) : 0);
-    }
-    if (!rest.empty())
-    {
-        GroupPlan &g = b.groups[gi++];
-        const bool fft = plan_fft(ctx, requests, rest);
-        prepare_group_mixed(ctx, L, rest, requests, g, b.h2d_bytes, fft ? 0 : plan_col_tile(ctx, requests, rest));
-        g.fft = fft;
+            prepare_group_mixed(ctx, L, idx, requests, g, b.h2d_bytes, plan_col_tile(ctx, requests, idx));
     }
 }
 
