@@ -91,7 +91,9 @@ public:
         report(t0, query_count);
     }
 
-    void search_knn(const float *queries, int query_count, int k, const std::string &output)
+    // Writes the kNN CSV; I_out / D_out (optional) receive the answers (query-major, k each).
+    void search_knn(const float *queries, int query_count, int k, const std::string &output,
+                    std::vector<uint64_t> *I_out = nullptr, std::vector<float> *D_out = nullptr)
     {
         std::vector<uint64_t> I(static_cast<size_t>(query_count) * k);
         std::vector<float> D(I.size());
@@ -108,6 +110,10 @@ public:
                              tm_ed_to_cc(D[static_cast<size_t>(q) * k + j], window));
         std::fclose(out);
         report(t0, query_count);
+        if (I_out)
+            *I_out = I;
+        if (D_out)
+            *D_out = D;
     }
 
     double summary_memory_bytes() const { return summary_bytes; }

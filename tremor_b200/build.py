@@ -18,6 +18,7 @@ HERE = Path(__file__).resolve().parent
 CSRC = HERE / 'csrc'
 OUT = HERE / '_build'
 LIB = HERE / 'libtremor_b200.so'
+CLI = HERE / 'tremor_b200_cli'
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 NVCC_FLAGS = ARCH + ['-O3', '-lineinfo', '-std=c++17', '-Xcompiler', '-fPIC', '--expt-relaxed-constexpr',
                      '-Xcompiler', '-Wall']
@@ -64,6 +65,11 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> Path:
     tmp = LIB.with_suffix('.so.tmp')
     _run([nvcc, *ARCH, '-shared', '-o', str(tmp), *objs, '-lcufft'], verbose)
     os.replace(tmp, LIB)
+    # the command-line driver (tremor_main's options and files), next to the library
+    cli_tmp = CLI.with_suffix('.tmp')
+    _run(['g++', '-O2', '-std=c++17', '-Wall', f'-I{HERE.parent / "include"}', str(HERE / 'cli' / 'tremor_b200_main.cpp'),
+          '-o', str(cli_tmp), f'-L{HERE}', '-ltremor_b200', "-Wl,-rpath,$ORIGIN"], verbose)
+    os.replace(cli_tmp, CLI)
     return LIB
 
 
