@@ -445,14 +445,10 @@ def run_serving(args, w):
     queue = np.array([c.start_ms - c.submit_ms for c in comps])
     service = np.array([c.done_ms - c.start_ms for c in comps])
     answers = sum(len(c.answers[0]) for c in comps)
-    t = torch.tensor([pairs, flops, span_ms], dtype=torch.float64, device=f'cuda:{local}')
-    if dist:
-        tot = t.clone()
-        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
-        mx = t.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        t = torch.stack([tot[0], tot[1], mx[2]])
-    pairs_all, flops_all, span_ms = t.tolist()
+    from tremor_b200.replicas import combine
+    dev = f'cuda:{local}'
+    pairs_all, span_ms = combine(pairs, span_ms, dist, dev)  # all work, the slowest rank's span
+    flops_all, _ = combine(flops, span_ms, dist, dev)
     value = pairs_all / (span_ms / 1e3) / 1e9
     if rank == 0:
         bf16_peak, _, peak_kind = peaks()
@@ -577,11 +573,11 @@ def run_ours(args, w):
     log('[bench] e2e host phases per step (create, run, close) ms: ' +
         ', '.join(f'{1000 * p / args.steps:.1f}' for p in phases))
 
-    t = torch.tensor([ms, e_ms, kms / max(launches, 1)], dtype=torch.float64, device=f'cuda:{local}')
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms, e_ms, k_avg_ms = t.tolist()
-    total_pairs = pairs * world
+    from tremor_b200.replicas import combine
+    dev = f'cuda:{local}'
+    total_pairs, ms = combine(pairs, ms, dist, dev)  # every replica's pairs, the slowest rank's time
+    _, e_ms = combine(0.0, e_ms, dist, dev)
+    _, k_avg_ms = combine(0.0, kms / max(launches, 1), dist, dev)
     value = total_pairs / (ms / 1e3) / 1e9
     e2e_value = total_pairs / (e_ms / 1e3) / 1e9
 

@@ -1,0 +1,85 @@
+"""Several ranks (tremor_b200.replicas) on CPU with the gloo backend, world size 2: the
+report's combination (total work, slowest rank), the contiguous window partitions, and the
+threshold shards of a partitioned search (each rank's oracle answers over its partition,
+gathered in rank order) against the whole record's answers."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+from tremor_b200 import replicas
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(('127.0.0.1', 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, x, q, m, corr, merge, out):
+    import datetime
+    import torch.distributed as dist
+    from tests import oracle_bindings as ob
+    os.environ['MASTER_ADDR'] = '127.0.0.1'
+    os.environ['MASTER_PORT'] = str(port)
+    dist.init_process_group('gloo', rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        total, slowest = replicas.combine(1000.0 + rank, 10.0 * (rank + 1), dist)
+        W = len(x) - m + 1
+        first, count = replicas.partition(W, world, rank)
+        part = x[first:first + count + m - 1]                 # the partition and its m - 1 halo
+        _, pos, dist_ed = ob.scan_threshold(part, q[None, :], m, corr, merge)
+        shard = [(int(p) + first, float(d)) for p, d in zip(pos, dist_ed)]
+        shards = replicas.gather_shards(shard, dist)
+        out.put((rank, total, slowest, (first, count), shards))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize('merge', [0, 25])
+def test_two_ranks_partitioned_threshold_search(merge):
+    rng = np.random.default_rng(5 + merge)
+    n, m, corr = 6000, 64, 0.5
+    x = rng.normal(size=n).astype(np.float32)
+    q = x[1000:1000 + m].copy()
+    x[2990:2990 + m] = q          # a match across the partition boundary region
+    ctx = mp.get_context('spawn')
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, x, q, m, corr, merge, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    results = sorted(out.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    (r0, total0, slow0, part0, shards0), (r1, total1, slow1, part1, shards1) = results
+    assert total0 == total1 == 2001.0 and slow0 == slow1 == 20.0
+    W = n - m + 1
+    assert part0 == (0, (W + 1) // 2) and part1 == ((W + 1) // 2, W // 2)
+    assert shards0 == shards1 and len(shards0) == 2
+    from tests import oracle_bindings as ob
+    gathered = [h for shard in shards0 for h in shard]
+    expected = []
+    for first, count in (part0, part1):          # the reference merges within each rank's shard
+        _, pos, d = ob.scan_threshold(x[first:first + count + m - 1], q[None, :], m, corr, merge)
+        expected += [(int(p) + first, float(v)) for p, v in zip(pos, d)]
+    assert gathered == expected
+    if merge == 0:                                # no merge: exactly the whole record's hits
+        _, pos, d = ob.scan_threshold(x, q[None, :], m, corr, 0)
+        assert gathered == [(int(p), float(v)) for p, v in zip(pos, d)]
+    assert any(p == 2990 for p, _ in gathered)
+
+
+def test_partition_tiles_the_windows():
+    for windows in (0, 1, 7, 1000, 12345):
+        for world in (1, 2, 3, 8):
+            parts = [replicas.partition(windows, world, r) for r in range(world)]
+            assert parts[0][0] == 0 and sum(c for _, c in parts) == windows
+            for (f0, c0), (f1, _) in zip(parts, parts[1:]):
+                assert f0 + c0 == f1
+            assert max(c for _, c in parts) - min(c for _, c in parts) <= 1
+    with pytest.raises(ValueError):
+        replicas.partition(10, 2, 2)
