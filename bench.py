@@ -51,7 +51,7 @@ WORKLOADS = {
     'precision_small': dict(n=1 << 25, q=64, m=4096, events=250, mode='knn', k=100, merge=0, corr=0.0,
                             per_step=64, seed=2028),
     'threshold': dict(n=1 << 26, q=256, m=2048, events=500, mode='threshold', k=1, merge=0, corr=0.8,
-                      per_step=64, seed=2027),
+                      per_step=256, seed=2027),
     # config 4: lengths log-uniform in [256, 8192] (multiples of 16), random centre
     # frequencies, 50/50 kNN (k in {1, 10, 100}, merge m/2) and threshold (0.6-0.9); the
     # whole batch is one step (one mixed-length launch)
