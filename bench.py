@@ -647,7 +647,7 @@ def main():
     p.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline leg')
     p.add_argument('--rate', type=float, default=0.0, help='serving: Poisson arrival rate (req/s)')
     p.add_argument('--requests', type=int, default=0, help='serving: requests in the timed stream')
-    p.add_argument('--workers', type=int, default=2, help='serving: batches in flight at once')
+    p.add_argument('--workers', type=int, default=1, help='serving: batches in flight at once')
     p.add_argument('--max-batch', type=int, default=256, help='serving: requests per batch at most')
     args = p.parse_args()
     if args.warmup < 3:

@@ -233,7 +233,9 @@ int tm_last_candidates(const tm_ctx *ctx, uint64_t *count);
  * calls stay usable. */
 typedef struct tm_serve_config
 {
-    int workers;            /* batches in flight at once (1-8; default 2) */
+    int workers;            /* batches in flight at once (1-8; default 1: on one GPU, concurrent
+                             * batches mostly compete for the SMs and split the queue into
+                             * smaller, less efficient batches) */
     int max_batch;          /* requests per batch at most (default 256) */
     uint64_t memory_budget; /* device bytes for requests in flight; 0: a quarter of the free memory */
 } tm_serve_config;

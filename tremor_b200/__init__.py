@@ -232,7 +232,7 @@ class Context:
         self._check(self._lib.tm_scan_batch(self._h, arr, len(requests), ctypes.byref(res)))
         return self._take(res, len(requests))
 
-    def serve(self, workers: int = 2, max_batch: int = 256, memory_budget: int = 0) -> 'Server':
+    def serve(self, workers: int = 1, max_batch: int = 256, memory_budget: int = 0) -> 'Server':
         """Starts continuous batching over this context's waveform (tm_serve_start)."""
         return Server(self, workers, max_batch, memory_budget)
 
@@ -357,7 +357,7 @@ class Server:
     """Continuous batching over a context's resident waveform (tm_serve_*): submit() from
     any thread, poll() from one."""
 
-    def __init__(self, ctx: Context, workers: int = 2, max_batch: int = 256, memory_budget: int = 0):
+    def __init__(self, ctx: Context, workers: int = 1, max_batch: int = 256, memory_budget: int = 0):
         self.ctx = ctx
         cfg = _ServeConfig(workers, max_batch, memory_budget)
         ctx._check(ctx._lib.tm_serve_start(ctx._h, ctypes.byref(cfg)))

@@ -239,7 +239,7 @@ int tm_serve_start(tm_ctx *ctx, const tm_serve_config *config)
         return TM_ERR_ARGUMENT;
     if (ctx->server && !ctx->server->stopped)
         return TM_ERR_STATE;
-    tm_serve_config cfg{2, 256, 0};
+    tm_serve_config cfg{1, 256, 0};
     if (config)
         cfg = *config;
     if (cfg.workers < 1 || cfg.workers > 8 || cfg.max_batch < 1)
