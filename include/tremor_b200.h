@@ -197,6 +197,10 @@ int tm_profile_enable(tm_ctx *ctx, int enable);
  * kernel launches of this library since the last reset. Resets the counters. */
 int tm_profile_read(tm_ctx *ctx, char *name, size_t name_capacity, int64_t *launches, double *milliseconds,
                     double *flops, int64_t *all_launches);
+/* Measured FP32 FMA rate of a device in TFLOP/s (2 flops per FMA; register-resident FMA
+ * chains on every SM, best of 4 timed launches): the roofline denominator of the FP32
+ * contraction kernel. No counterpart in the reference. */
+int tm_fp32_peak(int device, double *tflops);
 /* Milliseconds spent, since the last call and while profiling was enabled, in each of the
  * TM_PHASES phases of a search: [0] contraction kernel, [1] kNN bound, bucket list and
  * FP32 re-pass, [2] exact re-scoring, [3] answer filter and sort on the device, [4] copy
@@ -212,6 +216,17 @@ int tm_profile_phases(tm_ctx *ctx, double *milliseconds, int capacity);
  * context's window range. The bound holds when |d - exact| <= e (windows that are not
  * searched stay NaN in d and e). Small cases only: windows x count <= 2^31. */
 int tm_bound_diagnostics(tm_ctx *ctx, const float *queries, int count, int m, float *d, float *e, float *exact);
+/* One template, as the planner's worker seam calls the scan (Tremor.cpp:1946,
+ * refine_in_position_order, one template per call). tm_scan_knn: the canonical kNN
+ * answers of the context's windows (k entries in I/D, unfilled slots (0, FLT_MAX));
+ * answers whose distance exceeds bound_in (the caller's current k-th distance; FLT_MAX
+ * when it has none) are returned as (0, FLT_MAX), as the caller's queue would reject them
+ * (offer_knn_window, Tremor.cpp:1352-1362). tm_scan_threshold: the merged threshold hits
+ * (one request in *out). */
+int tm_scan_knn(tm_ctx *ctx, const float *templ, int m, int k, int merge_offset, float bound_in, uint64_t *I,
+                float *D);
+int tm_scan_threshold(tm_ctx *ctx, const float *templ, int m, float correlation, int merge_offset,
+                      tm_result **out);
 /* Device-to-host bytes the searches of this context copied since the last call (resets). */
 int tm_d2h_bytes(tm_ctx *ctx, uint64_t *bytes);
 /* The context's CUDA stream (a cudaStream_t), for callers that order or time work on it. */

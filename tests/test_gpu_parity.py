@@ -173,3 +173,22 @@ def test_prepared_batch_reruns_and_kernel_switch():
             for (p0, d0), (p1, d1) in zip(first, again):
                 assert np.array_equal(p0, p1) and np.array_equal(d0.view(np.uint32), d1.view(np.uint32))
         b.close()
+
+
+def test_single_template_entry_points():
+    """tm_scan_knn / tm_scan_threshold (one template, the worker seam's call): the same
+    answers as the batch call; a caller's bound drops the answers above it."""
+    x = _waveform(1 << 16, 91)
+    m = 128
+    q = _templates(x, m, np.random.default_rng(92), 2)
+    with tb.Context(x) as ctx:
+        (bp, bd), = ctx.scan_batch([tb.Request(q[0], tb.MODE_KNN, k=6, merge_offset=64)])
+        p, d = ctx.scan_knn(q[0], 6, merge_offset=64)
+        assert np.array_equal(p, bp) and np.array_equal(d.view(np.uint32), bd.view(np.uint32))
+        p2, d2 = ctx.scan_knn(q[0], 6, merge_offset=64, bound=float(bd[2]))
+        keep = bd <= bd[2]
+        assert np.array_equal(p2, np.where(keep, bp, 0))
+        assert np.array_equal(d2, np.where(keep, bd, np.finfo(np.float32).max))
+        (tp_, td_), = ctx.scan_batch([tb.Request(q[1], tb.MODE_THRESHOLD, correlation=0.6, merge_offset=10)])
+        p3, d3 = ctx.scan_threshold(q[1], 0.6, merge_offset=10)
+        assert np.array_equal(p3, tp_) and np.array_equal(d3.view(np.uint32), td_.view(np.uint32))

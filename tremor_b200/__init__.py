@@ -93,6 +93,9 @@ def load_library():
                                 ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                 ctypes.POINTER(ctypes.c_int64)]),
         'tm_profile_phases': (i, [_vp, _vp, i]),
+        'tm_scan_knn': (i, [_vp, _vp, i, i, i, f, _vp, _vp]),
+        'tm_fp32_peak': (i, [i, ctypes.POINTER(ctypes.c_double)]),
+        'tm_scan_threshold': (i, [_vp, _vp, i, f, i, pp]),
         'tm_serve_start': (i, [_vp, _vp]),
         'tm_submit': (i, [_vp, _vp, ctypes.POINTER(u64)]),
         'tm_poll': (i, [_vp, _vp, i, i, ctypes.POINTER(i)]),
@@ -235,6 +238,24 @@ class Context:
     def serve(self, workers: int = 1, max_batch: int = 256, memory_budget: int = 0) -> 'Server':
         """Starts continuous batching over this context's waveform (tm_serve_start)."""
         return Server(self, workers, max_batch, memory_budget)
+
+    def scan_knn(self, template: np.ndarray, k: int, merge_offset: int = 0, bound: float = float('inf')):
+        """(positions, distances) of one template's k answers (tm_scan_knn); answers above
+        `bound` come back as (0, FLT_MAX)."""
+        q = np.ascontiguousarray(template, dtype=np.float32)
+        pos = np.zeros(k, np.uint64)
+        dist = np.zeros(k, np.float32)
+        b = float(np.finfo(np.float32).max) if not np.isfinite(bound) else float(bound)
+        self._check(self._lib.tm_scan_knn(self._h, _ptr(q), len(q), k, merge_offset, b, _ptr(pos), _ptr(dist)))
+        return pos, dist
+
+    def scan_threshold(self, template: np.ndarray, correlation: float, merge_offset: int = 0):
+        """(positions, distances) of one template's threshold hits (tm_scan_threshold)."""
+        q = np.ascontiguousarray(template, dtype=np.float32)
+        res = _vp()
+        self._check(self._lib.tm_scan_threshold(self._h, _ptr(q), len(q), float(correlation), merge_offset,
+                                                ctypes.byref(res)))
+        return self._take(res, 1)[0]
 
     def batch(self, requests: Sequence[Request]) -> 'Batch':
         """A prepared batch whose templates stay resident on the device (tm_batch)."""
@@ -398,6 +419,16 @@ class Server:
 
     def __exit__(self, *exc):
         self.stop()
+
+
+def fp32_peak(device: int = 0) -> float:
+    """Measured FP32 FMA rate of the device in TFLOP/s (tm_fp32_peak)."""
+    lib = load_library()
+    v = ctypes.c_double(0.0)
+    rc = lib.tm_fp32_peak(device, ctypes.byref(v))
+    if rc != 0:
+        raise TremorError(rc, 'tm_fp32_peak')
+    return v.value
 
 
 def ed_to_cc(ed: float, m: int) -> float:

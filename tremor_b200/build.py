@@ -23,7 +23,8 @@ ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 NVCC_FLAGS = ARCH + ['-O3', '-lineinfo', '-std=c++17', '-Xcompiler', '-fPIC', '--expt-relaxed-constexpr',
                      '-Xcompiler', '-Wall']
 CU_SOURCES = ['tm_api.cu', 'tm_stats.cu', 'tm_scan_fp32.cu', 'tm_select.cu', 'tm_scan_umma.cu', 'tm_noalloc.cu',
-              'tm_prefix.cu', 'tm_answers.cu', 'tm_fft.cu', 'tm_groups.cu', 'tm_search.cu', 'tm_serve.cu']
+              'tm_prefix.cu', 'tm_answers.cu', 'tm_fft.cu', 'tm_groups.cu', 'tm_search.cu', 'tm_serve.cu',
+              'tm_probe.cu']
 CPP_SOURCES = ['tm_host.cpp']
 
 

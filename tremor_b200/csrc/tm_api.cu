@@ -419,6 +419,28 @@ int tm_search_knn(tm_ctx *ctx, const float *queries, int count, int m, int k, in
     return TM_OK;
 }
 
+int tm_scan_knn(tm_ctx *ctx, const float *templ, int m, int k, int merge_offset, float bound_in, uint64_t *I,
+                float *D)
+{
+    if (ctx == nullptr || templ == nullptr || I == nullptr || D == nullptr || k < 1 || std::isnan(bound_in))
+        return TM_ERR_ARGUMENT;
+    const int rc = tm_search_knn(ctx, templ, 1, m, k, merge_offset, I, D);
+    if (rc != TM_OK)
+        return rc;
+    for (int j = 0; j < k; j++)
+        if (!(D[j] <= bound_in))
+        {
+            I[j] = 0;
+            D[j] = FLT_MAX;
+        }
+    return TM_OK;
+}
+
+int tm_scan_threshold(tm_ctx *ctx, const float *templ, int m, float correlation, int merge_offset, tm_result **out)
+{
+    return tm_search_threshold(ctx, templ, 1, m, correlation, merge_offset, out);
+}
+
 int tm_search_threshold(tm_ctx *ctx, const float *queries, int count, int m, float correlation, int merge_offset,
                         tm_result **out)
 {
