@@ -222,3 +222,20 @@ def test_prefix_blocks_and_loud_event(tiles):
         ctx.set_tiles(tiles)
         answers = ctx.scan_batch(reqs)
     _check(x, reqs, answers)
+
+
+@pytest.mark.parametrize('tiles', [tb.TILES_ROWS, tb.TILES_COLS_128])
+def test_many_distinct_lengths_per_tile(tiles):
+    """Row tiles hold 128 templates whatever their lengths: 160 templates, the first 130 of
+    distinct lengths (every epilogue warp of the first tile sees 32 lengths, its table's
+    maximum), the rest sharing lengths across warp boundaries; answers equal the oracle's."""
+    x = _waveform(1 << 15, 77)
+    x = x[:20000].copy()
+    rng = np.random.default_rng(78)
+    lengths = [16 + 4 * i for i in range(130)] + [int(v) for v in rng.choice([40, 41, 200, 517], size=30)]
+    rng.shuffle(lengths)
+    reqs = _requests(x, rng, lengths)
+    with tb.Context(x) as ctx:
+        ctx.set_tiles(tiles)
+        answers = ctx.scan_batch(reqs)
+    _check(x, reqs, answers)

@@ -389,7 +389,7 @@ struct GroupPlan
     bool fft = false; // FFT branch (tm_fft.cu) instead of a contraction kernel
     int k_stride = 0;            // row stride of the template arrays
     uint32_t w_max = 0;          // windows of the shortest template
-    std::vector<tmb::TileInfo> tiles; // per tile: K blocks (row tiles: and distinct lengths)
+    std::vector<tmb::TileInfo> tiles; // per tile: K blocks
     DevBuf d_tiles;
     void release()
     {

@@ -35,7 +35,7 @@ struct ScanArgs
     const double2 *PT;     //   their block totals
     const double *PC;      //   and block centres
     const uint16_t *run;   // constant-run lengths
-    const TileInfo *tiles; // per 128-row tile: K blocks and distinct lengths
+    const TileInfo *tiles; // mixed lengths: per tile, its K blocks
     int k_stride;          // row stride of the template arrays
     uint64_t n;            // samples of the waveform (P has n + 1 entries)
     int col_tile;          // window-major kernel: templates per column tile (32, 64, 128); 0: row tiles

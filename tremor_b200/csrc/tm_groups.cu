@@ -132,10 +132,9 @@ void prepare_group(tm_ctx *ctx, Lane &L, int m, const std::vector<int> &idx, con
            sizeof(TemplParam) * T_pad;
 }
 
-// Host preparation of a mixed-length group: templates sorted by length (longest first).
-// Row tiles (col_tile 0, k_scan_umma): 128 rows, a tile closing early when a new length
-// would be its 65th distinct one. Column tiles (k_scan_wm): col_tile rows, any lengths.
-// Padding rows are inert; a tile's K extent is its longest template (shorter rows are
+// Host preparation of a mixed-length group: templates sorted by length (longest first),
+// in tiles of 128 rows (col_tile 0, k_scan_umma) or col_tile rows (k_scan_wm), any
+// lengths. Padding rows are inert; a tile's K extent is its longest template (shorter rows are
 // zero-padded, which leaves their dot products unchanged). Rows are the template slots of
 // the group: g.index[row] is the request (-1 for padding rows).
 void prepare_group_mixed(tm_ctx *ctx, Lane &L, const std::vector<int> &idx_in, const tm_request *reqs, GroupPlan &g,
@@ -147,39 +146,17 @@ void prepare_group_mixed(tm_ctx *ctx, Lane &L, const std::vector<int> &idx_in, c
     // rows: request per row (-1 = padding)
     std::vector<int> rows;
     std::vector<tmb::TileInfo> tiles;
-    std::vector<int> didx_of_row;
+    std::vector<int> tile_len; // the longest template of each tile
     for (size_t i = 0; i < idx.size();)
     {
-        tmb::TileInfo ti{};
         const size_t start = rows.size();
         const int longest = reqs[idx[i]].m;
         while (i < idx.size() && rows.size() - start < tile_rows)
-        {
-            const int m = reqs[idx[i]].m;
-            int d = 0;
-            if (col_tile == 0)
-            {
-                while (d < ti.D && ti.len[d] != m)
-                    d++;
-                if (d == ti.D)
-                {
-                    if (ti.D == tmb::kTileLens)
-                        break;
-                    ti.len[ti.D++] = m;
-                }
-            }
-            rows.push_back(idx[i]);
-            didx_of_row.push_back(d);
-            i++;
-        }
-        ti.len[0] = longest;
-        ti.kb = (longest + 63) / 64;
+            rows.push_back(idx[i++]);
         while (rows.size() - start < tile_rows)
-        {
             rows.push_back(-1);
-            didx_of_row.push_back(0);
-        }
-        tiles.push_back(ti);
+        tiles.push_back(tmb::TileInfo{(longest + 63) / 64});
+        tile_len.push_back(longest);
     }
     const int R = static_cast<int>(rows.size()); // multiple of the tile rows
     const int m_max = reqs[idx[0]].m;
@@ -225,13 +202,11 @@ void prepare_group_mixed(tm_ctx *ctx, Lane &L, const std::vector<int> &idx_in, c
     for (int t = 0; t < R; t++)
     {
         TemplParam &p = g.htp[t];
-        const tmb::TileInfo &ti = tiles[static_cast<size_t>(t) / tile_rows];
-        p.didx = didx_of_row[t];
         if (rows[t] < 0)
         {
             p.mode = TM_MODE_THRESHOLD;
             p.thr_ed = -FLT_MAX;
-            p.m = ti.len[0];
+            p.m = tile_len[static_cast<size_t>(t) / tile_rows];
             p.inv_m = 1.0 / p.m;
             p.wcount = 0;
             continue;
@@ -269,12 +244,6 @@ void prepare_group_mixed(tm_ctx *ctx, Lane &L, const std::vector<int> &idx_in, c
         else
             p.thr_ed = g.thr[t] = tm_host::cc_to_ed(r->correlation, m);
     }
-    for (tmb::TileInfo &ti : tiles)
-        for (int d = 0; d < ti.D; d++)
-        {
-            ti.wc[d] = wcount_of(ti.len[d]);
-            ti.inv_m[d] = 1.0 / static_cast<double>(ti.len[d]);
-        }
     g.tiles = tiles;
     cudaStream_t s = L.stream;
     g.q.reserve(sizeof(float) * elems);

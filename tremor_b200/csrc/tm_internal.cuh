@@ -36,18 +36,12 @@ struct TemplParam
     int64_t order_offset; // int offset of its block order
     uint32_t wcount;  // windows of this template in the searched range (mixed-length tiles)
     float qs;         // |q| sqrt(m)
-    int didx;         // mixed-length tiles: index of m in its tile's distinct lengths
 };
 
-// A 128-row tile of a mixed-length group: its distinct template lengths (at most 64).
-constexpr int kTileLens = 64;
+// A tile of a mixed-length group (128 template rows, or a column tile): its K extent.
 struct TileInfo
 {
-    int kb;                   // K blocks of 64 samples (longest template of the tile)
-    int D;                    // distinct lengths
-    int len[kTileLens];
-    uint32_t wc[kTileLens];   // windows of each length in the searched range
-    double inv_m[kTileLens];  // 1 / length
+    int kb; // K blocks of 64 samples (the longest template of the tile)
 };
 
 // A candidate window for exact re-scoring: template slot and window index relative

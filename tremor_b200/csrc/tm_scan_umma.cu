@@ -48,39 +48,35 @@ constexpr int B_BYTES = STRIP_CHUNKS * 128;   // 5 KiB per half
 constexpr int THREADS = 384;  // 4 role warps + 8 epilogue warps
 constexpr int BUILDERS = 64;
 constexpr int EPI = 256;      // epilogue threads
-constexpr int CH = 16;        // mixed tiles: windows per statistics chunk
-constexpr int NCH = TN / CH;
 constexpr uint32_t TMEM_COLS = 2 * TN;
 constexpr long long TIMEOUT_CYCLES = 4000000000ll; // ~2 s at 2 GHz
 
-// Shared memory. Mixed-length tiles trade one operand stage for the statistics pipeline:
-// window-end prefix sums of each distinct length (a 3-slot ring of 16-window chunks,
-// filled by bulk copies two chunks ahead) and the per-(window, length) statistics
-// (double-buffered by chunk).
+// Shared memory. Single-length tiles stage the per-window statistics of their length
+// (double-buffered by tile). Mixed-length tiles keep, per epilogue warp, the distinct
+// lengths of its 32 template rows and the statistics of its current group of windows for
+// each of those lengths; no other role reads them.
 template <bool MIXED> struct SmemT
 {
-    static constexpr int S = MIXED ? 3 : 4;    // operand stages
-    static constexpr int R = MIXED ? 3 : 1;    // ring slots of window-end prefix sums
-    static constexpr int W2 = MIXED ? 1 : 2;   // single-length window statistics buffers
-    static constexpr int M2 = MIXED ? 2 : 1;   // mixed-length per-tile buffers
-    static constexpr uint32_t STAGE = MIXED ? 64 : 256; // staged candidates per epilogue warp
+    static constexpr int S = 4;                 // operand stages
+    static constexpr int W2 = MIXED ? 1 : 2;    // single-length window statistics buffers
+    static constexpr int WL = MIXED ? 8 : 1;    // mixed: per-warp tables
+    static constexpr uint32_t STAGE = MIXED ? 128 : 256; // staged candidates per epilogue warp
     uint8_t a_hi[S][A_BYTES]; // 1024-byte aligned (swizzle atoms)
     uint8_t a_lo[S][A_BYTES];
     uint8_t b_hi[S][B_BYTES];
     uint8_t b_lo[S][B_BYTES];
-    double2 pend[R][MIXED ? kTileLens : 1][CH];  // P[j + len_d] per distinct length d
-    float4 st[M2][CH][MIXED ? kTileLens : 1];    // (mean, 1/std or 0 / -1, rel. std error, mean error)
-    double2 win_p[M2][TN];                       // mixed: prefix sums at each window start
-    uint16_t win_run[M2][TN];                    //   constant-run length at each window start
-    uint8_t win_miss[M2][TN];                    //   first sample missing
-    int lens[M2][kTileLens];                     //   distinct lengths of the tile
-    uint32_t lwc[M2][kTileLens];                 //   their window counts
-    double linv[M2][kTileLens];                  //   their inverses
-    float win_mean[W2][TN];                      // single-length tiles: window statistics
+    // (mean, 1/std or 0 / -1, rel. std error, mean error) of window i of a group of G
+    // windows for distinct length d at [warp][d G + (i ^ (d & 7))] (G x d < 256): lanes
+    // reading different lengths for the same window hit different banks
+    float4 wst[WL][256];
+    int wl_len[WL][32];        // the warp's distinct lengths
+    uint32_t wl_wc[WL][32];    //   their window counts in the searched range
+    double wl_inv[WL][32];     //   their inverses
+    float win_mean[W2][TN];    // single-length tiles: window statistics
     float win_inv[W2][TN];
-    Candidate stage[8][STAGE];                   // per epilogue warp: candidates before their flush
+    Candidate stage[8][STAGE]; // per epilogue warp: candidates before their flush
     uint64_t full_a[S], full_b[S], empty[S];
-    uint64_t acc_full[2], acc_empty[2], win_ready[2], drain, pend_bar[R], st_ready[2];
+    uint64_t acc_full[2], acc_empty[2], win_ready[2], drain;
     uint32_t tmem_base;
     int abort;
 };
@@ -198,15 +194,6 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v)
         v[i] = __uint_as_float(r[i]);
 }
 
-// 1-D bulk copy global -> shared (16-byte aligned addresses, size a multiple of 16).
-__device__ __forceinline__ void bulk_copy(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
-{
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     saddr(dst)),
-                 "l"(src), "r"(bytes), "r"(saddr(bar))
-                 : "memory");
-}
-
 __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float *v)
 {
     uint32_t r[8];
@@ -268,11 +255,8 @@ __global__ void __launch_bounds__(THREADS, 1)
             mbar_init(&sm.acc_full[b], 1);
             mbar_init(&sm.acc_empty[b], EPI);
             mbar_init(&sm.win_ready[b], EPI);
-            mbar_init(&sm.st_ready[b], EPI);
         }
         mbar_init(&sm.drain, 1);
-        for (int r = 0; r < Sm::R; r++)
-            mbar_init(&sm.pend_bar[r], EPI);
         sm.abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -420,39 +404,22 @@ __global__ void __launch_bounds__(THREADS, 1)
         const int row = quarter * 32 + lane;  // TMEM lane = template row within the tile
         const int et = threadIdx.x - 128;     // 0..255
         constexpr uint32_t STAGE = Sm::STAGE;
-        uint32_t tc = 0, pend_it = 0, st_it = 0, staged = 0;
+        const PrefixView pv{a.P, a.PT, a.PC};
+        uint32_t tc = 0, staged = 0;
         for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x, tc++)
         {
             const int buf = tc & 1;
-            const int mb = MIXED ? buf : 0;
             const int tt = (int)(tile / ua.w_tiles);
             const uint32_t j0 = (uint32_t)(tile % ua.w_tiles) * TN;
+            if (!MIXED)
             {
-                const int i = et; // one window per epilogue thread
-                const uint32_t j = j0 + i;
-                if (MIXED)
-                {
-                    const bool in = j < a.W;
-                    const double2 pv = in ? a.P[a.w0 + j] : make_double2(0.0, 0.0);
-                    sm.win_p[mb][i] = pv;
-                    sm.win_run[mb][i] = in ? a.run[a.w0 + j] : (uint16_t)65535;
-                    sm.win_miss[mb][i] = in ? (uint8_t)(a.raw[a.w0 + j] == kMissing) : (uint8_t)1;
-                    if (et < kTileLens)
-                    {
-                        sm.lens[mb][et] = a.tiles[tt].len[et];
-                        sm.lwc[mb][et] = a.tiles[tt].wc[et];
-                        sm.linv[mb][et] = a.tiles[tt].inv_m[et];
-                    }
-                }
-                else
-                {
-                    sm.win_mean[buf & (Sm::W2 - 1)][i] = j < a.W ? a.mean[j] : 0.0f;
-                    sm.win_inv[buf & (Sm::W2 - 1)][i] = j < a.W ? a.inv[j] : 0.0f;
-                }
+                const uint32_t j = j0 + et; // one window per epilogue thread
+                sm.win_mean[buf & (Sm::W2 - 1)][et] = j < a.W ? a.mean[j] : 0.0f;
+                sm.win_inv[buf & (Sm::W2 - 1)][et] = j < a.W ? a.inv[j] : 0.0f;
+                mbar_arrive(&sm.win_ready[buf]);
+                if (!mbar_wait_warp(&sm.win_ready[buf], (tc >> 1) & 1, sm.abort, ua.err, 7))
+                    goto done;
             }
-            mbar_arrive(&sm.win_ready[buf]);
-            if (!mbar_wait_warp(&sm.win_ready[buf], (tc >> 1) & 1, sm.abort, ua.err, 7))
-                goto done;
             const float shift = tile_shift<MIXED>(a, j0);
             const int t = tt * TM + row;
             TemplParam p;
@@ -466,7 +433,33 @@ __global__ void __launch_bounds__(THREADS, 1)
             {
                 p.mode = 0;
                 p.thr_ed = -kFltMax;
-                p.didx = 0;
+                p.m = 0;
+            }
+            // mixed: the distinct lengths of this warp's rows (at most 32), found while the
+            // tile's MMAs run; my_d is the lane's entry
+            int my_d = 0, nd = 0;
+            if (MIXED)
+            {
+                __syncwarp(); // the previous tile's readers of the tables are done
+                uint32_t pending = __ballot_sync(0xffffffffu, valid);
+                while (pending != 0u)
+                {
+                    const int leader = __ffs(pending) - 1;
+                    const int len = __shfl_sync(0xffffffffu, p.m, leader);
+                    const bool mine = valid && p.m == len;
+                    const uint32_t same = __ballot_sync(0xffffffffu, mine);
+                    if (mine)
+                        my_d = nd;
+                    if (lane == leader)
+                    {
+                        sm.wl_len[ew][nd] = len;
+                        sm.wl_wc[ew][nd] = p.wcount; // a function of the length alone
+                        sm.wl_inv[ew][nd] = p.inv_m;
+                    }
+                    nd++;
+                    pending &= ~same;
+                }
+                __syncwarp();
             }
             if (!mbar_wait_warp(&sm.acc_full[buf], (tc >> 1) & 1, sm.abort, ua.err, 6))
                 goto done;
@@ -475,70 +468,53 @@ __global__ void __launch_bounds__(THREADS, 1)
             const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(buf * TN);
             if (MIXED)
             {
-                // Phase A per 16-window chunk: statistics of every (window, distinct length)
-                // from the window-start prefix sums and the window-end prefix sums, which
-                // bulk copies (one per length, issued by thread d) bring two chunks ahead.
-                // Phase B: each lane's distances from its length's statistics.
-                const int D = a.tiles[tt].D;
-                constexpr uint32_t RING = Sm::R;
-                const PrefixView pv{a.P, a.PT, a.PC};
-                auto issue = [&](int cc, uint32_t k) {
-                    const uint32_t slot = k % RING;
-                    if (et < D)
-                    {
-                        // within the zero-padded prefix array: j0 + CH*cc < W + 256, len <= 16384
-                        const uint64_t src = a.w0 + j0 + (uint64_t)(CH * cc) + (uint64_t)sm.lens[mb][et];
-                        fence_proxy_async();
-                        mbar_expect_tx(&sm.pend_bar[slot], CH * 16);
-                        bulk_copy(&sm.pend[slot][et][0], a.P + src, CH * 16, &sm.pend_bar[slot]);
-                    }
-                    else
-                        mbar_arrive(&sm.pend_bar[slot]);
-                };
-                for (int cc = 0; cc < (int)RING - 1; cc++)
-                    issue(cc, pend_it + cc);
-                for (int cc = 0; cc < NCH; cc++, pend_it++, st_it++)
+                // This warp's 128 windows of the tile (128 half .. + 127) in groups of G
+                // windows, G x nd <= 256 table entries (G = 32 for up to 8 lengths):
+                // phase A: statistics of each (window, distinct length of the warp) from the
+                //   prefix sums at the window's start and end (G lanes per length read G
+                //   consecutive windows; the four loads of an item are independent);
+                // phase B: each lane's distances from its length's statistics, 8 windows
+                //   per TMEM load, one candidate emission per group.
+                const int glog = nd <= 8 ? 5 : (nd <= 16 ? 4 : 3);
+                const int G = 1 << glog;
+                for (int c0 = 128 * half; c0 < 128 * half + 128; c0 += G)
                 {
-                    if (cc + (int)RING - 1 < NCH)
-                        issue(cc + RING - 1, pend_it + RING - 1);
-                    if (!mbar_wait_warp(&sm.pend_bar[pend_it % RING], (pend_it / RING) & 1, sm.abort, ua.err, 8))
+                    for (int q = lane; q < (nd << glog); q += 32)
                     {
-                        for (uint32_t k = 1; k < RING && cc + (int)k < NCH; k++) // copies in flight land first
-                            mbar_drain(&sm.pend_bar[(pend_it + k) % RING], ((pend_it + k) / RING) & 1);
-                        goto done;
-                    }
-                    const int sb = st_it & 1;
-                    for (int q = et; q < D * CH; q += EPI)
-                    {
-                        const int d = q % D, i = q / D;
-                        const int ci = CH * cc + i;
-                        const uint32_t j = j0 + ci;
+                        const int i = q & (G - 1), d = q >> glog;
+                        const uint32_t j = j0 + (uint32_t)(c0 + i);
                         float4 r = make_float4(0.0f, 0.0f, 0.0f, 0.0f); // iv 0: not searched
-                        const int len = sm.lens[mb][d];
-                        if (j < sm.lwc[mb][d] && !sm.win_miss[mb][ci] && sm.win_run[mb][ci] < len)
+                        const int len = sm.wl_len[ew][d];
+                        if (j < sm.wl_wc[ew][d]) // then w0 + j + len <= n: both prefix entries exist
                         {
-                            WindowStats ws;
-                            if (window_prefix_stats(pv, sm.win_p[mb][ci], sm.pend[pend_it % RING][d][i], a.w0 + j,
-                                                    len, sm.linv[mb][d], ws) == 0)
-                                r = make_float4(ws.mu, ws.iv, ws.rel_sd, ws.e_mu);
-                            else
-                                r.y = -1.0f; // statistics not trustworthy: exact re-scoring decides
+                            const uint64_t g = a.w0 + j;
+                            const double2 qa = a.P[g], qb = a.P[g + (uint64_t)len];
+                            const float rv = a.raw[g];
+                            const uint16_t rn = a.run[g];
+                            if (rv != kMissing && rn < len)
+                            {
+                                WindowStats ws;
+                                if (window_prefix_stats(pv, qa, qb, g, len, sm.wl_inv[ew][d], ws) == 0)
+                                    r = make_float4(ws.mu, ws.iv, ws.rel_sd, ws.e_mu);
+                                else
+                                    r.y = -1.0f; // statistics not trustworthy: exact re-scoring decides
+                            }
                         }
-                        sm.st[sb][i][d] = r;
+                        sm.wst[ew][(d << glog) + (i ^ (d & 7))] = r;
                     }
-                    mbar_arrive(&sm.st_ready[sb]);
-                    if (!mbar_wait_warp(&sm.st_ready[sb], (st_it >> 1) & 1, sm.abort, ua.err, 9))
-                        goto done;
-                    float v[8];
-                    const int c0 = CH * cc + 8 * half; // this warp's 8 columns of the chunk
-                    tmem_ld8(taddr + c0, v);
+                    __syncwarp();
                     uint32_t mask = 0;
-                    if (valid)
+                    const float4 *mine = &sm.wst[ew][my_d << glog];
+                    for (int s8 = 0; s8 < G; s8 += 8)
                     {
+                        float v[8];
+                        tmem_ld8(taddr + c0 + s8, v);
+                        if (!valid)
+                            continue;
 #pragma unroll
                         for (int i = 0; i < 8; i++)
                         {
-                            const float4 r = sm.st[sb][8 * half + i][p.didx];
+                            const float4 r = mine[(s8 + i) ^ (my_d & 7)];
                             if (r.y == 0.0f)
                                 continue; // beyond the template's windows, missing first sample, constant
                             if (r.y < 0.0f)
@@ -546,7 +522,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                                 if (p.mode == 1)
                                     lmin = -inf_f();
                                 else
-                                    mask |= 1u << i;
+                                    mask |= 1u << (s8 + i);
                                 continue;
                             }
                             WindowStats ws;
@@ -559,7 +535,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                                                 dd, e);
                             if (a.dbg_d != nullptr)
                             {
-                                const size_t at = (size_t)t * a.W + j0 + c0 + i;
+                                const size_t at = (size_t)t * a.W + j0 + c0 + s8 + i;
                                 a.dbg_d[at] = dd;
                                 a.dbg_e[at] = e;
                             }
@@ -570,9 +546,10 @@ __global__ void __launch_bounds__(THREADS, 1)
                                 lmin = fminf(lmin, lo);
                             }
                             else if (lo <= p.thr_ed)
-                                mask |= 1u << i;
+                                mask |= 1u << (s8 + i);
                         }
                     }
+                    __syncwarp(); // every lane has read the group's statistics
                     stage_emit<STAGE>(mask, lane, (uint32_t)t, j0 + c0, sm.stage[ew], staged, a.cand, a.cand_count,
                                       a.cand_cap);
                 }
