@@ -310,14 +310,14 @@ struct tm_ctx
     // tiling cost model: kernel milliseconds for 128 templates x 2^25 windows, per group kind
     // (one length / several), shape (row tiles; column tiles of 128, 64, 32) and K (256,
     // 1024, 4096, 16384). Defaults: a B200 measurement; tm_autotune re-measures.
-    double tile_ms[2][4][4] = {{{17.5, 19.3, 68.8, 272.5},
-                                {29.9, 32.1, 90.9, 346.8},
-                                {31.8, 43.5, 157.4, 580.8},
-                                {36.7, 84.3, 308.9, 1129.8}},
-                               {{31.9, 35.9, 67.5, 261.8},
-                                {65.1, 70.5, 100.6, 351.7},
-                                {69.0, 78.3, 159.3, 580.5},
-                                {75.7, 92.5, 310.2, 1135.9}}};
+    double tile_ms[2][4][4] = {{{7.5, 17.2, 59.3, 259.0},
+                                {29.7, 31.5, 84.7, 331.8},
+                                {31.6, 42.9, 157.5, 581.6},
+                                {36.3, 83.4, 307.4, 1133.7}},
+                               {{11.1, 17.0, 59.3, 259.3},
+                                {82.1, 84.8, 100.2, 341.1},
+                                {84.7, 88.6, 160.7, 584.4},
+                                {90.0, 96.8, 306.7, 1126.6}}};
     std::map<int, std::unique_ptr<tmh::LengthStats>> lengths;
     uint64_t use_clock = 0;
     tmh::DevBuf suf; // window-statistics scratch (per-length statistics)

@@ -65,15 +65,17 @@ template <bool MIXED> struct SmemT
     uint8_t a_lo[S][A_BYTES];
     uint8_t b_hi[S][B_BYTES];
     uint8_t b_lo[S][B_BYTES];
-    // (mean, 1/std or 0 / -1, rel. std error, mean error) of window i of a group of G
-    // windows for distinct length d at [warp][d G + (i ^ (d & 7))] (G x d < 256): lanes
-    // reading different lengths for the same window hit different banks
+    // window terms (1/sigma, mu - shift, E0, 0) of window i of a group of G windows for
+    // distinct length d at [warp][d G + (i ^ (d & 7))] (G x d <= 256): lanes reading
+    // different lengths for the same window hit different banks
     float4 wst[WL][256];
     int wl_len[WL][32];        // the warp's distinct lengths
     uint32_t wl_wc[WL][32];    //   their window counts in the searched range
     double wl_inv[WL][32];     //   their inverses
-    float win_mean[W2][TN];    // single-length tiles: window statistics
-    float win_inv[W2][TN];
+    float4 wl_c[WL][32];       //   maxima over their rows of a1, a5, a6 and 1.25 (4 m + 2 qs)
+    float wl_b[WL][32];        //   and of 2.5 |s1|
+    float4 win4[W2][TN];       // single-length tiles: window terms (win_terms)
+    float win_h[W2][TN];
     Candidate stage[8][STAGE]; // per epilogue warp: candidates before their flush
     uint64_t full_a[S], full_b[S], empty[S];
     uint64_t acc_full[2], acc_empty[2], win_ready[2], drain;
@@ -228,6 +230,98 @@ template <bool MIXED> __device__ __forceinline__ float tile_shift(const ScanArgs
 {
     const uint32_t jm = min(j0 + TN / 2, a.W - 1);
     return MIXED ? a.x[a.w0 + jm] : a.mean[jm];
+}
+
+// The bound of fast_distance (tm_epilogue.cuh) with its window-only factors hoisted out
+// of the per-pair loop:
+//   e = a1 S + a2 + a3 max(d, 0) + a4 (1 + 2 Q) + a5 Q + a6 H,
+//   S = sqrt(1 + r^2), r = (mu - shift) / sigma, Q = (mu / sigma)^2, H = (|mu| + |shift|) / sigma,
+// evaluated as e = a3 max(d, 0) + eb with eb = a1 S + (2 a4 + a5) Q + a6 H + (a2 + a4).
+// Window terms: (1/sigma, mu - shift, S, Q) and H. A window that is not searched has
+// 1/sigma = 0 and S = NaN: its e, d - e and d + e are NaN, which no threshold comparison
+// accepts and fminf ignores, so the per-pair code needs no branch.
+__device__ __forceinline__ float nan_f() { return __int_as_float(0x7fc00000); }
+
+__device__ __forceinline__ float4 skip_terms(float &h)
+{
+    h = 0.0f;
+    return make_float4(0.0f, 0.0f, nan_f(), 0.0f);
+}
+
+__device__ __forceinline__ float4 win_terms(float mu, float iv, float shift, float &h)
+{
+    if (iv == 0.0f)
+        return skip_terms(h);
+    const float ms = mu - shift;
+    const float r = ms * iv, r0 = mu * iv;
+    h = (fabsf(mu) + fabsf(shift)) * iv;
+    return make_float4(iv, ms, sqrtf(1.0f + r * r), r0 * r0);
+}
+
+// Per-template (lane) constants of the hoisted bound. thr is the threshold on d - e, NaN
+// for kNN templates and padding rows (no window passes it).
+struct LaneTerms
+{
+    float s1, c_lin, a1, a3, a45, a6, c24, a2, thr;
+};
+
+__device__ __forceinline__ LaneTerms lane_terms(const TemplParam &p, bool valid)
+{
+    LaneTerms l;
+    l.s1 = p.s1;
+    l.c_lin = p.c_lin;
+    l.a1 = p.a1_main;
+    l.a3 = p.a3;
+    l.a45 = 2.0f * p.a4 + p.a5;
+    l.a6 = p.a6;
+    l.c24 = p.a2 + p.a4;
+    l.a2 = p.a2;
+    l.thr = (valid && p.mode != 1) ? p.thr_ed : nan_f();
+    return l;
+}
+
+// Mixed-length tiles: the window terms of one (window, length) from its statistics and
+// the length's coefficient maxima c = (a1, a5, a6, 1.25 (4 m + 2 qs)) and cb = 2.5 |s1|:
+// (1/sigma, mu - shift, E0, 0) with E0 = the window part of fast_distance_mixed's bound
+// without a2 (a1 S + a5 Q + a6 H + the statistics' own error term of stats_error). With
+// the maxima over the length's rows in place of each row's own coefficients, E0 bounds
+// that part for every row of the length.
+__device__ __forceinline__ float4 mixed_terms(const WindowStats &ws, float shift, float4 c, float cb)
+{
+    const float ms = ws.mu - shift;
+    const float r = ms * ws.iv, r0 = ws.mu * ws.iv;
+    const float e0 = c.x * sqrtf(1.0f + r * r) + c.y * (r0 * r0) + c.z * (fabsf(ws.mu) + fabsf(shift)) * ws.iv +
+                     c.w * ws.rel_sd + cb * (ws.e_mu * ws.iv);
+    return make_float4(ws.iv, ms, e0, 0.0f);
+}
+
+// Maximum of a non-negative float over the lanes where `mine` holds (0 when none).
+__device__ __forceinline__ float warp_max_nonneg(bool mine, float v)
+{
+    return __uint_as_float(__reduce_max_sync(0xffffffffu, mine ? __float_as_uint(v) : 0u));
+}
+
+// d and e of one pair from its shifted dot product (fast_distance's d, evaluated the same
+// way) and the window part eb of its bound.
+__device__ __forceinline__ void pair_bound(const LaneTerms &l, float dot, float iv, float ms, float eb, float &d,
+                                           float &e)
+{
+    const float cross = (dot - ms * l.s1) * iv;
+    d = l.c_lin - 2.0f * cross;
+    e = fmaf(l.a3, fmaxf(d, 0.0f), eb);
+}
+
+// Threshold bit i of mask when d - e <= thr; kNN bucket minima of d + e and d - e (used
+// only for kNN rows).
+__device__ __forceinline__ void pair_update(const LaneTerms &l, float dot, float iv, float ms, float eb, int i,
+                                            uint32_t &mask, float &umin, float &lmin)
+{
+    float d, e;
+    pair_bound(l, dot, iv, ms, eb, d, e);
+    const float lo = d - e;
+    umin = fminf(umin, d + e);
+    lmin = fminf(lmin, lo);
+    mask |= (lo <= l.thr ? 1u : 0u) << i;
 }
 
 template <bool MIXED>
@@ -414,8 +508,10 @@ __global__ void __launch_bounds__(THREADS, 1)
             if (!MIXED)
             {
                 const uint32_t j = j0 + et; // one window per epilogue thread
-                sm.win_mean[buf & (Sm::W2 - 1)][et] = j < a.W ? a.mean[j] : 0.0f;
-                sm.win_inv[buf & (Sm::W2 - 1)][et] = j < a.W ? a.inv[j] : 0.0f;
+                float h;
+                sm.win4[buf & (Sm::W2 - 1)][et] =
+                    j < a.W ? win_terms(a.mean[j], a.inv[j], tile_shift<false>(a, j0), h) : skip_terms(h);
+                sm.win_h[buf & (Sm::W2 - 1)][et] = h;
                 mbar_arrive(&sm.win_ready[buf]);
                 if (!mbar_wait_warp(&sm.win_ready[buf], (tc >> 1) & 1, sm.abort, ua.err, 7))
                     goto done;
@@ -431,9 +527,8 @@ __global__ void __launch_bounds__(THREADS, 1)
             }
             if (!valid)
             {
-                p.mode = 0;
+                p = TemplParam{};
                 p.thr_ed = -kFltMax;
-                p.m = 0;
             }
             // mixed: the distinct lengths of this warp's rows (at most 32), found while the
             // tile's MMAs run; my_d is the lane's entry
@@ -450,11 +545,19 @@ __global__ void __launch_bounds__(THREADS, 1)
                     const uint32_t same = __ballot_sync(0xffffffffu, mine);
                     if (mine)
                         my_d = nd;
+                    // bound coefficients of the length: maxima over its rows (all >= 0, so
+                    // the float bit patterns order like the values)
+                    const float c1 = warp_max_nonneg(mine, p.a1_main), c5 = warp_max_nonneg(mine, p.a5);
+                    const float c6 = warp_max_nonneg(mine, p.a6);
+                    const float cA = warp_max_nonneg(mine, 1.25f * (4.0f * (float)p.m + 2.0f * p.qs));
+                    const float cB = warp_max_nonneg(mine, 2.5f * fabsf(p.s1));
                     if (lane == leader)
                     {
                         sm.wl_len[ew][nd] = len;
                         sm.wl_wc[ew][nd] = p.wcount; // a function of the length alone
                         sm.wl_inv[ew][nd] = p.inv_m;
+                        sm.wl_c[ew][nd] = make_float4(c1, c5, c6, cA);
+                        sm.wl_b[ew][nd] = cB;
                     }
                     nd++;
                     pending &= ~same;
@@ -475,6 +578,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                 //   consecutive windows; the four loads of an item are independent);
                 // phase B: each lane's distances from its length's statistics, 8 windows
                 //   per TMEM load, one candidate emission per group.
+                const LaneTerms lt = lane_terms(p, valid);
                 const int glog = nd <= 8 ? 5 : (nd <= 16 ? 4 : 3);
                 const int G = 1 << glog;
                 for (int c0 = 128 * half; c0 < 128 * half + 128; c0 += G)
@@ -483,7 +587,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                     {
                         const int i = q & (G - 1), d = q >> glog;
                         const uint32_t j = j0 + (uint32_t)(c0 + i);
-                        float4 r = make_float4(0.0f, 0.0f, 0.0f, 0.0f); // iv 0: not searched
+                        float4 r = make_float4(0.0f, 0.0f, nan_f(), 0.0f); // not searched
                         const int len = sm.wl_len[ew][d];
                         if (j < sm.wl_wc[ew][d]) // then w0 + j + len <= n: both prefix entries exist
                         {
@@ -495,9 +599,9 @@ __global__ void __launch_bounds__(THREADS, 1)
                             {
                                 WindowStats ws;
                                 if (window_prefix_stats(pv, qa, qb, g, len, sm.wl_inv[ew][d], ws) == 0)
-                                    r = make_float4(ws.mu, ws.iv, ws.rel_sd, ws.e_mu);
+                                    r = mixed_terms(ws, shift, sm.wl_c[ew][d], sm.wl_b[ew][d]);
                                 else
-                                    r.y = -1.0f; // statistics not trustworthy: exact re-scoring decides
+                                    r.z = inf_f(); // statistics not trustworthy: d - e = -inf, exact re-scoring decides
                             }
                         }
                         sm.wst[ew][(d << glog) + (i ^ (d & 7))] = r;
@@ -509,45 +613,24 @@ __global__ void __launch_bounds__(THREADS, 1)
                     {
                         float v[8];
                         tmem_ld8(taddr + c0 + s8, v);
-                        if (!valid)
-                            continue;
 #pragma unroll
                         for (int i = 0; i < 8; i++)
                         {
-                            const float4 r = mine[(s8 + i) ^ (my_d & 7)];
-                            if (r.y == 0.0f)
-                                continue; // beyond the template's windows, missing first sample, constant
-                            if (r.y < 0.0f)
+                            const float4 w = mine[(s8 + i) ^ (my_d & 7)];
+                            pair_update(lt, v[i], w.x, w.y, w.z + lt.a2, s8 + i, mask, umin, lmin);
+                        }
+                        if (a.dbg_d != nullptr && valid)
+                            for (int i = 0; i < 8; i++)
                             {
-                                if (p.mode == 1)
-                                    lmin = -inf_f();
-                                else
-                                    mask |= 1u << (s8 + i);
-                                continue;
-                            }
-                            WindowStats ws;
-                            ws.mu = r.x;
-                            ws.iv = r.y;
-                            ws.rel_sd = r.z;
-                            ws.e_mu = r.w;
-                            float dd, e;
-                            fast_distance_mixed(p, p.a1_main, v[i], ws.mu, ws.iv, shift, stats_error(ws, p.m, p.qs, p.s1),
-                                                dd, e);
-                            if (a.dbg_d != nullptr)
-                            {
+                                const float4 w = mine[(s8 + i) ^ (my_d & 7)];
+                                if (w.x == 0.0f)
+                                    continue; // not searched, or untrustworthy statistics
+                                float dd, e;
+                                pair_bound(lt, v[i], w.x, w.y, w.z + lt.a2, dd, e);
                                 const size_t at = (size_t)t * a.W + j0 + c0 + s8 + i;
                                 a.dbg_d[at] = dd;
                                 a.dbg_e[at] = e;
                             }
-                            const float lo = dd - e;
-                            if (p.mode == 1)
-                            {
-                                umin = fminf(umin, dd + e);
-                                lmin = fminf(lmin, lo);
-                            }
-                            else if (lo <= p.thr_ed)
-                                mask |= 1u << (s8 + i);
-                        }
                     }
                     __syncwarp(); // every lane has read the group's statistics
                     stage_emit<STAGE>(mask, lane, (uint32_t)t, j0 + c0, sm.stage[ew], staged, a.cand, a.cand_count,
@@ -557,37 +640,33 @@ __global__ void __launch_bounds__(THREADS, 1)
             else
             {
                 const int wb = buf & (Sm::W2 - 1);
+                const LaneTerms lt = lane_terms(p, valid);
                 for (int c = 8 * half; c < 8 * half + 8; c++) // this warp's 128 of the 256 columns
                 {
                     float v[16];
                     tmem_ld16(taddr + c * 16, v);
                     uint32_t mask = 0;
-                    if (valid)
-                    {
 #pragma unroll
+                    for (int i = 0; i < 16; i++)
+                    {
+                        const float4 w = sm.win4[wb][c * 16 + i];
+                        const float eb = fmaf(lt.a1, w.z, fmaf(lt.a45, w.w, fmaf(lt.a6, sm.win_h[wb][c * 16 + i], lt.c24)));
+                        pair_update(lt, v[i], w.x, w.y, eb, i, mask, umin, lmin);
+                    }
+                    if (a.dbg_d != nullptr && valid)
                         for (int i = 0; i < 16; i++)
                         {
-                            const float iv = sm.win_inv[wb][c * 16 + i];
-                            if (iv == 0.0f)
+                            const float4 w = sm.win4[wb][c * 16 + i];
+                            if (w.x == 0.0f)
                                 continue;
+                            const float eb =
+                                fmaf(lt.a1, w.z, fmaf(lt.a45, w.w, fmaf(lt.a6, sm.win_h[wb][c * 16 + i], lt.c24)));
                             float dd, e;
-                            fast_distance(p, p.a1_main, v[i], sm.win_mean[wb][c * 16 + i], iv, shift, dd, e);
-                            if (a.dbg_d != nullptr)
-                            {
-                                const size_t at = (size_t)t * a.W + j0 + c * 16 + i;
-                                a.dbg_d[at] = dd;
-                                a.dbg_e[at] = e;
-                            }
-                            const float lo = dd - e;
-                            if (p.mode == 1)
-                            {
-                                umin = fminf(umin, dd + e);
-                                lmin = fminf(lmin, lo);
-                            }
-                            else if (lo <= p.thr_ed)
-                                mask |= 1u << i;
+                            pair_bound(lt, v[i], w.x, w.y, eb, dd, e);
+                            const size_t at = (size_t)t * a.W + j0 + c * 16 + i;
+                            a.dbg_d[at] = dd;
+                            a.dbg_e[at] = e;
                         }
-                    }
                     stage_emit<STAGE>(mask, lane, (uint32_t)t, j0 + c * 16, sm.stage[ew], staged, a.cand, a.cand_count,
                                       a.cand_cap);
                 }
