@@ -114,10 +114,12 @@ class ClockSampler:
         self.device, self.proc, self.lines = device, None, []
         self.first = threading.Event()
 
+    WARM_SAMPLES = 3
+
     def start(self):
-        """Starts sampling and returns once the first sample is in (at most 10 s): NVML's
-        start-up in nvidia-smi can hold the driver for about a second, which must not
-        fall inside the timed region."""
+        """Starts sampling and returns once the first WARM_SAMPLES samples are in (at most
+        10 s): NVML's start-up in nvidia-smi can hold the driver for about a second, which
+        must not fall inside the timed region."""
         try:
             self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.device), f'--query-gpu={self.FIELDS}',
                                           '--format=csv,noheader,nounits', '-lms', '200'],
@@ -131,7 +133,8 @@ class ClockSampler:
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
-            self.first.set()
+            if len(self.lines) >= self.WARM_SAMPLES:
+                self.first.set()
         self.first.set()
 
     def stop(self):
@@ -653,7 +656,8 @@ def run_ours(args, w):
                 'gpu_launches': all_launches, 'clocks': clocks,
                 'd2h_bytes_per_step_value': d2h_value // args.steps,
                 'candidates_last_step': ctx.last_candidates(),
-                'phases_ms_per_step': phase_ms}
+                'phases_ms_per_step': phase_ms,
+                'step_ms': [round(a.elapsed_time(b), 3) for a, b in zip(step_ev, step_ev[1:])]}
         print(json.dumps(line), flush=True)
     for b in batches:
         b.close()

@@ -123,6 +123,18 @@ int tm_ctx_create(const float *raw, uint64_t n, int device, tm_ctx **out)
     ctx->n = n;
     const int rc = guarded(ctx.get(), [&] {
         TM_CUDA(cudaSetDevice(device));
+        // per-batch buffers come from the device's default memory pool (DevBuf::reserve_on):
+        // let it keep up to 4 GiB of freed memory for the next batch instead of returning it
+        // to the driver at every synchronisation (a property of this process's pool only)
+        cudaMemPool_t pool = nullptr;
+        TM_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+        uint64_t keep = 0;
+        TM_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+        if (keep < (4ull << 30))
+        {
+            keep = 4ull << 30;
+            TM_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+        }
         ctx->main.open();
         const uint64_t total = n + tmb::kStagePad;
         ctx->raw.reserve(sizeof(float) * total);

@@ -102,25 +102,48 @@ struct DevBuf
 {
     void *p = nullptr;
     size_t bytes = 0;
+    bool pooled = false; // from the device's memory pool (reserve_on)
     void reserve(size_t need)
     {
         if (need <= bytes)
             return;
-        if (p)
-            cudaFree(p);
-        p = nullptr;
-        bytes = 0;
+        release();
         size_t b = std::max<size_t>(need, 256);
         TM_CUDA(cudaMalloc(&p, b));
         bytes = b;
     }
+    // Stream-ordered allocation from the device's default memory pool, for the buffers of
+    // one batch: freeing returns the memory to the pool without the device-wide
+    // synchronisation and unmapping of cudaFree (tens of milliseconds with a large
+    // context), and the next batch's allocation takes it back from there. A buffer that
+    // grows is freed after the work already queued on s.
+    void reserve_on(size_t need, cudaStream_t s)
+    {
+        if (need <= bytes)
+            return;
+        drop(s);
+        size_t b = std::max<size_t>(need, 256);
+        TM_CUDA(cudaMallocAsync(&p, b, s));
+        bytes = b;
+        pooled = true;
+    }
     template <class T> T *as() const { return static_cast<T *>(p); }
-    void release()
+    // Callers release only after the work that used the buffer has completed.
+    void release() { drop(0); }
+
+  private:
+    void drop(cudaStream_t s)
     {
         if (p)
-            cudaFree(p);
+        {
+            if (pooled)
+                cudaFreeAsync(p, s);
+            else
+                cudaFree(p);
+        }
         p = nullptr;
         bytes = 0;
+        pooled = false;
     }
 };
 

@@ -95,10 +95,10 @@ void prepare_group(tm_ctx *ctx, Lane &L, int m, const std::vector<int> &idx, con
         g.htp[t].m = m;
     }
     cudaStream_t s = L.stream;
-    g.q.reserve(sizeof(float) * static_cast<size_t>(T_pad) * m_pad);
-    g.order.reserve(sizeof(int) * static_cast<size_t>(T) * nblk);
-    g.tp.reserve(sizeof(TemplParam) * T_pad);
-    g.slots.reserve(sizeof(int) * std::max(g.nk, 1));
+    g.q.reserve_on(sizeof(float) * static_cast<size_t>(T_pad) * m_pad, s);
+    g.order.reserve_on(sizeof(int) * static_cast<size_t>(T) * nblk, s);
+    g.tp.reserve_on(sizeof(TemplParam) * T_pad, s);
+    g.slots.reserve_on(sizeof(int) * std::max(g.nk, 1), s);
     TM_CUDA(cudaMemcpyAsync(g.q.p, hq, sizeof(float) * static_cast<size_t>(T_pad) * m_pad, cudaMemcpyHostToDevice, s));
     TM_CUDA(cudaMemcpyAsync(g.order.p, ho, sizeof(int) * static_cast<size_t>(T) * nblk, cudaMemcpyHostToDevice, s));
     TM_CUDA(cudaMemcpyAsync(g.tp.p, g.htp.data(), sizeof(TemplParam) * T_pad, cudaMemcpyHostToDevice, s));
@@ -120,8 +120,8 @@ void prepare_group(tm_ctx *ctx, Lane &L, int m, const std::vector<int> &idx, con
                 hh[at] = bf16_bits(v);
                 hl[at] = bf16_bits(v - bf16_value(hh[at]));
             }
-        g.q_hi.reserve(sizeof(uint16_t) * elems);
-        g.q_lo.reserve(sizeof(uint16_t) * elems);
+        g.q_hi.reserve_on(sizeof(uint16_t) * elems, s);
+        g.q_lo.reserve_on(sizeof(uint16_t) * elems, s);
         TM_CUDA(cudaMemcpyAsync(g.q_hi.p, hh, sizeof(uint16_t) * elems, cudaMemcpyHostToDevice, s));
         TM_CUDA(cudaMemcpyAsync(g.q_lo.p, hl, sizeof(uint16_t) * elems, cudaMemcpyHostToDevice, s));
         h2d += 2 * sizeof(uint16_t) * static_cast<uint64_t>(T) * m;
@@ -246,13 +246,13 @@ void prepare_group_mixed(tm_ctx *ctx, Lane &L, const std::vector<int> &idx_in, c
     }
     g.tiles = tiles;
     cudaStream_t s = L.stream;
-    g.q.reserve(sizeof(float) * elems);
-    g.order.reserve(sizeof(int) * static_cast<size_t>(R) * nblk);
-    g.tp.reserve(sizeof(TemplParam) * R);
-    g.slots.reserve(sizeof(int) * std::max(g.nk, 1));
-    g.q_hi.reserve(sizeof(uint16_t) * elems);
-    g.q_lo.reserve(sizeof(uint16_t) * elems);
-    g.d_tiles.reserve(sizeof(tmb::TileInfo) * tiles.size());
+    g.q.reserve_on(sizeof(float) * elems, s);
+    g.order.reserve_on(sizeof(int) * static_cast<size_t>(R) * nblk, s);
+    g.tp.reserve_on(sizeof(TemplParam) * R, s);
+    g.slots.reserve_on(sizeof(int) * std::max(g.nk, 1), s);
+    g.q_hi.reserve_on(sizeof(uint16_t) * elems, s);
+    g.q_lo.reserve_on(sizeof(uint16_t) * elems, s);
+    g.d_tiles.reserve_on(sizeof(tmb::TileInfo) * tiles.size(), s);
     TM_CUDA(cudaMemcpyAsync(g.q.p, hq, sizeof(float) * elems, cudaMemcpyHostToDevice, s));
     TM_CUDA(cudaMemcpyAsync(g.order.p, ho, sizeof(int) * static_cast<size_t>(R) * nblk, cudaMemcpyHostToDevice, s));
     TM_CUDA(cudaMemcpyAsync(g.tp.p, g.htp.data(), sizeof(TemplParam) * R, cudaMemcpyHostToDevice, s));
@@ -439,6 +439,8 @@ void create_batch(tm_ctx *ctx, Lane &L, const tm_request *requests, int count, t
             specs.push_back(Spec{part, one_length && !serving ? 0 : 1});
         }
     }
+    for (size_t gi = specs.size(); gi < b.groups.size(); gi++) // a reused batch with fewer groups
+        b.groups[gi].release();
     b.groups.resize(specs.size());
     for (size_t gi = 0; gi < specs.size(); gi++)
     {
