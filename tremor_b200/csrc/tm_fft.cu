@@ -90,7 +90,7 @@ __global__ void k_fft_mul(const double2 *__restrict__ X, const double2 *__restri
 // kernels' epilogues (fast_distance_mixed), plus the FFT term 2 e_dot / sigma.
 __global__ void __launch_bounds__(256) k_fft_epilogue(const FftEpiArgs f)
 {
-    const TemplParam p = f.tp[f.t];
+    const TemplParam p = f.p;
     const uint32_t lp = blockIdx.y;                    // piece within the batch
     const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t g = (uint64_t)(f.p0 + lp) * kFftS + o; // global window start
@@ -107,8 +107,7 @@ __global__ void __launch_bounds__(256) k_fft_epilogue(const FftEpiArgs f)
         {
             const double dot = f.out[(size_t)lp * kFftL + o + (uint32_t)(p.m - 1)];
             const float shift = (float)f.shifts[f.p0 + lp];
-            const double sm = sqrt((double)p.m);
-            const float e_dot = (float)(kFftKappa * f.norms[f.p0 + lp] * sm * (2.0 * sm + sqrt((double)kFftL)) * 1.01);
+            const float e_dot = (float)(kFftKappa * f.norms[f.p0 + lp] * f.e_fac * 1.01);
             float d, e;
             fast_distance_mixed(p, p.a1_main, (float)dot, ws.mu, ws.iv, shift, stats_error(ws, p.m, p.qs, p.s1), d,
                                 e);

@@ -16,7 +16,8 @@ struct FftEpiArgs
     const double *out;     // count x kFftL correlation outputs of pieces p0 ..
     uint32_t p0, count;
     uint32_t t;            // template row
-    const TemplParam *tp;
+    TemplParam p;          // its constants, in the launch's parameter space (one broadcast copy)
+    double e_fac;          // sqrt(m) (2 sqrt(m) + sqrt(kFftL)): the template's factor of the output error
     uint64_t w0;           // window range start (windows are relative to it)
     PrefixView pv;
     const uint16_t *run;

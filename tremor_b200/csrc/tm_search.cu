@@ -598,7 +598,9 @@ void fft_contract(tm_ctx *ctx, Lane &L, const GroupPlan &g, const tmb::ScanArgs 
             f.p0 = p0;
             f.count = std::min<uint32_t>(B, P - p0);
             f.t = static_cast<uint32_t>(t);
-            f.tp = g.tp.as<TemplParam>();
+            f.p = g.htp[static_cast<size_t>(t)];
+            const double sm = std::sqrt(static_cast<double>(f.p.m));
+            f.e_fac = sm * (2.0 * sm + std::sqrt(static_cast<double>(tmb::kFftL)));
             f.w0 = a.w0;
             f.pv = tmb::PrefixView{a.P, a.PT, a.PC};
             f.run = a.run;
