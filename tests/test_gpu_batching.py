@@ -239,3 +239,27 @@ def test_many_distinct_lengths_per_tile(tiles):
         ctx.set_tiles(tiles)
         answers = ctx.scan_batch(reqs)
     _check(x, reqs, answers)
+
+
+def test_batches_created_and_destroyed_reuse_memory():
+    """Batches created, run and destroyed one after another take their device buffers
+    from the memory pool and give them back: the answers stay identical and the device's
+    free memory does not shrink from cycle to cycle."""
+    import torch
+    x = _waveform(1 << 17, 91)
+    rng = np.random.default_rng(92)
+    reqs = _requests(x, rng, [64, 200, 1000, 64, 333, 2048, 4096])
+    free, first = [], None
+    with tb.Context(x) as ctx:
+        for _ in range(20):
+            b = ctx.batch(reqs)
+            out = b.run()
+            b.close()
+            if first is None:
+                first = out
+            for (p0, d0), (p1, d1) in zip(first, out):
+                assert np.array_equal(p0, p1) and np.array_equal(d0.view(np.uint32), d1.view(np.uint32))
+            torch.cuda.synchronize()
+            free.append(torch.cuda.mem_get_info()[0])
+    assert free[-1] >= free[1] - (16 << 20), (free[1], free[-1])
+    _check(x, reqs, first)
