@@ -20,8 +20,9 @@
 //     supply the one-sample shift from row to row that no byte stride can express.
 //     Builder warps write the strip (hi and lo) from the waveform each stage.
 //
-// Warp roles (256 threads): warp 0 TMA producer, warp 1 TMEM owner + MMA issuer,
-// warps 2-3 strip builders, warps 4-7 epilogue (TMEM lane quarter = warp % 4).
+// Warp roles (384 threads): warp 0 TMA producer, warp 1 TMEM owner + MMA issuer,
+// warps 2-3 strip builders, warps 4-11 epilogue (TMEM lane quarter = warp % 4; warps w and
+// w + 4 split the tile's 256 columns).
 // Pipelines: S smem stages (full_a / full_b / empty mbarriers), two TMEM accumulators
 // of 256 columns (acc_full / acc_empty), persistent CTAs over (template tile, window
 // tile) pairs, template-tile-major so a tile's templates stay in L2.
