@@ -123,18 +123,16 @@ int tm_ctx_create(const float *raw, uint64_t n, int device, tm_ctx **out)
     ctx->n = n;
     const int rc = guarded(ctx.get(), [&] {
         TM_CUDA(cudaSetDevice(device));
-        // per-batch buffers come from the device's default memory pool (DevBuf::reserve_on):
-        // let it keep up to 4 GiB of freed memory for the next batch instead of returning it
-        // to the driver at every synchronisation (a property of this process's pool only)
-        cudaMemPool_t pool = nullptr;
-        TM_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
-        uint64_t keep = 0;
-        TM_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
-        if (keep < (4ull << 30))
-        {
-            keep = 4ull << 30;
-            TM_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
-        }
+        // per-batch buffers come from the context's own memory pool (DevBuf::reserve_on),
+        // which keeps up to 4 GiB of freed memory for the next batch instead of returning
+        // it to the driver at every synchronisation; the process's default pool is untouched
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        TM_CUDA(cudaMemPoolCreate(&ctx->pool, &props));
+        uint64_t keep = 4ull << 30;
+        TM_CUDA(cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep));
         ctx->main.open();
         const uint64_t total = n + tmb::kStagePad;
         ctx->raw.reserve(sizeof(float) * total);
@@ -169,6 +167,10 @@ int tm_ctx_destroy(tm_ctx *ctx)
     for (DevBuf *b : {&ctx->prefix, &ctx->ptot, &ctx->pcen, &ctx->run, &ctx->raw, &ctx->clean, &ctx->suf,
                       &ctx->fft_X, &ctx->fft_shift, &ctx->fft_norm})
         b->release();
+    // buffers of batches that outlive the context return to the pool when those batches
+    // are destroyed; the driver releases the pool's memory once none is outstanding
+    if (ctx->pool)
+        cudaMemPoolDestroy(ctx->pool);
     delete ctx;
     return TM_OK;
 }

@@ -112,18 +112,18 @@ struct DevBuf
         TM_CUDA(cudaMalloc(&p, b));
         bytes = b;
     }
-    // Stream-ordered allocation from the device's default memory pool, for the buffers of
-    // one batch: freeing returns the memory to the pool without the device-wide
+    // Stream-ordered allocation from a memory pool (the context's own), for the buffers
+    // of one batch: freeing returns the memory to the pool without the device-wide
     // synchronisation and unmapping of cudaFree (tens of milliseconds with a large
     // context), and the next batch's allocation takes it back from there. A buffer that
     // grows is freed after the work already queued on s.
-    void reserve_on(size_t need, cudaStream_t s)
+    void reserve_on(size_t need, cudaStream_t s, cudaMemPool_t pool)
     {
         if (need <= bytes)
             return;
         drop(s);
         size_t b = std::max<size_t>(need, 256);
-        TM_CUDA(cudaMallocAsync(&p, b, s));
+        TM_CUDA(cudaMallocFromPoolAsync(&p, b, pool, s));
         bytes = b;
         pooled = true;
     }
@@ -354,6 +354,9 @@ struct tm_ctx
     bool fft_ready = false;
     std::mutex fft_mu;
     double fft_ms = 1.4; // model: ms per template per 2^25 samples (B200; tm_autotune measures it)
+    // the context's own memory pool for per-batch buffers (DevBuf::reserve_on); it keeps
+    // up to 4 GiB of freed memory for the next batch
+    cudaMemPool_t pool = nullptr;
     std::string err;
     tmh::Lane main;                      // the synchronous calls' lane
     std::unique_ptr<tmh::Server> server; // serving engine, while started

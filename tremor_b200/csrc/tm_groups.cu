@@ -95,10 +95,10 @@ void prepare_group(tm_ctx *ctx, Lane &L, int m, const std::vector<int> &idx, con
         g.htp[t].m = m;
     }
     cudaStream_t s = L.stream;
-    g.q.reserve_on(sizeof(float) * static_cast<size_t>(T_pad) * m_pad, s);
-    g.order.reserve_on(sizeof(int) * static_cast<size_t>(T) * nblk, s);
-    g.tp.reserve_on(sizeof(TemplParam) * T_pad, s);
-    g.slots.reserve_on(sizeof(int) * std::max(g.nk, 1), s);
+    g.q.reserve_on(sizeof(float) * static_cast<size_t>(T_pad) * m_pad, s, ctx->pool);
+    g.order.reserve_on(sizeof(int) * static_cast<size_t>(T) * nblk, s, ctx->pool);
+    g.tp.reserve_on(sizeof(TemplParam) * T_pad, s, ctx->pool);
+    g.slots.reserve_on(sizeof(int) * std::max(g.nk, 1), s, ctx->pool);
     TM_CUDA(cudaMemcpyAsync(g.q.p, hq, sizeof(float) * static_cast<size_t>(T_pad) * m_pad, cudaMemcpyHostToDevice, s));
     TM_CUDA(cudaMemcpyAsync(g.order.p, ho, sizeof(int) * static_cast<size_t>(T) * nblk, cudaMemcpyHostToDevice, s));
     TM_CUDA(cudaMemcpyAsync(g.tp.p, g.htp.data(), sizeof(TemplParam) * T_pad, cudaMemcpyHostToDevice, s));
@@ -120,8 +120,8 @@ void prepare_group(tm_ctx *ctx, Lane &L, int m, const std::vector<int> &idx, con
                 hh[at] = bf16_bits(v);
                 hl[at] = bf16_bits(v - bf16_value(hh[at]));
             }
-        g.q_hi.reserve_on(sizeof(uint16_t) * elems, s);
-        g.q_lo.reserve_on(sizeof(uint16_t) * elems, s);
+        g.q_hi.reserve_on(sizeof(uint16_t) * elems, s, ctx->pool);
+        g.q_lo.reserve_on(sizeof(uint16_t) * elems, s, ctx->pool);
         TM_CUDA(cudaMemcpyAsync(g.q_hi.p, hh, sizeof(uint16_t) * elems, cudaMemcpyHostToDevice, s));
         TM_CUDA(cudaMemcpyAsync(g.q_lo.p, hl, sizeof(uint16_t) * elems, cudaMemcpyHostToDevice, s));
         h2d += 2 * sizeof(uint16_t) * static_cast<uint64_t>(T) * m;
@@ -246,13 +246,13 @@ void prepare_group_mixed(tm_ctx *ctx, Lane &L, const std::vector<int> &idx_in, c
     }
     g.tiles = tiles;
     cudaStream_t s = L.stream;
-    g.q.reserve_on(sizeof(float) * elems, s);
-    g.order.reserve_on(sizeof(int) * static_cast<size_t>(R) * nblk, s);
-    g.tp.reserve_on(sizeof(TemplParam) * R, s);
-    g.slots.reserve_on(sizeof(int) * std::max(g.nk, 1), s);
-    g.q_hi.reserve_on(sizeof(uint16_t) * elems, s);
-    g.q_lo.reserve_on(sizeof(uint16_t) * elems, s);
-    g.d_tiles.reserve_on(sizeof(tmb::TileInfo) * tiles.size(), s);
+    g.q.reserve_on(sizeof(float) * elems, s, ctx->pool);
+    g.order.reserve_on(sizeof(int) * static_cast<size_t>(R) * nblk, s, ctx->pool);
+    g.tp.reserve_on(sizeof(TemplParam) * R, s, ctx->pool);
+    g.slots.reserve_on(sizeof(int) * std::max(g.nk, 1), s, ctx->pool);
+    g.q_hi.reserve_on(sizeof(uint16_t) * elems, s, ctx->pool);
+    g.q_lo.reserve_on(sizeof(uint16_t) * elems, s, ctx->pool);
+    g.d_tiles.reserve_on(sizeof(tmb::TileInfo) * tiles.size(), s, ctx->pool);
     TM_CUDA(cudaMemcpyAsync(g.q.p, hq, sizeof(float) * elems, cudaMemcpyHostToDevice, s));
     TM_CUDA(cudaMemcpyAsync(g.order.p, ho, sizeof(int) * static_cast<size_t>(R) * nblk, cudaMemcpyHostToDevice, s));
     TM_CUDA(cudaMemcpyAsync(g.tp.p, g.htp.data(), sizeof(TemplParam) * R, cudaMemcpyHostToDevice, s));
