@@ -16,6 +16,11 @@ device pipeline, device->host answers). The waveform (1 GiB) is larger than L2, 
 no flush is needed between steps. With N GPUs every rank runs its own replica (the
 path needs no exchange); time is the max over ranks.
 
+After the timed legs, untimed: every answer of one step is recomputed in FP64
+(`fp64_error`: the error against FP64 stated per result, summarised), and the plain FP32
+kernel runs the same batches (`plain_fp32`, at most 3 steps); `vs_baseline` is value over
+that FP32 rate, the metric's own comparison.
+
 --impl reference: the reference's own CPU scan (SkipSequentialScan, sequential mode,
 built from the reference sources into oracle/_ref) on a bounded sample of the same
 workload (the first 2^24 samples, a few templates per step), all host threads.
@@ -598,6 +603,46 @@ def run_ours(args, w):
     log('[bench] e2e host phases per step (create, run, close) ms: ' +
         ', '.join(f'{1000 * p / args.steps:.1f}' for p in phases))
 
+    # the error of every answer of one step against FP64 (tm_result_fp64), untimed
+    ans = batches[0].run(fp64=True)
+    rel = np.concatenate([tb.Context.relative_error(d, f) for _, d, f in ans])
+    d64 = np.concatenate([f for _, _, f in ans])
+    fin = rel[np.isfinite(rel)]
+    fp64_error = {'answers': int(len(rel)), 'finite': int(len(fin)),
+                  'max_rel': float(fin.max()) if len(fin) else None,
+                  'median_rel': float(np.median(fin)) if len(fin) else None,
+                  'min_fp64_distance': float(d64[np.isfinite(d64)].min()) if np.isfinite(d64).any() else None,
+                  'within_1e-4': int((fin <= 1e-4).sum()),
+                  'what': 'every answer of one step (batch 0): |D - D64| / D64, D64 recomputed in FP64 '
+                          'from the raw samples (tm_result_fp64)'}
+
+    # the plain FP32 kernel on the same batches and windows: the metric's own comparison
+    plain = None
+    if kname == 'k_scan_umma' and args.kernel == 'auto' and not args.no_fp32:
+        ctx.set_kernel(tb.KERNEL_FP32)
+        fsteps = min(args.steps, 3)
+        fbatches = [ctx.batch(reqs[i * per:(i + 1) * per]) for i in range(min(nbatch, fsteps))]
+        fbatches[0].run()  # warm-up
+        ctx.profile_enable(True)
+        ctx.profile_read()
+        barrier()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        fpairs = 0
+        for s in range(fsteps):
+            fbatches[s % len(fbatches)].run()
+            fpairs += pair_count[s % len(fbatches)]
+        f1.record(stream)
+        barrier()
+        f_ms = f0.elapsed_time(f1)
+        fk, fl, fkms, fkflops, _ = ctx.profile_read()
+        ctx.profile_enable(False)
+        for b in fbatches:
+            b.close()
+        ctx.set_kernel(tb.KERNEL_AUTO)
+        plain = {'pairs': fpairs, 'ms': f_ms, 'kernel': fk, 'launches': fl, 'kernel_ms': fkms, 'flops': fkflops,
+                 'steps': fsteps}
+
     from tremor_b200.replicas import combine
     dev = f'cuda:{local}'
     total_pairs, ms = combine(pairs, ms, dist, dev)  # every replica's pairs, the slowest rank's time
@@ -605,6 +650,24 @@ def run_ours(args, w):
     _, k_avg_ms = combine(0.0, kms / max(launches, 1), dist, dev)
     value = total_pairs / (ms / 1e3) / 1e9
     e2e_value = total_pairs / (e_ms / 1e3) / 1e9
+
+    plain_line = None
+    if plain is not None:
+        fp_pairs, fp_ms = combine(plain['pairs'], plain['ms'], dist, dev)
+        _, fk_avg = combine(0.0, plain['kernel_ms'] / max(plain['launches'], 1), dist, dev)
+        plain_line = {'value': fp_pairs / (fp_ms / 1e3) / 1e9, 'unit': UNIT, 'steps': plain['steps'],
+                      'ms_per_step': fp_ms / plain['steps'], 'kernel': plain['kernel'],
+                      'kernel_ms_per_launch': fk_avg,
+                      'what': 'the plain FP32 kernel (TM_KERNEL_FP32) on the same batches, after the split-BF16 '
+                              'legs; CUDA events on the library stream'}
+        try:
+            fpk = tb.fp32_peak(local)
+            ach = plain['flops'] / max(plain['launches'], 1) / (fk_avg / 1e3) / 1e12
+            plain_line['roofline'] = {'bound': 'fp32', 'achieved': ach, 'peak': fpk, 'unit': 'TFLOP/s',
+                                      'frac': ach / fpk,
+                                      'peak_note': 'measured FP32 FMA rate (tm_fp32_peak)'}
+        except Exception as exc:  # informative
+            plain_line['roofline'] = {'error': str(exc)[:200]}
 
     if rank == 0:
         bf16_peak, _, peak_kind = peaks()
@@ -643,7 +706,13 @@ def run_ours(args, w):
                 cpu_info['mass_v3'] = {'error': str(exc)[:200]}
         line = {'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
                 'warmup': args.warmup, 'ms_per_step': ms / args.steps, 'higher_is_better': True, 'scaling': 'weak',
-                'vs_baseline': None, 'dtype': 'bf16x3+f32' if kname == 'k_scan_umma' else 'f32',
+                'vs_baseline': value / plain_line['value'] if plain_line else None,
+                'vs_baseline_note': 'value / plain_fp32.value: the metric is pairs/s against the plain FP32 '
+                                    'kernel, measured in this run (no published number exists)'
+                                    if plain_line else 'no FP32 leg in this run',
+                'plain_fp32': plain_line,
+                'fp64_error': fp64_error,
+                'dtype': 'bf16x3+f32' if kname == 'k_scan_umma' else 'f32',
                 'data': 'synthetic',
                 'config': {'workload': args.workload, 'n': w['n'], 'templates': w['q'], 'templates_per_step': per,
                            'm': w['m'], 'mode': w['mode'], 'k': w['k'], 'merge': w['merge'], 'corr': w['corr'],
@@ -677,6 +746,7 @@ def main():
     p.add_argument('--tiles', choices=['auto', 'rows', 'cols128', 'cols64', 'cols32'], default='auto',
                    help='tile shape of mixed-length groups (TILES_*)')
     p.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline leg')
+    p.add_argument('--no-fp32', action='store_true', help='skip the plain FP32 kernel leg')
     p.add_argument('--rate', type=float, default=0.0, help='serving: Poisson arrival rate (req/s)')
     p.add_argument('--requests', type=int, default=0, help='serving: requests in the timed stream')
     p.add_argument('--workers', type=int, default=1, help='serving: batches in flight at once')

@@ -163,13 +163,24 @@ int tm_batch_h2d_bytes(const tm_batch *batch, uint64_t *bytes);
 int tm_result_count(const tm_result *res, int request, uint64_t *count);
 int tm_result_get(const tm_result *res, int request, uint64_t *positions, float *distances, uint64_t capacity);
 void tm_result_free(tm_result *res);
+/* The error of each answer against FP64. For the answers of request `request` of res (a
+ * result of this context; the order of tm_result_get), writes min(count, capacity)
+ * doubles: the squared z-normalised distance of the same template and window recomputed
+ * entirely in FP64 from the raw samples (templ: the request's m template samples, raw or
+ * already z-normalised, z-normalised again here in FP64 by two passes; the window's
+ * two-pass FP64 mean and population std, missing samples counted as 0; an FP64 sum of
+ * squared differences). Answers of distance FLT_MAX (kNN padding, constant windows) get
+ * +inf. The relative error of answer i is |D_i - d64_i| / d64_i. No counterpart in the
+ * reference, whose validation compares correlations with an FP64 implementation within
+ * 2e-4 (experiments/validate_search.py:80-86, :127). */
+int tm_result_fp64(tm_ctx *ctx, const tm_result *res, int request, const float *templ, int m, double *d64,
+                   uint64_t capacity);
 
 /* ---- allocation-free statistics ------------------------------------------------------ */
 
 /* No counterpart in the reference: an entry point for callers that must not allocate
  * device memory (a live detector with a fixed latency budget, where cudaMalloc may
- * synchronise the device; a runtime whose pool allocator holds the free memory; work
- * recorded into a stream capture). It computes, on the calling thread's current device
+ * synchronise the device; a runtime whose pool allocator holds the free memory). It computes, on the calling thread's current device
  * and on `stream` (a cudaStream_t, 0 for the default stream), the statistics of every
  * window of length m of the device-resident waveform raw[0..n): mean, std and flags per
  * window into caller-owned device arrays of n - m + 1 elements, with the meaning of
@@ -178,7 +189,9 @@ void tm_result_free(tm_result *res);
  * nothing and does not synchronise: its only scratch is a fixed 8 MiB device array that
  * every GPU loading the library holds until the process exits, so n + m must not exceed
  * 524288 samples (larger inputs return TM_ERR_TOO_LARGE). The first call on a device
- * looks that array up on the device (make it before any stream capture). All calls share
+ * looks that array up on the device and keeps its address for the rest of the process
+ * (make that first call before any stream capture; after cudaDeviceReset on that device
+ * the kept address is stale, so do not call it again in that process). All calls share
  * the array: calls whose work overlaps on the GPU (other streams, other threads) race. */
 int tm_window_stats_noalloc(const float *raw, uint64_t n, int m, float *mean, float *stddev, uint8_t *flags,
                             void *stream);

@@ -8,6 +8,9 @@
 //       not reset between searches, SkipSequential.cpp:127-136).
 //   tmref_sss_stats                      : the per-window statistics that
 //       SkipSequentialScan::build computes (SkipSequential.cpp:157-190).
+//   tmref_sss_from_stats / tmref_sss_distances : the same class over a record in memory
+//       with given statistics (records too large for build()'s statistics in a test), and
+//       the reference's distance at given windows.
 //   tmref_l2_dist / tmref_znormalize / tmref_block_order / tmref_select_knn :
 //       the inline building blocks of ZnormSearch.hpp, for bit-level pinning.
 #include <cfloat>
@@ -116,6 +119,70 @@ extern "C"
     }
 
     void tmref_sss_destroy(void *handle) { delete static_cast<SkipSequentialScan *>(handle); }
+
+    // A sequential-mode scan (no lower bounds) over a record held in memory, with the
+    // per-window statistics given instead of computed by build(): the members build() sets
+    // for one rank (SkipSequential.cpp:138-163: window, first and count of the owned
+    // subsequences, raw samples, means, stds) are assigned directly. For records of
+    // 2^26-2^28 samples, where build()'s two-pass statistics (one dependent chain of m
+    // FP64 additions per window) take minutes; the statistics given are the oracle's
+    // restatement of them, pinned bit for bit to build()'s by the tests. The searches are
+    // then the reference's own (search_knn / search_threshold via tmref_sss_search).
+    void *tmref_sss_from_stats(const float *raw, uint64_t n, int m, const float *means, const float *stds,
+                               int merge_offset, int threads)
+    {
+        try
+        {
+            const uint64_t W = n - static_cast<uint64_t>(m) + 1;
+            auto *scan = new SkipSequentialScan(threads, 8, merge_offset, 0, false);
+            scan->window = m;
+            scan->first_subsequence = 0;
+            scan->subsequences = static_cast<idx_t>(W);
+            scan->raw.assign(raw, raw + n);
+            scan->means.assign(means, means + W);
+            scan->stds.assign(stds, stds + W);
+            return scan;
+        }
+        catch (const std::exception &)
+        {
+            return nullptr;
+        }
+    }
+
+    // The reference's FP32 distance (l2_dist_znorm_subsequence, no abandoning) of one raw
+    // template against the windows at `positions`, with the scan's statistics and its own
+    // template preparation (prepare_query: znormalize_inplace, query_block_order); -1 for a
+    // window whose first sample is missing (not searched).
+    int tmref_sss_distances(void *handle, const float *query_raw, const uint64_t *positions, uint64_t count,
+                            float *out)
+    {
+        auto *scan = static_cast<SkipSequentialScan *>(handle);
+        try
+        {
+            std::vector<ts_type> znorm, paa;
+            std::vector<int> order;
+            scan->prepare_query(query_raw, znorm, paa, order);
+            for (uint64_t i = 0; i < count; i++)
+            {
+                const uint64_t id = positions[i] - static_cast<uint64_t>(scan->first_subsequence);
+                if (id >= static_cast<uint64_t>(scan->subsequences))
+                    return -1;
+                if (scan->raw[id] == TREMOR_MISSING_VALUE)
+                {
+                    out[i] = -1.0f;
+                    continue;
+                }
+                int blocks = 0;
+                out[i] = l2_dist_znorm_subsequence(znorm.data(), scan->raw.data(), id, scan->window, scan->means[id],
+                                                   scan->stds[id], FLT_MAX, order.data(), &blocks);
+            }
+            return 0;
+        }
+        catch (const std::exception &)
+        {
+            return -1;
+        }
+    }
 
     float tmref_l2_dist(const float *query_znorm, const float *raw, uint64_t start, int m, float mean, float stddev,
                         float bound, const int *block_order, int *blocks_visited)

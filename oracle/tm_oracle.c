@@ -104,6 +104,125 @@ void tmo_window_stats(const float *raw, uint64_t windows, int m, float *mean_out
     }
 }
 
+/* tmo_window_stats for records of any size: the same per-window operations in the same
+ * order (SkipSequential.cpp:157-190: a sequential FP64 sum, the mean, a sequential FP64 sum
+ * of fused squares), for 32 consecutive windows at once. Sample t (relative to the block's
+ * first window) is the (t - j)-th term of window j, so walking the samples in order and
+ * adding each one to every window that contains it gives every window its terms in the
+ * reference's order; in the middle of the walk all 32 windows take the same sample, a
+ * broadcast that vectorises (AVX2 + FMA, which every host of the reference build has).
+ * The results are those of tmo_window_stats bit for bit (checked by tests/test_oracle.py).
+ * The reference's build() runs one window per thread, a dependent chain of m additions;
+ * at 2^28 samples and m = 4096 this form takes seconds where that takes minutes. */
+#define TMO_STATS_BLOCK 32
+
+typedef double tmo_v4d __attribute__((vector_size(32))); /* 4 windows' sums, one AVX2 register */
+
+__attribute__((target("avx2,fma"))) static void stats_block(const float *w, int m, double *mean, double *sd)
+{
+    double sum[TMO_STATS_BLOCK] = {0}, sq[TMO_STATS_BLOCK] = {0};
+    const int B = TMO_STATS_BLOCK, last = m + B - 1; /* samples t in [0, last) */
+    /* ramp-in (t < B - 1): windows 0..t; the full middle: all B windows (eight registers);
+     * ramp-out (t >= m): windows t - m + 1..B - 1 */
+    const int mid_lo = B - 1, mid_hi = m; /* t in [mid_lo, mid_hi) takes every window */
+    for (int t = 0; t < (mid_lo < last ? mid_lo : last); t++)
+    {
+        const double v = clean64(w[t]);
+        for (int j = (t - m + 1 > 0 ? t - m + 1 : 0); j <= t; j++)
+            sum[j] += v;
+    }
+    if (mid_lo < mid_hi)
+    {
+        tmo_v4d s[8];
+        memcpy(s, sum, sizeof(s));
+        for (int t = mid_lo; t < mid_hi; t++)
+        {
+            const double v = clean64(w[t]);
+            const tmo_v4d vv = {v, v, v, v};
+#pragma GCC unroll 8
+            for (int r = 0; r < 8; r++)
+                s[r] += vv;
+        }
+        memcpy(sum, s, sizeof(s));
+    }
+    for (int t = (mid_hi > mid_lo ? mid_hi : mid_lo); t < last; t++)
+    {
+        const double v = clean64(w[t]);
+        const int jlo = t - m + 1 > 0 ? t - m + 1 : 0, jhi = t < B - 1 ? t : B - 1;
+        for (int j = jlo; j <= jhi; j++)
+            sum[j] += v;
+    }
+    for (int j = 0; j < B; j++)
+        mean[j] = sum[j] / m;
+    for (int t = 0; t < (mid_lo < last ? mid_lo : last); t++)
+    {
+        const double v = clean64(w[t]);
+        for (int j = (t - m + 1 > 0 ? t - m + 1 : 0); j <= t; j++)
+        {
+            const double d = v - mean[j];
+            sq[j] = fma(d, d, sq[j]);
+        }
+    }
+    if (mid_lo < mid_hi)
+    {
+        tmo_v4d q[8], mu[8];
+        memcpy(q, sq, sizeof(q));
+        memcpy(mu, mean, sizeof(mu));
+        for (int t = mid_lo; t < mid_hi; t++)
+        {
+            const double v = clean64(w[t]);
+            const tmo_v4d vv = {v, v, v, v};
+#pragma GCC unroll 8
+            for (int r = 0; r < 8; r++)
+            {
+                const tmo_v4d d = vv - mu[r];
+                q[r] = __builtin_ia32_vfmaddpd256(d, d, q[r]); /* fused, as fma() */
+            }
+        }
+        memcpy(sq, q, sizeof(q));
+    }
+    for (int t = (mid_hi > mid_lo ? mid_hi : mid_lo); t < last; t++)
+    {
+        const double v = clean64(w[t]);
+        const int jlo = t - m + 1 > 0 ? t - m + 1 : 0, jhi = t < B - 1 ? t : B - 1;
+        for (int j = jlo; j <= jhi; j++)
+        {
+            const double d = v - mean[j];
+            sq[j] = fma(d, d, sq[j]);
+        }
+    }
+    for (int j = 0; j < B; j++)
+        sd[j] = sqrt(sq[j] / m);
+}
+
+void tmo_window_stats_fast(const float *raw, uint64_t windows, int m, float *mean_out, float *std_out)
+{
+    const long long blocks = (long long)(windows / TMO_STATS_BLOCK);
+#pragma omp parallel for schedule(dynamic, 64)
+    for (long long b = 0; b < blocks; b++)
+    {
+        const uint64_t id0 = (uint64_t)b * TMO_STATS_BLOCK;
+        const float *w = raw + id0;
+        double mean[TMO_STATS_BLOCK], sd[TMO_STATS_BLOCK];
+        stats_block(w, m, mean, sd);
+        for (int j = 0; j < TMO_STATS_BLOCK; j++)
+        {
+            const uint64_t id = id0 + (uint64_t)j;
+            if (w[j] == TMO_MISSING_VALUE)
+            {
+                mean_out[id] = 0.0f;
+                std_out[id] = 0.0f;
+                continue;
+            }
+            mean_out[id] = (float)mean[j];
+            std_out[id] = (float)(sd[j] <= 1e-12 ? 0.0 : sd[j]);
+        }
+    }
+    const uint64_t done = (uint64_t)blocks * TMO_STATS_BLOCK;
+    if (done < windows)
+        tmo_window_stats(raw + done, windows - done, m, mean_out + done, std_out + done);
+}
+
 /* hsum256 (ZnormSearch.hpp:92-97) of the lane-wise sum acc0 + acc1. */
 static inline float hsum16(const float *acc0, const float *acc1)
 {

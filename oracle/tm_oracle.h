@@ -41,6 +41,9 @@ void tmo_block_order(const float *query_znorm, int m, int *order);
  * population std of every window, stored as float; missing samples count as 0;
  * std <= 1e-12 -> 0; a window whose first sample is missing gets (0, 0). */
 void tmo_window_stats(const float *raw, uint64_t windows, int m, float *mean, float *stddev);
+/* The same statistics, bit for bit, 16 windows per vectorised pass (AVX2 + FMA hosts):
+ * for records of 2^26-2^28 samples. */
+void tmo_window_stats_fast(const float *raw, uint64_t windows, int m, float *mean, float *stddev);
 
 /* ZnormSearch.hpp:103-165: z-normalised squared ED with block early abandoning. */
 float tmo_l2_dist(const float *query_znorm, const float *raw, uint64_t start, int m, float mean, float stddev,

@@ -1,7 +1,7 @@
 """Generates the golden fixtures of tests/golden/ from the reference's OWN scan code.
 
-Run in a container where the reference sources are mounted (REF, default
-/root/reference):  python tests/golden/make_golden.py
+Run where the reference sources are mounted (REF; default: the `reference` checkout
+beside this repository):  python tests/golden/make_golden.py
 
 It builds oracle/_ref/libtremor_ref.so (the reference's SkipSequentialScan with a
 single-rank MPI stand-in, see oracle/Makefile), runs it on seeded inputs and
@@ -83,7 +83,7 @@ def read_csv(path):
 
 
 def main():
-    ref = os.environ.get('REF', '/root/reference')
+    ref = os.environ.get('REF', str(ROOT.parent / 'reference'))
     subprocess.run(['make', '-C', str(ROOT / 'oracle'), 'ref', f'REF={ref}'], check=True)
     lib = ctypes.CDLL(str(ROOT / 'oracle' / '_ref' / 'libtremor_ref.so'))
     P = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731

@@ -148,3 +148,54 @@ def test_mass_v3_restatement_matches_fp64_oracle():
         assert np.allclose(d[ok], expect, rtol=1e-9, atol=1e-7 * m)
         order = sorted(range(len(d)), key=lambda p: (d[p], p))[:k]
         assert order == np.argsort(-corr[qi], kind='stable')[:k].tolist()
+
+
+@pytest.mark.skipif(ref is None, reason='reference build (oracle/_ref) not present')
+def test_fast_window_stats_bit_identical_to_reference_build():
+    """tmo_window_stats_fast (the statistics of the full-size parity checks) equals, bit for
+    bit, what the reference's SkipSequentialScan::build computes (SkipSequential.cpp:157-190),
+    with missing samples, constant stretches and loud stretches in the record."""
+    rng = np.random.default_rng(23)
+    n = 1 << 18
+    x = (rng.normal(size=n) * 3.0 + 7.0).astype(np.float32)
+    x[1000:1040] = np.float32(-100000.0)
+    x[5000:9000] = 2.5
+    x[20000:20500] *= np.float32(1e5)
+    x[70001] = np.float32(-100000.0)
+    with tempfile.TemporaryDirectory() as tmp:
+        wf = os.path.join(tmp, 'w.bin')
+        x.tofile(wf)
+        for m in (16, 100, 256, 1000, 4096):
+            W = n - m + 1
+            rm = np.zeros(W, np.float32)
+            rs = np.zeros(W, np.float32)
+            assert ref.tmref_sss_stats(wf.encode(), n, m, 4, ob.P(rm), ob.P(rs)) == 0
+            fm, fs = ob.window_stats_fast(x, m)
+            assert np.array_equal(rm.view(np.uint32), fm.view(np.uint32)), m
+            assert np.array_equal(rs.view(np.uint32), fs.view(np.uint32)), m
+
+
+@pytest.mark.skipif(ref is None, reason='reference build (oracle/_ref) not present')
+@pytest.mark.parametrize('name', ['validate', 'chirp'])
+def test_reference_scan_from_stats_equals_golden(name):
+    """The reference's own scan over a record in memory with the oracle's statistics
+    (ReferenceScan, the full-size parity checks' reference) prints exactly the golden
+    rows that the reference's build() + search produced."""
+    meta, x, q = ob.load_golden(name)
+    m = meta['m']
+    for merge in meta['merges']:
+        with ob.ReferenceScan(x, m, merge_offset=merge, threads=4) as rs:
+            knn = rs.knn(q, meta['k'])
+            rows = [[str(i), str(j + 1), str(int(p)), c] for i, (pos, cc) in enumerate(knn)
+                    for j, (p, c) in enumerate(zip(pos, cc))]
+            assert rows == meta['knn'][str(merge)], (name, merge)
+            thr = rs.threshold(q, meta['threshold'])
+            rows = [[str(i), str(c), str(int(p)), cc] for i, (pos, ccs) in enumerate(thr)
+                    for c, (p, cc) in enumerate(zip(pos, ccs))]
+            assert rows == meta['threshold_hits'][str(merge)], (name, merge)
+            # the reference's distance bits at its own answers equal the oracle's
+            Io, Do = ob.scan_knn(x, q, m, meta['k'], merge)
+            for i in range(len(q)):
+                ok = Do[i] < ob.FLT_MAX
+                d = rs.distances(q[i], Io[i][ok])
+                assert np.array_equal(d.view(np.uint32), Do[i][ok].view(np.uint32)), (name, merge, i)

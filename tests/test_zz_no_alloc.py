@@ -2,7 +2,7 @@
 
 It serves callers that must not allocate device memory: a live detector with a fixed
 latency budget (cudaMalloc may synchronise the device), a runtime whose pool allocator
-holds the free memory, work recorded into a stream capture. They own the input and
+holds the free memory. They own the input and
 output device buffers (here: torch tensors made by the test, not by the call).
 
 Checked through the C ABI: two calls in a row (two template lengths, the second reusing

@@ -86,6 +86,7 @@ def load_library():
         'tm_result_count': (i, [_vp, i, ctypes.POINTER(u64)]),
         'tm_result_get': (i, [_vp, i, _vp, _vp, u64]),
         'tm_result_free': (None, [_vp]),
+        'tm_result_fp64': (i, [_vp, _vp, i, _vp, i, _vp, u64]),
         'tm_cc_to_ed': (f, [f, i]),
         'tm_ed_to_cc': (f, [f, i]),
         'tm_profile_enable': (i, [_vp, i]),
@@ -167,6 +168,15 @@ class Context:
         if rc != 0:
             raise TremorError(rc, self._lib.tm_last_error(self._h).decode())
 
+    @staticmethod
+    def relative_error(dist: np.ndarray, fp64: np.ndarray) -> np.ndarray:
+        """|D - D64| / D64 per answer (NaN for padding and constant windows, whose FP64
+        distance is +inf)."""
+        d = np.asarray(dist, np.float64)
+        f = np.asarray(fp64, np.float64)
+        with np.errstate(divide='ignore', invalid='ignore'):
+            return np.where(np.isfinite(f), np.abs(d - f) / f, np.nan)
+
     def set_kernel(self, kernel: int):
         self._check(self._lib.tm_set_kernel(self._h, kernel))
 
@@ -228,12 +238,15 @@ class Context:
                               r.flags)
         return arr
 
-    def scan_batch(self, requests: Sequence[Request]):
-        """Answers (positions, distances) per request, any mix of modes and lengths."""
+    def scan_batch(self, requests: Sequence[Request], fp64: bool = False):
+        """Answers (positions, distances) per request, any mix of modes and lengths. With
+        fp64=True each request's answers are (positions, distances, fp64_distances): every
+        answer's distance recomputed entirely in FP64 (tm_result_fp64), so its error
+        against FP64 is stated per result."""
         arr = self._requests(requests)
         res = _vp()
         self._check(self._lib.tm_scan_batch(self._h, arr, len(requests), ctypes.byref(res)))
-        return self._take(res, len(requests))
+        return self._take(res, len(requests), requests if fp64 else None)
 
     def serve(self, workers: int = 1, max_batch: int = 256, memory_budget: int = 0) -> 'Server':
         """Starts continuous batching over this context's waveform (tm_serve_start)."""
@@ -272,7 +285,10 @@ class Context:
         self._check(self._lib.tm_d2h_bytes(self._h, ctypes.byref(n)))
         return n.value
 
-    def _take(self, res, count) -> List[Tuple[np.ndarray, np.ndarray]]:
+    def _take(self, res, count, fp64_requests=None) -> List[Tuple[np.ndarray, ...]]:
+        """Copies the answers out of a tm_result and frees it. With fp64_requests (the
+        requests of the result, in order), each entry also carries the FP64 distances of its
+        answers (tm_result_fp64)."""
         out = []
         try:
             for i in range(count):
@@ -281,7 +297,13 @@ class Context:
                 pos = np.zeros(n.value, np.uint64)
                 dist = np.zeros(n.value, np.float32)
                 self._check(self._lib.tm_result_get(res, i, _ptr(pos), _ptr(dist), n.value))
-                out.append((pos, dist))
+                if fp64_requests is None:
+                    out.append((pos, dist))
+                    continue
+                t = fp64_requests[i].template
+                d64 = np.zeros(n.value, np.float64)
+                self._check(self._lib.tm_result_fp64(self._h, res, i, _ptr(t), len(t), _ptr(d64), n.value))
+                out.append((pos, dist, d64))
         finally:
             self._lib.tm_result_free(res)
         return out
@@ -338,10 +360,12 @@ class Batch:
         ctx._check(ctx._lib.tm_batch_create(ctx._h, arr, len(requests), ctypes.byref(h)))
         self._h = h
 
-    def run(self):
+    def run(self, fp64: bool = False):
+        """Answers per request; with fp64=True also each answer's FP64 distance (as
+        Context.scan_batch)."""
         res = _vp()
         self.ctx._check(self.ctx._lib.tm_batch_run(self.ctx._h, self._h, ctypes.byref(res)))
-        return self.ctx._take(res, self.count)
+        return self.ctx._take(res, self.count, self._keep if fp64 else None)
 
     def h2d_bytes(self) -> int:
         n = ctypes.c_uint64(0)

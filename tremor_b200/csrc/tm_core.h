@@ -130,6 +130,8 @@ struct DevBuf
     template <class T> T *as() const { return static_cast<T *>(p); }
     // Callers release only after the work that used the buffer has completed.
     void release() { drop(0); }
+    // Stream-ordered release of a pooled buffer: after the work already queued on s.
+    void release_on(cudaStream_t s) { drop(s); }
 
   private:
     void drop(cudaStream_t s)
@@ -359,7 +361,10 @@ struct tm_ctx
     cudaMemPool_t pool = nullptr;
     std::string err;
     tmh::Lane main;                      // the synchronous calls' lane
-    std::unique_ptr<tmh::Server> server; // serving engine, while started
+    // serving engine, while started; replaced only under server_mu, and the serving calls
+    // take their own reference under it, so a restart cannot free a server in use
+    std::shared_ptr<tmh::Server> server;
+    std::mutex server_mu;
 
     tm_ctx();  // both in tm_serve.cu, where the server's type is complete
     ~tm_ctx();
@@ -471,6 +476,6 @@ void create_batch(tm_ctx *ctx, Lane &L, const tm_request *requests, int count, t
 
 // tm_serve.cu
 void stop_server(tm_ctx *ctx);
-bool serving(const tm_ctx *ctx);
+bool serving(tm_ctx *ctx);
 
 } // namespace tmh

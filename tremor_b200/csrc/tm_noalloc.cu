@@ -6,8 +6,7 @@
 // afford cudaMalloc/cudaFree, which may synchronise the whole device and take
 // unbounded time; a host runtime that hands all free device memory to its own pool
 // allocator (PyTorch's caching allocator, for one) leaves nothing for an outside
-// cudaMalloc; and work recorded into a CUDA stream capture cannot allocate. Such a
-// caller owns its input and output buffers and passes them in.
+// cudaMalloc. Such a caller owns its input and output buffers and passes them in.
 //
 // What it computes: for every window j of length m of raw[0..n), the statistics the
 // reference keeps (SkipSequential.cpp:157-190): float mean and population std, (0, 0)
@@ -143,7 +142,8 @@ __global__ void k_stats_from_suffix(const float *__restrict__ raw, const double2
 }
 
 // Device address of g_suffix on each device, resolved once per device (with that device
-// current) by the first call on it.
+// current) by the first call on it and kept until the process exits: a cudaDeviceReset
+// unloads the module, after which the kept address is stale.
 constexpr int kMaxDevices = 64;
 std::mutex g_mutex;
 double2 *g_addr[kMaxDevices] = {};

@@ -204,14 +204,24 @@ static void serve_worker(Server *sv, Lane *L)
     }
 }
 
-// Completes what was submitted, then joins the workers; completions stay pollable.
+// The context's current server (or null), by a reference taken under the context's lock.
+static std::shared_ptr<Server> current_server(tm_ctx *ctx)
+{
+    std::lock_guard<std::mutex> lk(ctx->server_mu);
+    return ctx->server;
+}
+
+// Completes what was submitted, then joins the workers; completions stay pollable, and a
+// consumer waiting in tm_poll without a limit is woken once nothing is left to complete.
 void stop_server(tm_ctx *ctx)
 {
-    Server *sv = ctx->server.get();
-    if (sv == nullptr || sv->stopped)
+    std::shared_ptr<Server> sv = current_server(ctx);
+    if (!sv)
         return;
     {
         std::lock_guard<std::mutex> lk(sv->mu);
+        if (sv->stopping)
+            return; // stopped, or being stopped by another thread
         sv->stopping = true;
     }
     sv->work_cv.notify_all();
@@ -221,11 +231,22 @@ void stop_server(tm_ctx *ctx)
     for (auto &L : sv->lanes)
         L->close();
     sv->lanes.clear();
-    sv->stopped = true;
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        sv->stopped = true;
+    }
+    sv->done_cv.notify_all();
 }
 
 
-bool serving(const tm_ctx *ctx) { return ctx->server && !ctx->server->stopped; }
+bool serving(tm_ctx *ctx)
+{
+    std::shared_ptr<Server> sv = current_server(ctx);
+    if (!sv)
+        return false;
+    std::lock_guard<std::mutex> lk(sv->mu);
+    return !sv->stopped;
+}
 
 } // namespace tmh
 
@@ -237,7 +258,7 @@ int tm_serve_start(tm_ctx *ctx, const tm_serve_config *config)
 {
     if (ctx == nullptr)
         return TM_ERR_ARGUMENT;
-    if (ctx->server && !ctx->server->stopped)
+    if (serving(ctx))
         return TM_ERR_STATE;
     tm_serve_config cfg{1, 256, 0};
     if (config)
@@ -255,8 +276,7 @@ int tm_serve_start(tm_ctx *ctx, const tm_serve_config *config)
             TM_CUDA(cudaMemGetInfo(&free_b, &total_b));
             cfg.memory_budget = free_b / 4;
         }
-        ctx->server.reset();
-        auto sv = std::make_unique<Server>();
+        auto sv = std::make_shared<Server>();
         sv->ctx = ctx;
         sv->cfg = cfg;
         for (int i = 0; i < cfg.workers; i++)
@@ -265,7 +285,11 @@ int tm_serve_start(tm_ctx *ctx, const tm_serve_config *config)
             sv->lanes.back()->open();
         }
         Server *p = sv.get();
-        ctx->server = std::move(sv);
+        {
+            // the previous (stopped) server is freed once no serving call holds it
+            std::lock_guard<std::mutex> lk(ctx->server_mu);
+            ctx->server = std::move(sv);
+        }
         for (int i = 0; i < cfg.workers; i++)
             p->threads.emplace_back(serve_worker, p, p->lanes[i].get());
     });
@@ -275,8 +299,8 @@ int tm_submit(tm_ctx *ctx, const tm_request *request, uint64_t *ticket)
 {
     if (ctx == nullptr || request == nullptr || ticket == nullptr)
         return TM_ERR_ARGUMENT;
-    Server *sv = ctx->server.get();
-    if (sv == nullptr || sv->stopped)
+    std::shared_ptr<Server> sv = current_server(ctx);
+    if (!sv)
         return TM_ERR_STATE;
     const int rc = validate_requests(ctx, request, 1);
     if (rc != TM_OK)
@@ -312,13 +336,14 @@ int tm_poll(tm_ctx *ctx, tm_completion *out, int capacity, int timeout_ms, int *
     if (ctx == nullptr || count == nullptr || capacity < 0 || (capacity > 0 && out == nullptr))
         return TM_ERR_ARGUMENT;
     *count = 0;
-    Server *sv = ctx->server.get();
-    if (sv == nullptr)
+    std::shared_ptr<Server> sv = current_server(ctx);
+    if (!sv)
         return TM_ERR_STATE;
     std::unique_lock<std::mutex> lk(sv->mu);
     if (sv->done.empty() && timeout_ms != 0)
     {
-        auto ready = [&] { return !sv->done.empty(); };
+        // a stopped server completes nothing more: return instead of waiting for good
+        auto ready = [&] { return !sv->done.empty() || sv->stopped; };
         if (timeout_ms < 0)
             sv->done_cv.wait(lk, ready);
         else
@@ -338,7 +363,7 @@ int tm_serve_stop(tm_ctx *ctx)
 {
     if (ctx == nullptr)
         return TM_ERR_ARGUMENT;
-    if (!ctx->server)
+    if (!current_server(ctx))
         return TM_ERR_STATE;
     stop_server(ctx);
     return TM_OK;
@@ -349,8 +374,8 @@ int tm_serve_status(tm_ctx *ctx, uint64_t *pending, uint64_t *in_flight, uint64_
 {
     if (ctx == nullptr)
         return TM_ERR_ARGUMENT;
-    Server *sv = ctx->server.get();
-    if (sv == nullptr)
+    std::shared_ptr<Server> sv = current_server(ctx);
+    if (!sv)
         return TM_ERR_STATE;
     std::lock_guard<std::mutex> lk(sv->mu);
     if (pending)
