@@ -1,7 +1,7 @@
 """Benchmark of the exact template-matching scan on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload precision|plain_knn|threshold] [--kernel auto|fp32|bf16]
+                    [--workload precision|plain_knn|threshold|...] [--kernel auto|fp32|bf16]
 
 Workload (default "precision"): a seeded synthetic waveform of 2^28 float32 samples
 (AR(2) noise x slow envelope, 2000 injected chirp events), 1024 chirp templates of
@@ -48,8 +48,9 @@ UNIT = 'G pairs/s'
 
 WORKLOADS = {
     # precision = config 3, plain_knn = config 1, threshold = config 2
+    # config 3 names the contraction: split-BF16 tensor cores (the default kernel here)
     'precision': dict(n=1 << 28, q=1024, m=4096, events=2000, mode='knn', k=100, merge=0, corr=0.0,
-                      per_step=128, seed=2028),
+                      per_step=128, seed=2028, kernel='bf16'),
     'plain_knn': dict(n=1 << 22, q=16, m=1024, events=50, mode='knn', k=10, merge=512, corr=0.0,
                       per_step=16, seed=2026),
     # the precision workload's kernel on 2^25 samples (> L2) and 64 templates: ncu captures
@@ -67,6 +68,9 @@ WORKLOADS = {
     # few long templates (the FFT branch's case): 2^28 samples, 8 chirps of 16384, kNN k=10
     'long_templates': dict(n=1 << 28, q=8, m=16384, events=200, mode='knn', k=10, merge=8192, corr=0.0,
                            per_step=8, seed=2031),
+    # the fused in-tree FFT branch (templates up to 8192): 2^28 samples, 8 chirps of 8192
+    'fft_templates': dict(n=1 << 28, q=8, m=8192, events=200, mode='knn', k=10, merge=4096, corr=0.0,
+                          per_step=8, seed=2032),
     # config 5: 2^29 samples resident with their prefix sums; a Poisson stream of requests
     # (lengths log-uniform in [128, 16384], 50/50 kNN / threshold as in config 4) served
     # with continuous batching; one step = one request
@@ -521,6 +525,8 @@ def run_ours(args, w):
     rank, world, local, dist = dist_setup(args.gpus)
     torch.cuda.set_device(local)
     x, q = make_workload(w)
+    if args.kernel is None:
+        args.kernel = w.get('kernel', 'auto')
     kernel = {'auto': tb.KERNEL_AUTO, 'fp32': tb.KERNEL_FP32, 'bf16': tb.KERNEL_SPLIT_BF16}[args.kernel]
     ctx = tb.Context(x, device=local)
     ctx.set_kernel(kernel)
@@ -618,7 +624,7 @@ def run_ours(args, w):
 
     # the plain FP32 kernel on the same batches and windows: the metric's own comparison
     plain = None
-    if kname == 'k_scan_umma' and args.kernel == 'auto' and not args.no_fp32:
+    if kname == 'k_scan_umma' and not args.no_fp32:
         ctx.set_kernel(tb.KERNEL_FP32)
         fsteps = min(args.steps, 3)
         fbatches = [ctx.batch(reqs[i * per:(i + 1) * per]) for i in range(min(nbatch, fsteps))]
@@ -639,7 +645,7 @@ def run_ours(args, w):
         ctx.profile_enable(False)
         for b in fbatches:
             b.close()
-        ctx.set_kernel(tb.KERNEL_AUTO)
+        ctx.set_kernel(kernel)
         plain = {'pairs': fpairs, 'ms': f_ms, 'kernel': fk, 'launches': fl, 'kernel_ms': fkms, 'flops': fkflops,
                  'steps': fsteps}
 
@@ -742,7 +748,8 @@ def main():
     p.add_argument('--warmup', type=int, default=3)
     p.add_argument('--impl', choices=['ours', 'reference'], default='ours')
     p.add_argument('--workload', choices=sorted(WORKLOADS), default='precision')
-    p.add_argument('--kernel', choices=['auto', 'fp32', 'bf16'], default='auto')
+    p.add_argument('--kernel', choices=['auto', 'fp32', 'bf16'], default=None,
+                   help='contraction kernel (default: the workload\'s, else auto)')
     p.add_argument('--tiles', choices=['auto', 'rows', 'cols128', 'cols64', 'cols32'], default='auto',
                    help='tile shape of mixed-length groups (TILES_*)')
     p.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline leg')

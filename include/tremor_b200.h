@@ -115,10 +115,11 @@ int tm_set_tiles(tm_ctx *ctx, int tiles);
 /* Tiling model of the planner behind TM_TILES_AUTO: kernel milliseconds of 128 templates x
  * 2^25 windows, [group kind: one length, several][shape: rows, columns 128, 64, 32]
  * [K: 256, 1024, 4096, 16384], 32 doubles in that order, then the FFT branch's
- * milliseconds per template per 2^25 samples. tm_autotune measures it on this device (a
- * few seconds, its own synthetic record), stores it in the context and copies it to ms (up
- * to capacity values); returns 33 or an error. tm_set_tile_model installs a saved one
- * (count 33, or 32 to keep the FFT figure). No counterpart in the reference. */
+ * milliseconds per template per 2^25 samples for templates of up to 8192 samples and for
+ * longer ones. tm_autotune measures it on this device (a few seconds, its own synthetic
+ * record), stores it in the context and copies it to ms (up to capacity values); returns 34
+ * or an error. tm_set_tile_model installs a saved one (count 34; 33 keeps the long-template
+ * FFT figure, 32 both). No counterpart in the reference. */
 int tm_autotune(tm_ctx *ctx, double *ms, int capacity);
 int tm_set_tile_model(tm_ctx *ctx, const double *ms, int count);
 /* Restricts searches to windows [first, first + count) (a data partition as in

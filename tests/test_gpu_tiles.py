@@ -12,13 +12,13 @@ pytestmark = pytest.mark.gpu
 def test_autotune_model():
     x = _waveform(1 << 16, 31)
     with tb.Context(x) as ctx:
-        table, fft_ms = ctx.autotune()
+        table, fft_ms, fft_long_ms = ctx.autotune()
         assert table.shape == (2, 4, 4) and np.all(np.isfinite(table)) and np.all(table > 0)
-        assert np.isfinite(fft_ms) and fft_ms > 0
+        assert np.isfinite(fft_ms) and fft_ms > 0 and np.isfinite(fft_long_ms) and fft_long_ms > 0
         # more samples per window cost more on every shape; long templates favour wide tiles
         assert np.all(np.diff(table[:, :, 1:], axis=2) > 0)
         assert np.all(table[:, 0, 3] < table[:, 3, 3])
-        ctx.set_tile_model(table, fft_ms)
+        ctx.set_tile_model(table, fft_ms, fft_long_ms)
         with pytest.raises(tb.TremorError):
             ctx.set_tile_model(np.zeros(32))
 

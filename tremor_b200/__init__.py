@@ -185,19 +185,22 @@ class Context:
         self._check(self._lib.tm_set_tiles(self._h, tiles))
 
     def autotune(self):
-        """Measures the planner's model on this device (tm_autotune): (table, fft_ms). table:
-        milliseconds of 128 templates x 2^25 windows, shape [kind (one length, several),
-        tile shape (rows, columns 128 / 64 / 32), K (256, 1024, 4096, 16384)]; fft_ms: the FFT
-        branch's milliseconds per template per 2^25 samples."""
-        out = np.zeros(33, np.float64)
-        rc = self._lib.tm_autotune(self._h, out.ctypes.data, 33)
+        """Measures the planner's model on this device (tm_autotune): (table, fft_ms,
+        fft_long_ms). table: milliseconds of 128 templates x 2^25 windows, shape [kind (one
+        length, several), tile shape (rows, columns 128 / 64 / 32), K (256, 1024, 4096,
+        16384)]; fft_ms, fft_long_ms: the FFT branch's milliseconds per template per 2^25
+        samples for templates of up to 8192 samples and for longer ones."""
+        out = np.zeros(34, np.float64)
+        rc = self._lib.tm_autotune(self._h, out.ctypes.data, 34)
         self._check(min(rc, 0))
-        return out[:32].reshape(2, 4, 4), float(out[32])
+        return out[:32].reshape(2, 4, 4), float(out[32]), float(out[33])
 
-    def set_tile_model(self, ms: np.ndarray, fft_ms: float = None):
+    def set_tile_model(self, ms: np.ndarray, fft_ms: float = None, fft_long_ms: float = None):
         arr = np.ascontiguousarray(ms, dtype=np.float64).reshape(-1)
         if fft_ms is not None:
             arr = np.concatenate([arr, [float(fft_ms)]])
+            if fft_long_ms is not None:
+                arr = np.concatenate([arr, [float(fft_long_ms)]])
         self._check(self._lib.tm_set_tile_model(self._h, arr.ctypes.data, len(arr)))
 
     def set_window_range(self, first: int, count: int):

@@ -27,17 +27,19 @@ def main():
     p.add_argument('--device', type=int, default=0)
     args = p.parse_args()
     with tb.Context(np.random.default_rng(0).normal(size=1 << 16).astype(np.float32), device=args.device) as ctx:
-        table, fft_ms = ctx.autotune()
+        table, fft_ms, fft_long_ms = ctx.autotune()
     for kind, name in enumerate(('one length', 'several lengths')):
         print(f'{name}: ms per 128 templates x 2^25 windows, K = {KS}')
         for v, shape in enumerate(SHAPES):
             tf = [2.0 * 128 * (1 << 25) * k / (table[kind, v, i] * 1e-3) / 1e12 for i, k in enumerate(KS)]
             print(f'  {shape:26s} ' + '  '.join(f'{table[kind, v, i]:8.1f} ms ({t:5.0f} TF)' for i, t in
                                                   enumerate(tf)))
-    print(f'FFT branch: {fft_ms:.2f} ms per template per 2^25 samples (any length up to 16384)')
+    print(f'FFT branch: {fft_ms:.3f} ms per template per 2^25 samples (lengths up to 8192), '
+          f'{fft_long_ms:.3f} (8193 to 16384)')
     if args.out:
         with open(args.out, 'w') as f:
-            json.dump({'k': KS, 'shapes': SHAPES, 'ms': table.tolist(), 'fft_ms': fft_ms}, f, indent=1)
+            json.dump({'k': KS, 'shapes': SHAPES, 'ms': table.tolist(), 'fft_ms': fft_ms,
+                       'fft_long_ms': fft_long_ms}, f, indent=1)
 
 
 if __name__ == '__main__':

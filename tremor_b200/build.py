@@ -24,7 +24,7 @@ NVCC_FLAGS = ARCH + ['-O3', '-lineinfo', '-std=c++17', '-Xcompiler', '-fPIC', '-
                      '-Xcompiler', '-Wall']
 CU_SOURCES = ['tm_api.cu', 'tm_stats.cu', 'tm_scan_fp32.cu', 'tm_select.cu', 'tm_scan_umma.cu', 'tm_noalloc.cu',
               'tm_prefix.cu', 'tm_answers.cu', 'tm_fft.cu', 'tm_groups.cu', 'tm_search.cu', 'tm_serve.cu',
-              'tm_probe.cu', 'tm_fp64.cu']
+              'tm_probe.cu', 'tm_fp64.cu', 'tm_fftk.cu']
 CPP_SOURCES = ['tm_host.cpp']
 
 

@@ -165,7 +165,8 @@ int tm_ctx_destroy(tm_ctx *ctx)
         kv.second->flags.release();
     }
     for (DevBuf *b : {&ctx->prefix, &ctx->ptot, &ctx->pcen, &ctx->run, &ctx->raw, &ctx->clean, &ctx->suf,
-                      &ctx->fft_X, &ctx->fft_shift, &ctx->fft_norm})
+                      &ctx->fft_X, &ctx->fft_shift, &ctx->fft_norm, &ctx->fft2_X, &ctx->fft2_shift, &ctx->fft2_norm,
+                      &ctx->fft2_roots})
         b->release();
     // buffers of batches that outlive the context return to the pool when those batches
     // are destroyed; the driver releases the pool's memory once none is outstanding
@@ -258,11 +259,26 @@ int tm_autotune(tm_ctx *ctx, double *ms, int capacity)
                     table[mixed][v][ki] = per * (33554432.0 / windows);
                 }
             }
-        // the FFT branch: 8 of the last templates (its time does not depend on the length)
+        // the FFT branch, 8 templates each (its time does not depend on the length within
+        // either kind): templates of up to 8192 samples (the fused kernels; 4096 here) and
+        // longer ones (16384)
         tc->tiles = TM_TILES_FFT;
+        double fft_per[2];
+        for (int kind = 0; kind < 2; kind++)
         {
+            std::vector<std::vector<float>> ft(8);
+            std::vector<tm_request> fr(8);
+            for (int t = 0; t < 8; t++)
+            {
+                const int m = kind == 0 ? 4096 : 16384;
+                ft[t].resize(static_cast<size_t>(m));
+                for (int i = 0; i < m; i++)
+                    ft[t][i] = std::sin(0.003f * static_cast<float>(i) * (1.0f + 0.01f * t) +
+                                        1e-6f * static_cast<float>(i) * static_cast<float>(i));
+                fr[t] = tm_request{ft[t].data(), m, TM_MODE_THRESHOLD, 1, 0, 0.995f, 0u};
+            }
             tm_batch b;
-            create_batch(tc, tc->main, reqs.data(), 8, b);
+            create_batch(tc, tc->main, fr.data(), 8, b);
             tm_result res;
             run_batch(tc, tc->main, b, res);
             tc->main.profile = true;
@@ -270,26 +286,29 @@ int tm_autotune(tm_ctx *ctx, double *ms, int capacity)
             tc->main.prof_launches = 0;
             run_batch(tc, tc->main, b, res);
             tc->main.profile = false;
+            fft_per[kind] = tc->main.prof_ms / 8.0 * (33554432.0 / static_cast<double>(n));
         }
-        const double fft_ms = tc->main.prof_ms / 8.0 * (33554432.0 / static_cast<double>(n));
         std::memcpy(ctx->tile_ms, table, sizeof(table));
-        ctx->fft_ms = fft_ms;
-        for (int i = 0; i < std::min(capacity, 33); i++)
-            ms[i] = i < 32 ? (&table[0][0][0])[i] : fft_ms;
+        ctx->fft_ms = fft_per[0];
+        ctx->fft_long_ms = fft_per[1];
+        for (int i = 0; i < std::min(capacity, 34); i++)
+            ms[i] = i < 32 ? (&table[0][0][0])[i] : fft_per[i - 32];
     });
-    return rc == TM_OK ? 33 : rc;
+    return rc == TM_OK ? 34 : rc;
 }
 
 int tm_set_tile_model(tm_ctx *ctx, const double *ms, int count)
 {
-    if (ctx == nullptr || ms == nullptr || (count != 32 && count != 33))
+    if (ctx == nullptr || ms == nullptr || count < 32 || count > 34)
         return TM_ERR_ARGUMENT;
     for (int i = 0; i < count; i++)
         if (!(ms[i] > 0.0) || !std::isfinite(ms[i]))
             return TM_ERR_ARGUMENT;
     std::memcpy(ctx->tile_ms, ms, sizeof(ctx->tile_ms));
-    if (count == 33)
+    if (count >= 33)
         ctx->fft_ms = ms[32];
+    if (count == 34)
+        ctx->fft_long_ms = ms[33];
     return TM_OK;
 }
 

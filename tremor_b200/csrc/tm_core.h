@@ -273,6 +273,7 @@ struct Lane
     cufftHandle fft_plan1 = 0, fft_planB = 0;
     bool fft_plans = false;
     DevBuf fft_y, fft_Y, fft_Z, fft_out;
+    DevBuf fft2_Y, fft2_rows; // fused branch: template spectra and rows of a launch
     // instrumentation
     bool profile = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr, ev4 = nullptr;
@@ -302,7 +303,7 @@ struct Lane
             fft_plans = false;
         }
         for (DevBuf *b : {&tkey, &bmin_u, &bmin_l, &list, &counters, &cand, &dist, &akeys, &avals, &avals64, &sort_tmp,
-                          &segs, &fft_y, &fft_Y, &fft_Z, &fft_out})
+                          &segs, &fft_y, &fft_Y, &fft_Z, &fft_out, &fft2_Y, &fft2_rows})
             b->release();
         for (HostBuf *b : {&h_split, &h_q, &h_order, &h_slots, &h_counters})
             b->release();
@@ -355,7 +356,16 @@ struct tm_ctx
     uint32_t fft_P = 0;
     bool fft_ready = false;
     std::mutex fft_mu;
-    double fft_ms = 1.4; // model: ms per template per 2^25 samples (B200; tm_autotune measures it)
+    // the fused in-tree FFT branch for templates of up to 8192 samples (tm_fftk.cu): spectra
+    // of pieces of 16384 samples every 8192, their shifts and norms, the twiddle tables
+    tmh::DevBuf fft2_X, fft2_shift, fft2_norm, fft2_roots;
+    uint32_t fft2_P = 0;
+    bool fft2_ready = false;
+    int sms = 148;
+    // model: the FFT branch's ms per template per 2^25 samples, for templates of up to 8192
+    // samples (the fused kernels) and longer ones (B200 defaults; tm_autotune measures both)
+    double fft_ms = 0.25;
+    double fft_long_ms = 1.4;
     // the context's own memory pool for per-batch buffers (DevBuf::reserve_on); it keeps
     // up to 4 GiB of freed memory for the next batch
     cudaMemPool_t pool = nullptr;

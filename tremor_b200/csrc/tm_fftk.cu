@@ -1,0 +1,432 @@
+// In-tree FP64 FFT kernels of the FFT branch for templates of up to kF2S = 8192 samples:
+// the spectra of the record's pieces, the templates' spectra, and one fused kernel that
+// correlates every template of a group with every piece and evaluates the distance bound,
+// bucket minima and threshold candidates straight from shared memory. TREMOR's FFT branch
+// (fft_fallback.hpp:67-117: per piece, the product with the template spectrum, an inverse
+// real FFT, the dot product of each window and the distance filter with an error bound) has
+// this structure; here neither the product spectrum nor the correlation leaves the SM.
+//
+// Pieces: kF2L = 16384 samples starting every kF2S = 8192 samples (shifted by s_p, the
+// centre of the prefix block holding the piece's start, rounded to float). Window
+// j = p kF2S + o (0 <= o < kF2S) of piece p has its dot product at output o + m - 1 of the
+// circular correlation, which does not wrap for m <= kF2L - kF2S + 1.
+//
+// Real transforms of length L = 16384 go through complex ones of N = L / 2 = 8192 points:
+//   forward: z[n] = x[2n] + i x[2n+1], Z = FFT_N(z),
+//            X[k] = (Z[k] + conj Z[N-k]) / 2 - i e^{-2 pi i k / L} (Z[k] - conj Z[N-k]) / 2;
+//   inverse: for a Hermitian spectrum V (V[k] = X[k] Y[k]),
+//            C[k] = (V[k] + conj V[N-k]) + i e^{2 pi i k / L} (V[k] - conj V[N-k]),
+//            c = IFFT_N(C) (unnormalised), out[2n] = Re c[n], out[2n+1] = Im c[n],
+//            and out / L is the circular correlation of x with the reversed template.
+// The complex FFTs are Stockham radix-16, 16, 16 then 2 (N = 8192; Govindaraju et al.,
+// "High Performance Discrete Fourier Transforms on Graphics Processors", SC 2008): 512
+// threads, each holding 16 points in registers between a pass's shared-memory read and its
+// write, so every pass works in place; the buffer is padded by one point per 16 so that
+// the first pass's stride-16 writes hit distinct banks. The final radix-2 pass of the
+// inverse is evaluated where its outputs are read (by the distance epilogue).
+//
+// Twiddles: e^{2 pi i e / 16384} = R2[e >> 7] R1[e & 127] from two 128-entry tables
+// computed on the host in extended precision and rounded (error <= 4u with u = 2^-53,
+// the product included); a pass's powers w^r (r = 1..15) by repeated multiplication
+// (error <= 7 r u <= 105u). Error of an output (Higham, Accuracy and Stability of
+// Numerical Algorithms, Thm 24.2, ||fl(FFT x) - FFT x||_2 <= t eta / (1 - t eta) ||FFT x||_2,
+// eta = mu + gamma_4 (sqrt 2 + mu), mu the twiddle error): with mu = 105u and t = 16 (13
+// complex stages plus the real-transform packing) and a factor 10 for the radix-16 and
+// packing arithmetic, kappa = 10 x 16 x 111u; then, as for the length-32768 pieces
+// (tm_fft.cu), every correlation output is within kappa ||x - s_p||_2 ||q||_2 (2 sqrt m +
+// sqrt L) of the exact one.
+#include <cmath>
+
+#include "../../include/tremor_b200.h"
+#include "tm_epilogue.cuh"
+#include "tm_fft.cuh"
+
+namespace tmb {
+
+constexpr int kF2T = 512;                        // threads per block
+constexpr int kF2Buf = kF2N + kF2N / 16 + 16;    // padded complex entries of the work buffer
+constexpr double kF2Kappa = 10.0 * 16.0 * 111.0 * 1.1102230246251565e-16;
+constexpr size_t kF2Smem = sizeof(double2) * (size_t)(kF2Buf + 256);
+
+__device__ __forceinline__ int pidx(int i) { return i + (i >> 4); }
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b)
+{
+    return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 conj2(double2 a) { return make_double2(a.x, -a.y); }
+// a * (s i): s = +1 or -1
+template <int S> __device__ __forceinline__ double2 mul_si(double2 a)
+{
+    return S > 0 ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
+}
+
+// e^{S 2 pi i e / 16384}, 0 <= e < 16384, from the shared tables R (R1 then R2).
+template <int S> __device__ __forceinline__ double2 root(const double2 *R, int e)
+{
+    const double2 w = cmul(R[128 + (e >> 7)], R[e & 127]);
+    return S > 0 ? w : conj2(w);
+}
+
+// 4-point DFT with e^{S 2 pi i / 4} = S i, in place on x0..x3.
+template <int S> __device__ __forceinline__ void dft4(double2 &x0, double2 &x1, double2 &x2, double2 &x3)
+{
+    const double2 a = cadd(x0, x2), b = csub(x0, x2), c = cadd(x1, x3), d = mul_si<S>(csub(x1, x3));
+    x0 = cadd(a, c);
+    x2 = csub(a, c);
+    x1 = cadd(b, d);
+    x3 = csub(b, d);
+}
+
+// 16-point DFT in natural order, as 4 x 4: t[b][c] = DFT4_a(v[4a + b])[c], times
+// W16^{bc}, then X[c + 4d] = DFT4_b(t[b][c])[d].
+template <int S> __device__ __forceinline__ void dft16(double2 (&v)[16])
+{
+    constexpr double c1 = 0.92387953251128675613, s1 = 0.38268343236508977173, h = 0.70710678118654752440;
+#pragma unroll
+    for (int b = 0; b < 4; b++)
+        dft4<S>(v[b], v[4 + b], v[8 + b], v[12 + b]); // v[4c + b] now holds t[b][c]
+    // twiddles W16^{bc} (b, c = 1..3): exponents 1, 2, 3, 2, 4, 6, 3, 6, 9
+    const double2 w1 = make_double2(c1, S * s1), w2 = make_double2(h, S * h), w3 = make_double2(s1, S * c1);
+    const double2 w6 = make_double2(-h, S * h), w9 = make_double2(-c1, -S * s1);
+    v[4 + 1] = cmul(v[4 + 1], w1);
+    v[8 + 1] = cmul(v[8 + 1], w2);
+    v[12 + 1] = cmul(v[12 + 1], w3);
+    v[4 + 2] = cmul(v[4 + 2], w2);
+    v[8 + 2] = mul_si<S>(v[8 + 2]); // W16^4 = S i
+    v[12 + 2] = cmul(v[12 + 2], w6);
+    v[4 + 3] = cmul(v[4 + 3], w3);
+    v[8 + 3] = cmul(v[8 + 3], w6);
+    v[12 + 3] = cmul(v[12 + 3], w9);
+#pragma unroll
+    for (int c = 0; c < 4; c++)
+        dft4<S>(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]); // X[c + 4d] in v[4c + d]
+    // natural order: X[c + 4d] from v[4c + d] (a 4 x 4 transpose of registers)
+#pragma unroll
+    for (int c = 0; c < 4; c++)
+#pragma unroll
+        for (int d = c + 1; d < 4; d++)
+        {
+            const double2 t = v[4 * c + d];
+            v[4 * c + d] = v[4 * d + c];
+            v[4 * d + c] = t;
+        }
+}
+
+// One Stockham radix-16 pass over the padded buffer (N = 8192, 512 threads, in place: every
+// thread reads its 16 points, the block synchronises, then every thread writes).
+template <int S> __device__ __forceinline__ void pass16(double2 *buf, const double2 *R, int Ns)
+{
+    const int j = threadIdx.x;
+    double2 v[16];
+#pragma unroll
+    for (int r = 0; r < 16; r++)
+        v[r] = buf[pidx(j + 512 * r)];
+    __syncthreads();
+    const int k = j & (Ns - 1);
+    if (Ns > 1)
+    {
+        const double2 w1 = root<S>(R, k * (1024 / Ns)); // W^k, W = e^{S 2 pi i / (16 Ns)}
+        double2 w = w1;
+#pragma unroll
+        for (int r = 1; r < 16; r++)
+        {
+            v[r] = cmul(v[r], w);
+            if (r < 15)
+                w = cmul(w, w1);
+        }
+    }
+    dft16<S>(v);
+    const int d0 = (j - k) * 16 + k;
+#pragma unroll
+    for (int r = 0; r < 16; r++)
+        buf[pidx(d0 + r * Ns)] = v[r];
+    __syncthreads();
+}
+
+// The three radix-16 passes of an 8192-point transform; the radix-2 pass is left to the
+// caller (final_out, or the forward kernel's explicit pass).
+template <int S> __device__ __forceinline__ void fft8192_r16(double2 *buf, const double2 *R)
+{
+    pass16<S>(buf, R, 1);
+    pass16<S>(buf, R, 16);
+    pass16<S>(buf, R, 256);
+}
+
+// Output i (0 <= i < 8192) of the final radix-2 pass: c[i] = a + w b, c[i + 4096] = a - w b
+// with a = buf[i mod 4096], b = buf[i mod 4096 + 4096], w = e^{S 2 pi i (i mod 4096) / 8192}.
+template <int S> __device__ __forceinline__ double2 final_out(const double2 *buf, const double2 *R, int i)
+{
+    const int i0 = i & 4095;
+    const double2 a = buf[pidx(i0)], b = cmul(buf[pidx(i0 + 4096)], root<S>(R, 2 * i0));
+    return i < 4096 ? cadd(a, b) : csub(a, b);
+}
+
+__device__ __forceinline__ void load_roots(double2 *R, const double2 *roots)
+{
+    for (int i = threadIdx.x; i < 256; i += blockDim.x)
+        R[i] = roots[i];
+}
+
+// Forward real FFT of one piece of the record (blockIdx.x < pieces) or one template row
+// (templates: reversed and zero-padded to kF2L), into out[blockIdx.x * kF2H ..].
+__global__ void __launch_bounds__(kF2T, 1) k_fft2_forward(const float *__restrict__ clean, uint64_t n,
+                                                         const double *__restrict__ centres, uint32_t p0,
+                                                         const float *__restrict__ q, const TemplParam *__restrict__ tp,
+                                                         const int *__restrict__ rows, const double2 *__restrict__ roots,
+                                                         double2 *__restrict__ out, double *__restrict__ shifts,
+                                                         double *__restrict__ norms)
+{
+    extern __shared__ double2 sm2[];
+    double2 *buf = sm2, *R = sm2 + kF2Buf;
+    __shared__ double part[kF2T / 32];
+    load_roots(R, roots);
+    const bool templ = q != nullptr;
+    double s = 0.0, sq = 0.0;
+    uint64_t start = 0;
+    const float *qt = nullptr;
+    int m = 0;
+    if (templ)
+    {
+        const TemplParam &p = tp[rows[blockIdx.x]];
+        qt = q + p.q_offset;
+        m = p.m;
+    }
+    else
+    {
+        start = (uint64_t)(p0 + blockIdx.x) * kF2S;
+        s = (double)(float)centres[start >> kPrefixBlockLog];
+    }
+    for (int i = threadIdx.x; i < kF2N; i += kF2T)
+    {
+        double a, b;
+        if (templ)
+        {
+            const int i0 = 2 * i, i1 = 2 * i + 1; // y[i] = q[m - 1 - i]
+            a = i0 < m ? (double)qt[m - 1 - i0] : 0.0;
+            b = i1 < m ? (double)qt[m - 1 - i1] : 0.0;
+        }
+        else
+        {
+            const uint64_t g = start + 2 * (uint64_t)i;
+            a = g < n ? (double)clean[g] - s : 0.0;
+            b = g + 1 < n ? (double)clean[g + 1] - s : 0.0;
+            sq = fma(a, a, sq);
+            sq = fma(b, b, sq);
+        }
+        buf[pidx(i)] = make_double2(a, b);
+    }
+    __syncthreads();
+    fft8192_r16<-1>(buf, R);
+    // the radix-2 pass, in place (each thread owns the pairs (i, i + 4096) it touches)
+    for (int i = threadIdx.x; i < 4096; i += kF2T)
+    {
+        const double2 a = buf[pidx(i)], b = cmul(buf[pidx(i + 4096)], root<-1>(R, 2 * i));
+        buf[pidx(i)] = cadd(a, b);
+        buf[pidx(i + 4096)] = csub(a, b);
+    }
+    __syncthreads();
+    double2 *o = out + (size_t)blockIdx.x * kF2H;
+    for (int k = threadIdx.x; k <= kF2N / 2; k += kF2T)
+    {
+        // X[k] and X[N - k] from Z[k] and Z[N - k] (Z[N] = Z[0])
+        const double2 A = buf[pidx(k)], Bc = conj2(buf[pidx(k == 0 ? 0 : kF2N - k)]);
+        const double2 E = make_double2(0.5 * (A.x + Bc.x), 0.5 * (A.y + Bc.y));
+        const double2 D = csub(A, Bc);
+        const double2 O = make_double2(0.5 * D.y, -0.5 * D.x); // -i (A - B) / 2
+        const double2 w = root<-1>(R, k);                       // e^{-2 pi i k / L}
+        o[k] = cadd(E, cmul(O, w));
+        if (k == 0)
+            o[kF2N] = csub(E, O); // twiddle e^{-i pi} = -1
+        else if (k < kF2N / 2)
+        {
+            const double2 A2 = conj2(Bc), B2c = conj2(A); // Z[N - k], conj Z[k]
+            const double2 E2 = make_double2(0.5 * (A2.x + B2c.x), 0.5 * (A2.y + B2c.y));
+            const double2 D2 = csub(A2, B2c);
+            const double2 O2 = make_double2(0.5 * D2.y, -0.5 * D2.x);
+            o[kF2N - k] = csub(E2, cmul(O2, conj2(w))); // e^{-2 pi i (N - k) / L} = -e^{2 pi i k / L}
+        }
+    }
+    if (!templ)
+    {
+        for (int off = 16; off > 0; off >>= 1)
+            sq += __shfl_down_sync(0xffffffffu, sq, off);
+        if ((threadIdx.x & 31) == 0)
+            part[threadIdx.x >> 5] = sq;
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+            double t = 0.0;
+            for (int w = 0; w < kF2T / 32; w++)
+                t += part[w];
+            shifts[p0 + blockIdx.x] = s;
+            norms[p0 + blockIdx.x] = sqrt(t) * (1.0 + 1e-12); // rounding of the norm itself, generously
+        }
+    }
+}
+
+// The fused correlation: persistent blocks over pieces; per piece, every template of the
+// launch: C from X[p] Y[t] (the product and the real-transform packing in one step), the
+// radix-16 passes, then one thread per window: its dot product from the final radix-2
+// pass, the distance and bound as the contraction kernels' epilogues (fast_distance_mixed
+// with prefix-sum statistics) plus the FFT's own error, then kNN bucket minima or threshold
+// candidates.
+__global__ void __launch_bounds__(kF2T, 1) k_fft2_corr(const Fft2Args a)
+{
+    extern __shared__ double2 sm2[];
+    double2 *buf = sm2, *R = sm2 + kF2Buf;
+    load_roots(R, a.roots);
+    const int lane = threadIdx.x & 31;
+    const double inv_l = 1.0 / (double)kF2L;
+    for (uint32_t pi = blockIdx.x; pi < a.p_count; pi += gridDim.x)
+    {
+        const uint32_t p = a.p_first + pi;
+        const double2 *X = a.X + (size_t)p * kF2H;
+        const float shift = (float)a.shifts[p];
+        const double norm = a.norms[p];
+        for (int ti = 0; ti < a.nrows; ti++)
+        {
+            const int t = a.rows[ti];
+            const TemplParam P = a.tp[t];
+            const uint64_t piece_w = (uint64_t)p * kF2S;
+            // windows of this piece in the template's range [w0, w0 + wcount)
+            if (piece_w + kF2S <= a.w0 || piece_w >= a.w0 + (uint64_t)P.wcount)
+                continue;
+            const double2 *Y = a.Y + (size_t)ti * kF2H;
+            __syncthreads(); // the previous template's epilogue has read buf
+            for (int k = threadIdx.x; k <= kF2N / 2; k += kF2T)
+            {
+                const int kn = kF2N - k;
+                const double2 Vk = cmul(X[k], Y[k]), Vn = cmul(X[kn], Y[kn]);
+                const double2 w = root<1>(R, k); // e^{2 pi i k / L}
+                // C[k] = E + i O with E = Vk + conj Vn, O = w (Vk - conj Vn); C[N - k] = conj E + i conj O
+                const double2 E = cadd(Vk, conj2(Vn));
+                const double2 O = cmul(csub(Vk, conj2(Vn)), w);
+                if (k == 0)
+                    buf[pidx(0)] = cadd(E, mul_si<1>(O)); // C[0] (Vn = V[N], the Nyquist bin)
+                else
+                {
+                    buf[pidx(k)] = cadd(E, mul_si<1>(O));
+                    if (k < kF2N / 2)
+                        buf[pidx(kn)] = cadd(conj2(E), mul_si<1>(conj2(O)));
+                }
+            }
+            __syncthreads();
+            fft8192_r16<1>(buf, R);
+            // epilogue: windows o = it * 512 + thread (a warp's 32 windows are consecutive)
+            const double sm_ = sqrt((double)P.m);
+            const float e_dot = (float)(kF2Kappa * norm * sm_ * (2.0 * sm_ + sqrt((double)kF2L)) * 1.01);
+            for (int it = 0; it < kF2S / kF2T; it++)
+            {
+                const uint32_t o = (uint32_t)(it * kF2T) + threadIdx.x;
+                const uint64_t g = piece_w + o;
+                const bool in_range = g >= a.w0 && g - a.w0 < P.wcount;
+                const uint32_t jr = in_range ? (uint32_t)(g - a.w0) : 0u;
+                bool ok = in_range && a.raw[g] != kMissing && a.run[g] < (uint16_t)min(P.m, 65535);
+                float up = inf_f(), lo = inf_f();
+                bool hit = false;
+                if (ok)
+                {
+                    WindowStats ws;
+                    if (window_prefix_stats(a.pv, a.pv.Q[g], a.pv.Q[g + (uint64_t)P.m], g, P.m, P.inv_m, ws) == 0)
+                    {
+                        const int nn = (int)o + P.m - 1;
+                        const double2 c = final_out<1>(buf, R, nn >> 1);
+                        const double dot = ((nn & 1) ? c.y : c.x) * inv_l;
+                        float d, e;
+                        fast_distance_mixed(P, P.a1_main, (float)dot, ws.mu, ws.iv, shift,
+                                            stats_error(ws, P.m, P.qs, P.s1), d, e);
+                        e += 2.0f * e_dot * ws.iv * 1.01f;
+                        if (a.dbg_d != nullptr)
+                        {
+                            a.dbg_d[(size_t)t * a.W + jr] = d;
+                            a.dbg_e[(size_t)t * a.W + jr] = e;
+                        }
+                        up = d + e;
+                        lo = d - e;
+                        hit = lo <= P.thr_ed;
+                    }
+                    else
+                    {
+                        lo = -inf_f();
+                        hit = true;
+                    }
+                }
+                if (P.mode == TM_MODE_KNN)
+                {
+                    // bucket minima: a warp's 32 windows lie in at most two buckets
+                    const uint32_t bucket = jr / kBucket;
+                    const unsigned act = __ballot_sync(0xffffffffu, in_range);
+                    if (act == 0u)
+                        continue;
+                    const uint32_t b0 = __shfl_sync(0xffffffffu, bucket, __ffs(act) - 1);
+                    const unsigned same = __ballot_sync(0xffffffffu, in_range && bucket == b0);
+                    const unsigned other = act & ~same;
+                    const uint32_t ku = float_key(up), kl = float_key(lo);
+                    const uint32_t u0 = __reduce_min_sync(0xffffffffu, same & (1u << lane) ? ku : 0xffffffffu);
+                    const uint32_t l0 = __reduce_min_sync(0xffffffffu, same & (1u << lane) ? kl : 0xffffffffu);
+                    const uint32_t u1 = __reduce_min_sync(0xffffffffu, other & (1u << lane) ? ku : 0xffffffffu);
+                    const uint32_t l1 = __reduce_min_sync(0xffffffffu, other & (1u << lane) ? kl : 0xffffffffu);
+                    const uint32_t none = float_key(inf_f());
+                    if (lane == __ffs(act) - 1 && (u0 != none || l0 != none) && u0 != 0xffffffffu)
+                    {
+                        atomicMin(&a.bmin_u[(size_t)t * a.nb + b0], u0);
+                        atomicMin(&a.bmin_l[(size_t)t * a.nb + b0], l0);
+                    }
+                    if (other != 0u && lane == __ffs(other) - 1 && (u1 != none || l1 != none))
+                    {
+                        atomicMin(&a.bmin_u[(size_t)t * a.nb + bucket], u1);
+                        atomicMin(&a.bmin_l[(size_t)t * a.nb + bucket], l1);
+                    }
+                }
+                else
+                    emit_candidates(hit ? 1u : 0u, lane, (uint32_t)t, jr, a.cand, a.cand_count, a.cand_cap);
+            }
+        }
+    }
+}
+
+void fft2_roots(double2 *host256)
+{
+    // R1[a] = e^{2 pi i a / 16384}, R2[b] = e^{2 pi i 128 b / 16384}, in extended precision
+    const long double two_pi = 6.283185307179586476925286766559005768L;
+    for (int a = 0; a < 128; a++)
+    {
+        const long double t1 = two_pi * (long double)a / 16384.0L, t2 = two_pi * (long double)(128 * a) / 16384.0L;
+        host256[a] = make_double2((double)cosl(t1), (double)sinl(t1));
+        host256[128 + a] = make_double2((double)cosl(t2), (double)sinl(t2));
+    }
+}
+
+uint32_t fft2_pieces(uint64_t n) { return (uint32_t)((n + kF2S - 1) / kF2S); }
+
+cudaError_t launch_fft2_pieces(const float *clean, uint64_t n, const double *centres, uint32_t p0, uint32_t count,
+                               const double2 *roots, double2 *X, double *shifts, double *norms, cudaStream_t s)
+{
+    cudaFuncSetAttribute(k_fft2_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kF2Smem);
+    if (count > 0)
+        k_fft2_forward<<<count, kF2T, kF2Smem, s>>>(clean, n, centres, p0, nullptr, nullptr, nullptr, roots,
+                                                     X + (size_t)p0 * kF2H, shifts, norms);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fft2_templates(const float *q, const TemplParam *tp, const int *rows, int nrows,
+                                  const double2 *roots, double2 *Y, cudaStream_t s)
+{
+    cudaFuncSetAttribute(k_fft2_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kF2Smem);
+    if (nrows > 0)
+        k_fft2_forward<<<nrows, kF2T, kF2Smem, s>>>(nullptr, 0, nullptr, 0, q, tp, rows, roots, Y, nullptr, nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fft2_corr(const Fft2Args &a, int sms, cudaStream_t s)
+{
+    cudaFuncSetAttribute(k_fft2_corr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kF2Smem);
+    if (a.p_count > 0 && a.nrows > 0)
+        k_fft2_corr<<<(unsigned)std::min<uint32_t>(a.p_count, (uint32_t)sms), kF2T, kF2Smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+} // namespace tmb

@@ -375,10 +375,12 @@ size_t plan_fft_split(const tm_ctx *ctx, const tm_request *reqs, const std::vect
     for (size_t i = 0; i < n; i++)
         m[i] = reqs[sorted_idx[i]].m;
     size_t best_f = 0;
-    double best = tensor_cost_sorted(ctx, m.data(), n);
+    double best = tensor_cost_sorted(ctx, m.data(), n), fft_cost = 0.0;
     for (size_t f = 1; f <= n; f++)
     {
-        const double c = static_cast<double>(f) * ctx->fft_ms + tensor_cost_sorted(ctx, m.data() + f, n - f);
+        // the fused kernels take templates of up to 8192 samples; longer ones cost more
+        fft_cost += m[f - 1] <= tmb::kF2S ? ctx->fft_ms : ctx->fft_long_ms;
+        const double c = fft_cost + tensor_cost_sorted(ctx, m.data() + f, n - f);
         if (c < best)
         {
             best = c;

@@ -546,6 +546,87 @@ void ensure_fft(tm_ctx *ctx, Lane &L)
     ctx->fft_ready = true;
 }
 
+// Spectra of the record's pieces of 16384 samples every 8192 for the fused FFT branch
+// (tm_fftk.cu), their shifts and norms, and the twiddle tables: built once per context.
+void ensure_fft2(tm_ctx *ctx, Lane &L)
+{
+    std::lock_guard<std::mutex> lk(ctx->fft_mu);
+    if (ctx->fft2_ready)
+        return;
+    ensure_prefix(ctx, L);
+    cudaStream_t s = L.stream;
+    const uint32_t P = tmb::fft2_pieces(ctx->n);
+    ctx->fft2_X.reserve(sizeof(double2) * static_cast<size_t>(P) * tmb::kF2H);
+    ctx->fft2_shift.reserve(sizeof(double) * P);
+    ctx->fft2_norm.reserve(sizeof(double) * P);
+    ctx->fft2_roots.reserve(sizeof(double2) * 256);
+    std::vector<double2> roots(256);
+    tmb::fft2_roots(roots.data());
+    TM_CUDA(cudaMemcpyAsync(ctx->fft2_roots.p, roots.data(), sizeof(double2) * 256, cudaMemcpyHostToDevice, s));
+    const uint32_t B = 16384; // pieces per launch
+    for (uint32_t p0 = 0; p0 < P; p0 += B)
+    {
+        TM_CUDA(tmb::launch_fft2_pieces(ctx->clean.as<float>(), ctx->n, ctx->pcen.as<double>(), p0,
+                                        std::min<uint32_t>(B, P - p0), ctx->fft2_roots.as<double2>(),
+                                        ctx->fft2_X.as<double2>(), ctx->fft2_shift.as<double>(),
+                                        ctx->fft2_norm.as<double>(), s));
+        count_launch(L);
+    }
+    TM_CUDA(cudaStreamSynchronize(s));
+    int sms = 0;
+    TM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    ctx->sms = sms;
+    ctx->fft2_P = P;
+    ctx->fft2_ready = true;
+}
+
+// The fused FFT branch for the group's rows `rows` (templates of up to 8192 samples): their
+// spectra, then one persistent launch over the pieces their windows touch.
+static void fft2_contract(tm_ctx *ctx, Lane &L, const GroupPlan &g, const tmb::ScanArgs &a,
+                          const std::vector<int> &rows)
+{
+    ensure_fft2(ctx, L);
+    cudaStream_t s = L.stream;
+    const int nr = static_cast<int>(rows.size());
+    L.fft2_Y.reserve(sizeof(double2) * static_cast<size_t>(nr) * tmb::kF2H);
+    L.fft2_rows.reserve(sizeof(int) * static_cast<size_t>(nr));
+    TM_CUDA(cudaMemcpyAsync(L.fft2_rows.p, rows.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, s));
+    TM_CUDA(tmb::launch_fft2_templates(g.q.as<float>(), g.tp.as<TemplParam>(), L.fft2_rows.as<int>(), nr,
+                                       ctx->fft2_roots.as<double2>(), L.fft2_Y.as<double2>(), s));
+    uint64_t wmax = 0;
+    for (int t : rows)
+        wmax = std::max<uint64_t>(wmax, g.htp[static_cast<size_t>(t)].wcount);
+    const uint64_t first = a.w0, last = a.w0 + wmax - 1;
+    const uint32_t pa = static_cast<uint32_t>(first / tmb::kF2S);
+    const uint32_t pb = std::min<uint32_t>(static_cast<uint32_t>(last / tmb::kF2S), ctx->fft2_P - 1);
+    tmb::Fft2Args f{};
+    f.X = ctx->fft2_X.as<double2>();
+    f.shifts = ctx->fft2_shift.as<double>();
+    f.norms = ctx->fft2_norm.as<double>();
+    f.p_first = pa;
+    f.p_count = pb >= pa ? pb - pa + 1 : 0;
+    f.Y = L.fft2_Y.as<double2>();
+    f.rows = L.fft2_rows.as<int>();
+    f.nrows = nr;
+    f.tp = g.tp.as<TemplParam>();
+    f.roots = ctx->fft2_roots.as<double2>();
+    f.w0 = a.w0;
+    f.W = a.W;
+    f.pv = tmb::PrefixView{a.P, a.PT, a.PC};
+    f.run = a.run;
+    f.raw = a.raw;
+    f.bmin_u = a.bmin_u;
+    f.bmin_l = a.bmin_l;
+    f.nb = a.nb;
+    f.cand = a.cand;
+    f.cand_count = a.cand_count;
+    f.cand_cap = a.cand_cap;
+    f.dbg_d = a.dbg_d;
+    f.dbg_e = a.dbg_e;
+    TM_CUDA(tmb::launch_fft2_corr(f, ctx->sms, s));
+    count_launch(L, 2);
+}
+
 // The lane's FFT plans and buffers.
 void ensure_lane_fft(Lane &L)
 {
@@ -573,15 +654,27 @@ void ensure_lane_fft(Lane &L)
 // list as the contraction kernels (a: the launch arguments those would get).
 void fft_contract(tm_ctx *ctx, Lane &L, const GroupPlan &g, const tmb::ScanArgs &a)
 {
-    ensure_fft(ctx, L);
-    ensure_lane_fft(L);
-    cudaStream_t s = L.stream;
-    const uint32_t B = tmb::kFftBatch, P = ctx->fft_P;
+    // templates of up to 8192 samples: the fused in-tree kernels; longer ones (up to 16384):
+    // pieces of 32768 samples through the toolkit's FFT
+    std::vector<int> short_rows, long_rows;
     for (int t = 0; t < g.T; t++)
     {
         const TemplParam &p = g.htp[t];
         if (g.index[t] < 0 || p.wcount == 0)
             continue;
+        (p.m <= tmb::kF2S ? short_rows : long_rows).push_back(t);
+    }
+    if (!short_rows.empty())
+        fft2_contract(ctx, L, g, a, short_rows);
+    if (long_rows.empty())
+        return;
+    ensure_fft(ctx, L);
+    ensure_lane_fft(L);
+    cudaStream_t s = L.stream;
+    const uint32_t B = tmb::kFftBatch, P = ctx->fft_P;
+    for (int t : long_rows)
+    {
+        const TemplParam &p = g.htp[t];
         TM_CUDA(tmb::launch_fft_template(g.q.as<float>() + p.q_offset, p.m, L.fft_y.as<double>(), s));
         TM_CUFFT(cufftExecD2Z(L.fft_plan1, L.fft_y.as<cufftDoubleReal>(),
                               reinterpret_cast<cufftDoubleComplex *>(L.fft_Y.p)));
