@@ -23,7 +23,7 @@ ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 NVCC_FLAGS = ARCH + ['-O3', '-lineinfo', '-std=c++17', '-Xcompiler', '-fPIC', '--expt-relaxed-constexpr',
                      '-Xcompiler', '-Wall']
 CU_SOURCES = ['tm_api.cu', 'tm_stats.cu', 'tm_scan_fp32.cu', 'tm_select.cu', 'tm_scan_umma.cu', 'tm_noalloc.cu',
-              'tm_prefix.cu', 'tm_answers.cu', 'tm_fft.cu', 'tm_groups.cu', 'tm_search.cu', 'tm_serve.cu',
+              'tm_prefix.cu', 'tm_answers.cu', 'tm_groups.cu', 'tm_search.cu', 'tm_serve.cu',
               'tm_probe.cu', 'tm_fp64.cu', 'tm_fftk.cu']
 CPP_SOURCES = ['tm_host.cpp']
 
@@ -64,7 +64,7 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> Path:
             print(log)
     objs = [str(OUT / (s + '.o')) for s in CU_SOURCES + CPP_SOURCES]
     tmp = LIB.with_suffix('.so.tmp')
-    _run([nvcc, *ARCH, '-shared', '-o', str(tmp), *objs, '-lcufft'], verbose)
+    _run([nvcc, *ARCH, '-shared', '-o', str(tmp), *objs], verbose)
     os.replace(tmp, LIB)
     # the command-line driver (tremor_main's options and files), next to the library
     cli_tmp = CLI.with_suffix('.tmp')

@@ -165,8 +165,8 @@ int tm_ctx_destroy(tm_ctx *ctx)
         kv.second->flags.release();
     }
     for (DevBuf *b : {&ctx->prefix, &ctx->ptot, &ctx->pcen, &ctx->run, &ctx->raw, &ctx->clean, &ctx->suf,
-                      &ctx->fft_X, &ctx->fft_shift, &ctx->fft_norm, &ctx->fft2_X, &ctx->fft2_shift, &ctx->fft2_norm,
-                      &ctx->fft2_roots})
+                      &ctx->fft2_X, &ctx->fft2_shift, &ctx->fft2_norm, &ctx->fft3_X, &ctx->fft3_shift,
+                      &ctx->fft3_norm, &ctx->fft_roots, &ctx->fft_scratch})
         b->release();
     // buffers of batches that outlive the context return to the pool when those batches
     // are destroyed; the driver releases the pool's memory once none is outstanding
@@ -585,7 +585,7 @@ int tm_bound_diagnostics(tm_ctx *ctx, const float *queries, int count, int m, fl
             idx[i] = i;
         }
         if (ctx->tiles >= TM_TILES_COLS_128 && ctx->kernel != TM_KERNEL_FP32 && tmb::umma_supported(m, count, 0) &&
-            (ctx->tiles != TM_TILES_FFT || m <= tmb::kFftS))
+            (ctx->tiles != TM_TILES_FFT || m <= tmb::kFftMaxM))
         {
             bound_diagnostics_wm(ctx, m, idx, reqs, d, e, exact);
             return;

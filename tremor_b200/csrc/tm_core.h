@@ -33,7 +33,6 @@
 #include "tm_prefix.cuh"
 #include "tm_fft.cuh"
 
-#include <cufft.h>
 
 namespace tmb {
 cudaError_t launch_clean(const float *raw, float *clean, uint64_t n, uint64_t n_total, cudaStream_t s);
@@ -269,11 +268,8 @@ struct Lane
     std::vector<std::shared_ptr<PinnedBlock>> pool;
     HostBuf h_split, h_q, h_order, h_slots, h_counters;
     uint32_t cand_cap = 1u << 22, list_cap = 1u << 20;
-    // FFT branch: plans (one template; a batch of pieces) and buffers, created on first use
-    cufftHandle fft_plan1 = 0, fft_planB = 0;
-    bool fft_plans = false;
-    DevBuf fft_y, fft_Y, fft_Z, fft_out;
-    DevBuf fft2_Y, fft2_rows; // fused branch: template spectra and rows of a launch
+    // FFT branch: the template spectra and rows of a launch (both piece lengths)
+    DevBuf fft2_Y, fft3_Y, fft_rows;
     // instrumentation
     bool profile = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr, ev4 = nullptr;
@@ -296,14 +292,8 @@ struct Lane
     {
         if (stream)
             cudaStreamSynchronize(stream);
-        if (fft_plans)
-        {
-            cufftDestroy(fft_plan1);
-            cufftDestroy(fft_planB);
-            fft_plans = false;
-        }
         for (DevBuf *b : {&tkey, &bmin_u, &bmin_l, &list, &counters, &cand, &dist, &akeys, &avals, &avals64, &sort_tmp,
-                          &segs, &fft_y, &fft_Y, &fft_Z, &fft_out, &fft2_Y, &fft2_rows})
+                          &segs, &fft2_Y, &fft3_Y, &fft_rows})
             b->release();
         for (HostBuf *b : {&h_split, &h_q, &h_order, &h_slots, &h_counters})
             b->release();
@@ -351,16 +341,13 @@ struct tm_ctx
     // their block totals and centres, constant runs
     tmh::DevBuf prefix, ptot, pcen, run;
     bool prefix_ready = false;
-    // FFT branch: spectra of the record's pieces, their shifts and norms (built on first use)
-    tmh::DevBuf fft_X, fft_shift, fft_norm;
-    uint32_t fft_P = 0;
-    bool fft_ready = false;
+    // FFT branch (tm_fftk.cu), built on first use: spectra of pieces of 16384 samples every
+    // 8192 (templates of up to 8192 samples) and of pieces of 32768 every 16384 (longer ones),
+    // their shifts and norms; the twiddle tables; the forward transforms' scratch
+    tmh::DevBuf fft2_X, fft2_shift, fft2_norm, fft3_X, fft3_shift, fft3_norm, fft_roots, fft_scratch;
+    uint32_t fft2_P = 0, fft3_P = 0;
+    bool fft2_ready = false, fft3_ready = false;
     std::mutex fft_mu;
-    // the fused in-tree FFT branch for templates of up to 8192 samples (tm_fftk.cu): spectra
-    // of pieces of 16384 samples every 8192, their shifts and norms, the twiddle tables
-    tmh::DevBuf fft2_X, fft2_shift, fft2_norm, fft2_roots;
-    uint32_t fft2_P = 0;
-    bool fft2_ready = false;
     int sms = 148;
     // model: the FFT branch's ms per template per 2^25 samples, for templates of up to 8192
     // samples (the fused kernels) and longer ones (B200 defaults; tm_autotune measures both)
@@ -457,15 +444,6 @@ struct tm_batch
             g.release();
     }
 };
-
-#define TM_CUFFT(call)                                                                                            \
-    do                                                                                                            \
-    {                                                                                                             \
-        const cufftResult r_ = (call);                                                                            \
-        if (r_ != CUFFT_SUCCESS)                                                                                  \
-            throw tmh::Failure{r_ == CUFFT_ALLOC_FAILED ? TM_ERR_NO_MEMORY : TM_ERR_CUDA,                        \
-                               std::string(#call) + ": cuFFT error " + std::to_string(static_cast<int>(r_))};    \
-    } while (0)
 
 namespace tmh {
 

@@ -1,39 +1,48 @@
-// In-tree FP64 FFT kernels of the FFT branch for templates of up to kF2S = 8192 samples:
-// the spectra of the record's pieces, the templates' spectra, and one fused kernel that
-// correlates every template of a group with every piece and evaluates the distance bound,
-// bucket minima and threshold candidates straight from shared memory. TREMOR's FFT branch
-// (fft_fallback.hpp:67-117: per piece, the product with the template spectrum, an inverse
-// real FFT, the dot product of each window and the distance filter with an error bound) has
-// this structure; here neither the product spectrum nor the correlation leaves the SM.
+// In-tree FP64 FFT kernels of the FFT branch: the spectra of the record's pieces, the
+// templates' spectra, and one fused kernel that correlates every template of a group with
+// every piece and evaluates the distance bound, bucket minima and threshold candidates
+// straight from shared memory. TREMOR's FFT branch (fft_fallback.hpp:67-117: per piece,
+// the product with the template spectrum, an inverse real FFT, the dot product of each
+// window and the distance filter with an error bound) has this structure; here neither the
+// product spectrum nor the correlation leaves the SM.
 //
-// Pieces: kF2L = 16384 samples starting every kF2S = 8192 samples (shifted by s_p, the
-// centre of the prefix block holding the piece's start, rounded to float). Window
-// j = p kF2S + o (0 <= o < kF2S) of piece p has its dot product at output o + m - 1 of the
-// circular correlation, which does not wrap for m <= kF2L - kF2S + 1.
+// Two piece lengths, both with the step half the length (the window j = p S + o,
+// 0 <= o < S, of piece p has its dot product at output o + m - 1 of the circular
+// correlation, which does not wrap for m <= L - S + 1); each piece is shifted by s_p, the
+// centre of the prefix block holding its start, rounded to float:
+//   L = 16384, S = 8192  (kF2*): templates of up to 8192 samples;
+//   L = 32768, S = 16384 (kF3*): templates of up to 16384 samples.
 //
-// Real transforms of length L = 16384 go through complex ones of N = L / 2 = 8192 points:
+// Real transforms of length L go through complex ones of N = L / 2 points:
 //   forward: z[n] = x[2n] + i x[2n+1], Z = FFT_N(z),
 //            X[k] = (Z[k] + conj Z[N-k]) / 2 - i e^{-2 pi i k / L} (Z[k] - conj Z[N-k]) / 2;
 //   inverse: for a Hermitian spectrum V (V[k] = X[k] Y[k]),
 //            C[k] = (V[k] + conj V[N-k]) + i e^{2 pi i k / L} (V[k] - conj V[N-k]),
 //            c = IFFT_N(C) (unnormalised), out[2n] = Re c[n], out[2n+1] = Im c[n],
 //            and out / L is the circular correlation of x with the reversed template.
-// The complex FFTs are Stockham radix-16, 16, 16 then 2 (N = 8192; Govindaraju et al.,
-// "High Performance Discrete Fourier Transforms on Graphics Processors", SC 2008): 512
-// threads, each holding 16 points in registers between a pass's shared-memory read and its
-// write, so every pass works in place; the buffer is padded by one point per 16 so that
-// the first pass's stride-16 writes hit distinct banks. The final radix-2 pass of the
-// inverse is evaluated where its outputs are read (by the distance epilogue).
+// Every complex transform is built from 8192-point ones, Stockham radix-16, 16, 16 then 2
+// (Govindaraju et al., "High Performance Discrete Fourier Transforms on Graphics
+// Processors", SC 2008): 512 threads, each holding 16 points in registers between a pass's
+// shared-memory read and its write, so every pass works in place; the buffer is padded by
+// one point per 16 so that the first pass's stride-16 writes hit distinct banks. The final
+// radix-2 pass of an inverse is evaluated where its outputs are read (by the distance
+// epilogue). For N = 16384 the forward transform splits z into its even and odd points
+// (Z[k] = E[k] + W^k O[k], Z[k + 8192] = E[k] - W^k O[k], W = e^{-2 pi i / 16384}); the
+// inverse splits C the other way (a[n] = C[n] + C[n + 8192] gives c[2k], b[n] = (C[n] -
+// C[n + 8192]) e^{2 pi i n / 16384} gives c[2k + 1]), two 8192-point passes per piece.
 //
-// Twiddles: e^{2 pi i e / 16384} = R2[e >> 7] R1[e & 127] from two 128-entry tables
-// computed on the host in extended precision and rounded (error <= 4u with u = 2^-53,
-// the product included); a pass's powers w^r (r = 1..15) by repeated multiplication
-// (error <= 7 r u <= 105u). Error of an output (Higham, Accuracy and Stability of
-// Numerical Algorithms, Thm 24.2, ||fl(FFT x) - FFT x||_2 <= t eta / (1 - t eta) ||FFT x||_2,
-// eta = mu + gamma_4 (sqrt 2 + mu), mu the twiddle error): with mu = 105u and t = 16 (13
-// complex stages plus the real-transform packing) and a factor 10 for the radix-16 and
-// packing arithmetic, kappa = 10 x 16 x 111u; then, as for the length-32768 pieces
-// (tm_fft.cu), every correlation output is within kappa ||x - s_p||_2 ||q||_2 (2 sqrt m +
+// Twiddles: e^{2 pi i e / 32768} = R2[e >> 7] R1[e & 127] from tables of 128 and 256 entries
+// computed on the host in extended precision and rounded (error <= 4u with u = 2^-53, the
+// product included); a pass's powers w^r (r = 1..15) by repeated multiplication (error
+// <= 7 r u <= 105u). Error of an output (Higham, Accuracy and Stability of Numerical
+// Algorithms, Thm 24.2, ||fl(FFT x) - FFT x||_2 <= t eta / (1 - t eta) ||FFT x||_2,
+// eta = mu + gamma_4 (sqrt 2 + mu), mu the twiddle error): with mu = 105u, t = log2 L + 2
+// (the complex stages plus the real-transform packing and the even/odd split) and a factor
+// 10 for the radix-16 and packing arithmetic, kappa = 10 t 111u. With X = FFT(x - s_p),
+// Y = FFT(reversed q), ||X||_2 = sqrt(L) ||x - s_p||_2, ||Y||_inf <= ||q||_1 <= sqrt(m)
+// ||q||_2: ||fl(X) fl(Y) - X Y||_2 <= kappa sqrt(L) ||x - s_p|| ||q|| (sqrt m + sqrt L)
+// (+ rounding), and the inverse adds kappa ||X Y||_2 <= kappa sqrt(L) ||x - s_p|| sqrt(m)
+// ||q||, so every correlation output is within kappa ||x - s_p||_2 ||q||_2 (2 sqrt m +
 // sqrt L) of the exact one.
 #include <cmath>
 
@@ -44,9 +53,12 @@
 namespace tmb {
 
 constexpr int kF2T = 512;                        // threads per block
-constexpr int kF2Buf = kF2N + kF2N / 16 + 16;    // padded complex entries of the work buffer
+constexpr int kFPts = 8192;                      // points of the in-shared-memory transforms
+constexpr int kF2Buf = kFPts + kFPts / 16 + 16;  // padded complex entries of the work buffer
+constexpr int kFRoots = 384;                     // twiddle table entries (R1 then R2)
 constexpr double kF2Kappa = 10.0 * 16.0 * 111.0 * 1.1102230246251565e-16;
-constexpr size_t kF2Smem = sizeof(double2) * (size_t)(kF2Buf + 256);
+constexpr double kF3Kappa = 10.0 * 17.0 * 111.0 * 1.1102230246251565e-16;
+constexpr size_t kF2Smem = sizeof(double2) * (size_t)(kF2Buf + kFRoots);
 
 __device__ __forceinline__ int pidx(int i) { return i + (i >> 4); }
 
@@ -63,7 +75,7 @@ template <int S> __device__ __forceinline__ double2 mul_si(double2 a)
     return S > 0 ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
 }
 
-// e^{S 2 pi i e / 16384}, 0 <= e < 16384, from the shared tables R (R1 then R2).
+// e^{S 2 pi i e / 32768}, 0 <= e < 32768, from the shared tables R (R1 then R2).
 template <int S> __device__ __forceinline__ double2 root(const double2 *R, int e)
 {
     const double2 w = cmul(R[128 + (e >> 7)], R[e & 127]);
@@ -128,7 +140,7 @@ template <int S> __device__ __forceinline__ void pass16(double2 *buf, const doub
     const int k = j & (Ns - 1);
     if (Ns > 1)
     {
-        const double2 w1 = root<S>(R, k * (1024 / Ns)); // W^k, W = e^{S 2 pi i / (16 Ns)}
+        const double2 w1 = root<S>(R, k * (2048 / Ns)); // W^k, W = e^{S 2 pi i / (16 Ns)}
         double2 w = w1;
 #pragma unroll
         for (int r = 1; r < 16; r++)
@@ -160,14 +172,83 @@ template <int S> __device__ __forceinline__ void fft8192_r16(double2 *buf, const
 template <int S> __device__ __forceinline__ double2 final_out(const double2 *buf, const double2 *R, int i)
 {
     const int i0 = i & 4095;
-    const double2 a = buf[pidx(i0)], b = cmul(buf[pidx(i0 + 4096)], root<S>(R, 2 * i0));
+    const double2 a = buf[pidx(i0)], b = cmul(buf[pidx(i0 + 4096)], root<S>(R, 4 * i0));
     return i < 4096 ? cadd(a, b) : csub(a, b);
 }
 
 __device__ __forceinline__ void load_roots(double2 *R, const double2 *roots)
 {
-    for (int i = threadIdx.x; i < 256; i += blockDim.x)
+    for (int i = threadIdx.x; i < kFRoots; i += blockDim.x)
         R[i] = roots[i];
+}
+
+// The shared epilogue of both correlation kernels for one window o of piece p (global
+// start g = piece_w + o): distance and bound from the dot product (taken from the transform
+// in shared memory by `dot_of`, evaluated only for windows that are searched), then kNN
+// bucket minima or threshold candidates. Every lane of the warp must call it; the warp's
+// windows lie within 64 consecutive positions, so in at most two buckets.
+template <class DotOf>
+__device__ __forceinline__ void corr_window(const Fft2Args &a, const TemplParam &P, int t, bool in_piece,
+                                            uint64_t g, float shift, float e_dot, int lane, DotOf dot_of)
+{
+    const bool in_range = in_piece && g >= a.w0 && g - a.w0 < P.wcount;
+    const uint32_t jr = in_range ? (uint32_t)(g - a.w0) : 0u;
+    const bool ok = in_range && a.raw[g] != kMissing && a.run[g] < (uint16_t)min(P.m, 65535);
+    float up = inf_f(), lo = inf_f();
+    bool hit = false;
+    if (ok)
+    {
+        WindowStats ws;
+        if (window_prefix_stats(a.pv, a.pv.Q[g], a.pv.Q[g + (uint64_t)P.m], g, P.m, P.inv_m, ws) == 0)
+        {
+            const double dot = dot_of();
+            float d, e;
+            fast_distance_mixed(P, P.a1_main, (float)dot, ws.mu, ws.iv, shift, stats_error(ws, P.m, P.qs, P.s1), d,
+                                e);
+            e += 2.0f * e_dot * ws.iv * 1.01f;
+            if (a.dbg_d != nullptr)
+            {
+                a.dbg_d[(size_t)t * a.W + jr] = d;
+                a.dbg_e[(size_t)t * a.W + jr] = e;
+            }
+            up = d + e;
+            lo = d - e;
+            hit = lo <= P.thr_ed;
+        }
+        else
+        {
+            lo = -inf_f();
+            hit = true;
+        }
+    }
+    if (P.mode == TM_MODE_KNN)
+    {
+        const uint32_t bucket = jr / kBucket;
+        const unsigned act = __ballot_sync(0xffffffffu, in_range);
+        if (act == 0u)
+            return;
+        const uint32_t b0 = __shfl_sync(0xffffffffu, bucket, __ffs(act) - 1);
+        const unsigned same = __ballot_sync(0xffffffffu, in_range && bucket == b0);
+        const unsigned other = act & ~same;
+        const uint32_t ku = float_key(up), kl = float_key(lo);
+        const uint32_t u0 = __reduce_min_sync(0xffffffffu, same & (1u << lane) ? ku : 0xffffffffu);
+        const uint32_t l0 = __reduce_min_sync(0xffffffffu, same & (1u << lane) ? kl : 0xffffffffu);
+        const uint32_t u1 = __reduce_min_sync(0xffffffffu, other & (1u << lane) ? ku : 0xffffffffu);
+        const uint32_t l1 = __reduce_min_sync(0xffffffffu, other & (1u << lane) ? kl : 0xffffffffu);
+        const uint32_t none = float_key(inf_f());
+        if (lane == __ffs(act) - 1 && (u0 != none || l0 != none) && u0 != 0xffffffffu)
+        {
+            atomicMin(&a.bmin_u[(size_t)t * a.nb + b0], u0);
+            atomicMin(&a.bmin_l[(size_t)t * a.nb + b0], l0);
+        }
+        if (other != 0u && lane == __ffs(other) - 1 && (u1 != none || l1 != none))
+        {
+            atomicMin(&a.bmin_u[(size_t)t * a.nb + bucket], u1);
+            atomicMin(&a.bmin_l[(size_t)t * a.nb + bucket], l1);
+        }
+    }
+    else
+        emit_candidates(hit ? 1u : 0u, lane, (uint32_t)t, jr, a.cand, a.cand_count, a.cand_cap);
 }
 
 // Forward real FFT of one piece of the record (blockIdx.x < pieces) or one template row
@@ -223,7 +304,7 @@ __global__ void __launch_bounds__(kF2T, 1) k_fft2_forward(const float *__restric
     // the radix-2 pass, in place (each thread owns the pairs (i, i + 4096) it touches)
     for (int i = threadIdx.x; i < 4096; i += kF2T)
     {
-        const double2 a = buf[pidx(i)], b = cmul(buf[pidx(i + 4096)], root<-1>(R, 2 * i));
+        const double2 a = buf[pidx(i)], b = cmul(buf[pidx(i + 4096)], root<-1>(R, 4 * i));
         buf[pidx(i)] = cadd(a, b);
         buf[pidx(i + 4096)] = csub(a, b);
     }
@@ -236,7 +317,7 @@ __global__ void __launch_bounds__(kF2T, 1) k_fft2_forward(const float *__restric
         const double2 E = make_double2(0.5 * (A.x + Bc.x), 0.5 * (A.y + Bc.y));
         const double2 D = csub(A, Bc);
         const double2 O = make_double2(0.5 * D.y, -0.5 * D.x); // -i (A - B) / 2
-        const double2 w = root<-1>(R, k);                       // e^{-2 pi i k / L}
+        const double2 w = root<-1>(R, 2 * k);                   // e^{-2 pi i k / L}
         o[k] = cadd(E, cmul(O, w));
         if (k == 0)
             o[kF2N] = csub(E, O); // twiddle e^{-i pi} = -1
@@ -300,7 +381,7 @@ __global__ void __launch_bounds__(kF2T, 1) k_fft2_corr(const Fft2Args a)
             {
                 const int kn = kF2N - k;
                 const double2 Vk = cmul(X[k], Y[k]), Vn = cmul(X[kn], Y[kn]);
-                const double2 w = root<1>(R, k); // e^{2 pi i k / L}
+                const double2 w = root<1>(R, 2 * k); // e^{2 pi i k / L}
                 // C[k] = E + i O with E = Vk + conj Vn, O = w (Vk - conj Vn); C[N - k] = conj E + i conj O
                 const double2 E = cadd(Vk, conj2(Vn));
                 const double2 O = cmul(csub(Vk, conj2(Vn)), w);
@@ -321,86 +402,230 @@ __global__ void __launch_bounds__(kF2T, 1) k_fft2_corr(const Fft2Args a)
             for (int it = 0; it < kF2S / kF2T; it++)
             {
                 const uint32_t o = (uint32_t)(it * kF2T) + threadIdx.x;
-                const uint64_t g = piece_w + o;
-                const bool in_range = g >= a.w0 && g - a.w0 < P.wcount;
-                const uint32_t jr = in_range ? (uint32_t)(g - a.w0) : 0u;
-                bool ok = in_range && a.raw[g] != kMissing && a.run[g] < (uint16_t)min(P.m, 65535);
-                float up = inf_f(), lo = inf_f();
-                bool hit = false;
-                if (ok)
-                {
-                    WindowStats ws;
-                    if (window_prefix_stats(a.pv, a.pv.Q[g], a.pv.Q[g + (uint64_t)P.m], g, P.m, P.inv_m, ws) == 0)
-                    {
-                        const int nn = (int)o + P.m - 1;
-                        const double2 c = final_out<1>(buf, R, nn >> 1);
-                        const double dot = ((nn & 1) ? c.y : c.x) * inv_l;
-                        float d, e;
-                        fast_distance_mixed(P, P.a1_main, (float)dot, ws.mu, ws.iv, shift,
-                                            stats_error(ws, P.m, P.qs, P.s1), d, e);
-                        e += 2.0f * e_dot * ws.iv * 1.01f;
-                        if (a.dbg_d != nullptr)
-                        {
-                            a.dbg_d[(size_t)t * a.W + jr] = d;
-                            a.dbg_e[(size_t)t * a.W + jr] = e;
-                        }
-                        up = d + e;
-                        lo = d - e;
-                        hit = lo <= P.thr_ed;
-                    }
-                    else
-                    {
-                        lo = -inf_f();
-                        hit = true;
-                    }
-                }
-                if (P.mode == TM_MODE_KNN)
-                {
-                    // bucket minima: a warp's 32 windows lie in at most two buckets
-                    const uint32_t bucket = jr / kBucket;
-                    const unsigned act = __ballot_sync(0xffffffffu, in_range);
-                    if (act == 0u)
-                        continue;
-                    const uint32_t b0 = __shfl_sync(0xffffffffu, bucket, __ffs(act) - 1);
-                    const unsigned same = __ballot_sync(0xffffffffu, in_range && bucket == b0);
-                    const unsigned other = act & ~same;
-                    const uint32_t ku = float_key(up), kl = float_key(lo);
-                    const uint32_t u0 = __reduce_min_sync(0xffffffffu, same & (1u << lane) ? ku : 0xffffffffu);
-                    const uint32_t l0 = __reduce_min_sync(0xffffffffu, same & (1u << lane) ? kl : 0xffffffffu);
-                    const uint32_t u1 = __reduce_min_sync(0xffffffffu, other & (1u << lane) ? ku : 0xffffffffu);
-                    const uint32_t l1 = __reduce_min_sync(0xffffffffu, other & (1u << lane) ? kl : 0xffffffffu);
-                    const uint32_t none = float_key(inf_f());
-                    if (lane == __ffs(act) - 1 && (u0 != none || l0 != none) && u0 != 0xffffffffu)
-                    {
-                        atomicMin(&a.bmin_u[(size_t)t * a.nb + b0], u0);
-                        atomicMin(&a.bmin_l[(size_t)t * a.nb + b0], l0);
-                    }
-                    if (other != 0u && lane == __ffs(other) - 1 && (u1 != none || l1 != none))
-                    {
-                        atomicMin(&a.bmin_u[(size_t)t * a.nb + bucket], u1);
-                        atomicMin(&a.bmin_l[(size_t)t * a.nb + bucket], l1);
-                    }
-                }
-                else
-                    emit_candidates(hit ? 1u : 0u, lane, (uint32_t)t, jr, a.cand, a.cand_count, a.cand_cap);
+                corr_window(a, P, t, true, piece_w + o, shift, e_dot, lane, [&]() {
+                    const int nn = (int)o + P.m - 1;
+                    const double2 c = final_out<1>(buf, R, nn >> 1);
+                    return ((nn & 1) ? c.y : c.x) * inv_l;
+                });
             }
         }
     }
 }
 
-void fft2_roots(double2 *host256)
+// Forward real FFT of length kF3L of pieces (item i: piece p0 + i) or template rows (item i:
+// rows[i], reversed and zero-padded), into out[item * kF3H ..]: persistent blocks, the
+// even-point transform E parked in the block's slice of `scratch` (kFPts points) while the
+// odd-point one O stays in shared memory, then the two combined and unpacked.
+__global__ void __launch_bounds__(kF2T, 1) k_fft3_forward(const float *__restrict__ clean, uint64_t n,
+                                                         const double *__restrict__ centres, uint32_t p0,
+                                                         uint32_t count, const float *__restrict__ q,
+                                                         const TemplParam *__restrict__ tp, const int *__restrict__ rows,
+                                                         const double2 *__restrict__ roots, double2 *__restrict__ out,
+                                                         double *__restrict__ shifts, double *__restrict__ norms,
+                                                         double2 *__restrict__ scratch)
 {
-    // R1[a] = e^{2 pi i a / 16384}, R2[b] = e^{2 pi i 128 b / 16384}, in extended precision
+    extern __shared__ double2 sm2[];
+    double2 *buf = sm2, *R = sm2 + kF2Buf;
+    __shared__ double part[kF2T / 32];
+    load_roots(R, roots);
+    double2 *Es = scratch + (size_t)blockIdx.x * kFPts;
+    const bool templ = q != nullptr;
+    for (uint32_t item = blockIdx.x; item < count; item += gridDim.x)
+    {
+        double s = 0.0, sq = 0.0;
+        uint64_t start = 0;
+        const float *qt = nullptr;
+        int m = 0;
+        if (templ)
+        {
+            const TemplParam &p = tp[rows[item]];
+            qt = q + p.q_offset;
+            m = p.m;
+        }
+        else
+        {
+            start = (uint64_t)(p0 + item) * kF3S;
+            s = (double)(float)centres[start >> kPrefixBlockLog];
+        }
+        for (int half = 0; half < 2; half++)
+        {
+            __syncthreads(); // buf and Es are free (the previous half's or item's readers are done)
+            for (int i = threadIdx.x; i < kFPts; i += kF2T)
+            {
+                // point 2i + half of z: samples 4i + 2 half and 4i + 2 half + 1
+                const uint64_t t0 = 4 * (uint64_t)i + 2 * (uint64_t)half;
+                double va, vb;
+                if (templ)
+                {
+                    va = t0 < (uint64_t)m ? (double)qt[m - 1 - (int)t0] : 0.0;
+                    vb = t0 + 1 < (uint64_t)m ? (double)qt[m - 2 - (int)t0] : 0.0;
+                }
+                else
+                {
+                    const uint64_t g = start + t0;
+                    va = g < n ? (double)clean[g] - s : 0.0;
+                    vb = g + 1 < n ? (double)clean[g + 1] - s : 0.0;
+                    sq = fma(va, va, sq);
+                    sq = fma(vb, vb, sq);
+                }
+                buf[pidx(i)] = make_double2(va, vb);
+            }
+            __syncthreads();
+            fft8192_r16<-1>(buf, R);
+            for (int i = threadIdx.x; i < 4096; i += kF2T)
+            {
+                const double2 x0 = buf[pidx(i)], x1 = cmul(buf[pidx(i + 4096)], root<-1>(R, 4 * i));
+                buf[pidx(i)] = cadd(x0, x1);
+                buf[pidx(i + 4096)] = csub(x0, x1);
+            }
+            __syncthreads();
+            if (half == 0)
+                for (int k = threadIdx.x; k < kFPts; k += kF2T)
+                    Es[k] = buf[pidx(k)];
+        }
+        __syncthreads(); // Es written, buf holds O
+        // Z[k] = E[k] + W^k O[k] (k < 8192), Z[k + 8192] = E[k] - W^k O[k], W^k = e^{-2 pi i k / 16384}
+        auto Z = [&](int k) -> double2 {
+            const int k0 = k & (kFPts - 1);
+            const double2 wo = cmul(buf[pidx(k0)], root<-1>(R, 2 * k0));
+            return k < kFPts ? cadd(Es[k0], wo) : csub(Es[k0], wo);
+        };
+        constexpr int N = kF3N;
+        double2 *o = out + (size_t)item * kF3H;
+        for (int k = threadIdx.x; k <= N / 2; k += kF2T)
+        {
+            const double2 A = Z(k), Bc = conj2(Z(k == 0 ? 0 : N - k));
+            const double2 E = make_double2(0.5 * (A.x + Bc.x), 0.5 * (A.y + Bc.y));
+            const double2 D = csub(A, Bc);
+            const double2 O = make_double2(0.5 * D.y, -0.5 * D.x);
+            const double2 w = root<-1>(R, k); // e^{-2 pi i k / 32768}
+            o[k] = cadd(E, cmul(O, w));
+            if (k == 0)
+                o[N] = csub(E, O);
+            else if (k < N / 2)
+            {
+                const double2 A2 = conj2(Bc), B2c = conj2(A);
+                const double2 E2 = make_double2(0.5 * (A2.x + B2c.x), 0.5 * (A2.y + B2c.y));
+                const double2 D2 = csub(A2, B2c);
+                const double2 O2 = make_double2(0.5 * D2.y, -0.5 * D2.x);
+                o[N - k] = csub(E2, cmul(O2, conj2(w)));
+            }
+        }
+        if (!templ)
+        {
+            for (int off = 16; off > 0; off >>= 1)
+                sq += __shfl_down_sync(0xffffffffu, sq, off);
+            if ((threadIdx.x & 31) == 0)
+                part[threadIdx.x >> 5] = sq;
+            __syncthreads();
+            if (threadIdx.x == 0)
+            {
+                double tot = 0.0;
+                for (int w = 0; w < kF2T / 32; w++)
+                    tot += part[w];
+                shifts[p0 + item] = s;
+                norms[p0 + item] = sqrt(tot) * (1.0 + 1e-12);
+            }
+        }
+    }
+}
+
+// The fused correlation for pieces of kF3L samples (templates of up to kF3S samples): per
+// piece and template, two halves h = 0, 1: the product with the template spectrum, the
+// real-transform packing and the even/odd split in one step (h = 0: a[n] = C[n] + C[n + 8192];
+// h = 1: b[n] = (C[n] - C[n + 8192]) e^{2 pi i n / 16384}), the radix-16 passes, then the
+// windows whose output index has c index parity h (out[n0] with (n0 >> 1) & 1 == h, two of
+// every four consecutive windows), each from the final radix-2 pass.
+__global__ void __launch_bounds__(kF2T, 1) k_fft3_corr(const Fft2Args a)
+{
+    extern __shared__ double2 sm2[];
+    double2 *buf = sm2, *R = sm2 + kF2Buf;
+    load_roots(R, a.roots);
+    const int lane = threadIdx.x & 31;
+    const double inv_l = 1.0 / (double)kF3L;
+    constexpr int N = kF3N;
+    for (uint32_t pi = blockIdx.x; pi < a.p_count; pi += gridDim.x)
+    {
+        const uint32_t p = a.p_first + pi;
+        const double2 *X = a.X + (size_t)p * kF3H;
+        const float shift = (float)a.shifts[p];
+        const double norm = a.norms[p];
+        for (int ti = 0; ti < a.nrows; ti++)
+        {
+            const int t = a.rows[ti];
+            const TemplParam P = a.tp[t];
+            const uint64_t piece_w = (uint64_t)p * kF3S;
+            if (piece_w + kF3S <= a.w0 || piece_w >= a.w0 + (uint64_t)P.wcount)
+                continue;
+            const double2 *Y = a.Y + (size_t)ti * kF3H;
+            const double sm_ = sqrt((double)P.m);
+            const float e_dot = (float)(kF3Kappa * norm * sm_ * (2.0 * sm_ + sqrt((double)kF3L)) * 1.01);
+            const int base = P.m - 1;
+            for (int h = 0; h < 2; h++)
+            {
+                __syncthreads(); // the previous half's epilogue has read buf
+                for (int u = threadIdx.x; u <= kFPts / 2; u += kF2T)
+                {
+                    // C[u], C[N - u] from V[u], V[N - u]; C[u + 8192], C[8192 - u] from V[u + 8192], V[8192 - u]
+                    const double2 V1 = cmul(X[u], Y[u]), V1n = cmul(X[N - u], Y[N - u]);
+                    const double2 E1 = cadd(V1, conj2(V1n)), O1 = cmul(csub(V1, conj2(V1n)), root<1>(R, u));
+                    const double2 Cu = cadd(E1, mul_si<1>(O1)), CNu = cadd(conj2(E1), mul_si<1>(conj2(O1)));
+                    const int u2 = u + kFPts;
+                    const double2 V2 = cmul(X[u2], Y[u2]), V2n = cmul(X[N - u2], Y[N - u2]);
+                    const double2 E2 = cadd(V2, conj2(V2n)), O2 = cmul(csub(V2, conj2(V2n)), root<1>(R, u2));
+                    const double2 Cv = cadd(E2, mul_si<1>(O2)), C8u = cadd(conj2(E2), mul_si<1>(conj2(O2)));
+                    if (h == 0)
+                    {
+                        buf[pidx(u)] = cadd(Cu, Cv);
+                        if (u > 0 && u < kFPts / 2)
+                            buf[pidx(kFPts - u)] = cadd(C8u, CNu);
+                    }
+                    else
+                    {
+                        buf[pidx(u)] = cmul(csub(Cu, Cv), root<1>(R, 2 * u));
+                        if (u > 0 && u < kFPts / 2)
+                            buf[pidx(kFPts - u)] = cmul(csub(C8u, CNu), root<1>(R, 2 * (kFPts - u)));
+                    }
+                }
+                __syncthreads();
+                fft8192_r16<1>(buf, R);
+                // windows of this half: v -> n0 = 4 ((v >> 1) + (base >> 2)) + 2 h + (v & 1), o = n0 - base
+                for (int it = 0; it < 17; it++)
+                {
+                    const int v = it * kF2T + (int)threadIdx.x;
+                    const int n0 = 4 * ((v >> 1) + (base >> 2)) + 2 * h + (v & 1);
+                    const int o = n0 - base;
+                    const bool in_piece = o >= 0 && o < kF3S;
+                    const uint64_t g = piece_w + (uint64_t)(in_piece ? o : 0);
+                    corr_window(a, P, t, in_piece, g, shift, e_dot, lane, [&]() {
+                        const double2 c = final_out<1>(buf, R, n0 >> 2);
+                        return ((n0 & 1) ? c.y : c.x) * inv_l;
+                    });
+                }
+            }
+        }
+    }
+}
+
+void fft_roots(double2 *host384)
+{
+    // R1[a] = e^{2 pi i a / 32768} (a < 128), R2[b] = e^{2 pi i 128 b / 32768} (b < 256), in
+    // extended precision
     const long double two_pi = 6.283185307179586476925286766559005768L;
     for (int a = 0; a < 128; a++)
     {
-        const long double t1 = two_pi * (long double)a / 16384.0L, t2 = two_pi * (long double)(128 * a) / 16384.0L;
-        host256[a] = make_double2((double)cosl(t1), (double)sinl(t1));
-        host256[128 + a] = make_double2((double)cosl(t2), (double)sinl(t2));
+        const long double t = two_pi * (long double)a / 32768.0L;
+        host384[a] = make_double2((double)cosl(t), (double)sinl(t));
+    }
+    for (int b = 0; b < 256; b++)
+    {
+        const long double t = two_pi * (long double)(128 * b) / 32768.0L;
+        host384[128 + b] = make_double2((double)cosl(t), (double)sinl(t));
     }
 }
 
 uint32_t fft2_pieces(uint64_t n) { return (uint32_t)((n + kF2S - 1) / kF2S); }
+uint32_t fft3_pieces(uint64_t n) { return (uint32_t)((n + kF3S - 1) / kF3S); }
 
 cudaError_t launch_fft2_pieces(const float *clean, uint64_t n, const double *centres, uint32_t p0, uint32_t count,
                                const double2 *roots, double2 *X, double *shifts, double *norms, cudaStream_t s)
@@ -426,6 +651,36 @@ cudaError_t launch_fft2_corr(const Fft2Args &a, int sms, cudaStream_t s)
     cudaFuncSetAttribute(k_fft2_corr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kF2Smem);
     if (a.p_count > 0 && a.nrows > 0)
         k_fft2_corr<<<(unsigned)std::min<uint32_t>(a.p_count, (uint32_t)sms), kF2T, kF2Smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fft3_pieces(const float *clean, uint64_t n, const double *centres, uint32_t p0, uint32_t count,
+                               const double2 *roots, double2 *X, double *shifts, double *norms, double2 *scratch,
+                               int blocks, cudaStream_t s)
+{
+    cudaFuncSetAttribute(k_fft3_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kF2Smem);
+    if (count > 0)
+        k_fft3_forward<<<(unsigned)std::min<uint32_t>(count, (uint32_t)blocks), kF2T, kF2Smem, s>>>(
+            clean, n, centres, p0, count, nullptr, nullptr, nullptr, roots, X + (size_t)p0 * kF3H, shifts, norms,
+            scratch);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fft3_templates(const float *q, const TemplParam *tp, const int *rows, int nrows,
+                                  const double2 *roots, double2 *Y, double2 *scratch, int blocks, cudaStream_t s)
+{
+    cudaFuncSetAttribute(k_fft3_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kF2Smem);
+    if (nrows > 0)
+        k_fft3_forward<<<(unsigned)std::min<int>(nrows, blocks), kF2T, kF2Smem, s>>>(
+            nullptr, 0, nullptr, 0, (uint32_t)nrows, q, tp, rows, roots, Y, nullptr, nullptr, scratch);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fft3_corr(const Fft2Args &a, int sms, cudaStream_t s)
+{
+    cudaFuncSetAttribute(k_fft3_corr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kF2Smem);
+    if (a.p_count > 0 && a.nrows > 0)
+        k_fft3_corr<<<(unsigned)std::min<uint32_t>(a.p_count, (uint32_t)sms), kF2T, kF2Smem, s>>>(a);
     return cudaGetLastError();
 }
 

@@ -365,7 +365,7 @@ size_t plan_fft_split(const tm_ctx *ctx, const tm_request *reqs, const std::vect
     if (n == 0 || ctx->kernel == TM_KERNEL_FP32 || !tmb::umma_supported(0, 0, 0))
         return 0;
     for (int i : sorted_idx)
-        if (reqs[i].m > tmb::kFftS)
+        if (reqs[i].m > tmb::kFftMaxM)
             return 0;
     if (ctx->tiles == TM_TILES_FFT)
         return n;

@@ -501,115 +501,110 @@ void execute_group(tm_ctx *ctx, Lane &L, GroupPlan &g, tm_result &res)
     });
 }
 
-// Spectra of the record's overlapping pieces (tm_fft.cu), their shifts and norms: built
-// once per context (under a lock: serving workers may ask at once).
-void ensure_fft(tm_ctx *ctx, Lane &L)
+// Spectra of the record's pieces for the FFT branch (tm_fftk.cu), their shifts and norms,
+// and the twiddle tables: built once per context and piece length (long = pieces of 32768
+// samples every 16384, else 16384 every 8192), under a lock (serving workers may ask at once).
+static void ensure_fft(tm_ctx *ctx, Lane &L, bool long_pieces)
 {
     std::lock_guard<std::mutex> lk(ctx->fft_mu);
-    if (ctx->fft_ready)
+    if (long_pieces ? ctx->fft3_ready : ctx->fft2_ready)
         return;
     ensure_prefix(ctx, L);
     cudaStream_t s = L.stream;
-    const uint32_t P = tmb::fft_pieces(ctx->n);
-    const uint32_t B = tmb::kFftBatch;
-    const uint64_t Ppad = (static_cast<uint64_t>(P) + B - 1) / B * B; // whole batches; extra pieces stay zero
-    ctx->fft_X.reserve(sizeof(double2) * Ppad * tmb::kFftH);
-    ctx->fft_shift.reserve(sizeof(double) * Ppad);
-    ctx->fft_norm.reserve(sizeof(double) * Ppad);
-    TM_CUDA(cudaMemsetAsync(ctx->fft_X.p, 0, sizeof(double2) * Ppad * tmb::kFftH, s));
-    TM_CUDA(cudaMemsetAsync(ctx->fft_shift.p, 0, sizeof(double) * Ppad, s));
-    TM_CUDA(cudaMemsetAsync(ctx->fft_norm.p, 0, sizeof(double) * Ppad, s));
-    DevBuf pieces;
-    pieces.reserve(sizeof(double) * static_cast<size_t>(B) * tmb::kFftL);
-    cufftHandle plan;
-    int len = tmb::kFftL;
-    TM_CUFFT(cufftPlanMany(&plan, 1, &len, nullptr, 1, tmb::kFftL, nullptr, 1, tmb::kFftH, CUFFT_D2Z,
-                           static_cast<int>(B)));
-    std::unique_ptr<cufftHandle, void (*)(cufftHandle *)> hold(&plan, [](cufftHandle *h) { cufftDestroy(*h); });
-    TM_CUFFT(cufftSetStream(plan, s));
-    for (uint32_t p0 = 0; p0 < P; p0 += B)
+    if (ctx->fft_roots.p == nullptr)
     {
-        const uint32_t cnt = std::min<uint32_t>(B, P - p0);
-        if (cnt < B)
-            TM_CUDA(cudaMemsetAsync(pieces.p, 0, sizeof(double) * static_cast<size_t>(B) * tmb::kFftL, s));
-        TM_CUDA(tmb::launch_fft_gather(ctx->clean.as<float>(), ctx->n, ctx->pcen.as<double>(), p0, cnt,
-                                       pieces.as<double>(), ctx->fft_shift.as<double>(), ctx->fft_norm.as<double>(),
-                                       s));
-        TM_CUFFT(cufftExecD2Z(plan, pieces.as<cufftDoubleReal>(),
-                              reinterpret_cast<cufftDoubleComplex *>(ctx->fft_X.as<double2>() +
-                                                                     static_cast<size_t>(p0) * tmb::kFftH)));
-        count_launch(L, 2);
+        std::vector<double2> roots(tmb::kFftRoots);
+        tmb::fft_roots(roots.data());
+        ctx->fft_roots.reserve(sizeof(double2) * tmb::kFftRoots);
+        TM_CUDA(cudaMemcpyAsync(ctx->fft_roots.p, roots.data(), sizeof(double2) * tmb::kFftRoots,
+                                cudaMemcpyHostToDevice, s));
+        int sms = 0;
+        TM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+        ctx->sms = sms;
+        ctx->fft_scratch.reserve(sizeof(double2) * static_cast<size_t>(sms) * tmb::kFftScratchPts);
     }
-    TM_CUDA(cudaStreamSynchronize(s));
-    pieces.release();
-    ctx->fft_P = P;
-    ctx->fft_ready = true;
-}
-
-// Spectra of the record's pieces of 16384 samples every 8192 for the fused FFT branch
-// (tm_fftk.cu), their shifts and norms, and the twiddle tables: built once per context.
-void ensure_fft2(tm_ctx *ctx, Lane &L)
-{
-    std::lock_guard<std::mutex> lk(ctx->fft_mu);
-    if (ctx->fft2_ready)
-        return;
-    ensure_prefix(ctx, L);
-    cudaStream_t s = L.stream;
-    const uint32_t P = tmb::fft2_pieces(ctx->n);
-    ctx->fft2_X.reserve(sizeof(double2) * static_cast<size_t>(P) * tmb::kF2H);
-    ctx->fft2_shift.reserve(sizeof(double) * P);
-    ctx->fft2_norm.reserve(sizeof(double) * P);
-    ctx->fft2_roots.reserve(sizeof(double2) * 256);
-    std::vector<double2> roots(256);
-    tmb::fft2_roots(roots.data());
-    TM_CUDA(cudaMemcpyAsync(ctx->fft2_roots.p, roots.data(), sizeof(double2) * 256, cudaMemcpyHostToDevice, s));
     const uint32_t B = 16384; // pieces per launch
-    for (uint32_t p0 = 0; p0 < P; p0 += B)
+    if (!long_pieces)
     {
-        TM_CUDA(tmb::launch_fft2_pieces(ctx->clean.as<float>(), ctx->n, ctx->pcen.as<double>(), p0,
-                                        std::min<uint32_t>(B, P - p0), ctx->fft2_roots.as<double2>(),
-                                        ctx->fft2_X.as<double2>(), ctx->fft2_shift.as<double>(),
-                                        ctx->fft2_norm.as<double>(), s));
-        count_launch(L);
+        const uint32_t P = tmb::fft2_pieces(ctx->n);
+        ctx->fft2_X.reserve(sizeof(double2) * static_cast<size_t>(P) * tmb::kF2H);
+        ctx->fft2_shift.reserve(sizeof(double) * P);
+        ctx->fft2_norm.reserve(sizeof(double) * P);
+        for (uint32_t p0 = 0; p0 < P; p0 += B)
+        {
+            TM_CUDA(tmb::launch_fft2_pieces(ctx->clean.as<float>(), ctx->n, ctx->pcen.as<double>(), p0,
+                                            std::min<uint32_t>(B, P - p0), ctx->fft_roots.as<double2>(),
+                                            ctx->fft2_X.as<double2>(), ctx->fft2_shift.as<double>(),
+                                            ctx->fft2_norm.as<double>(), s));
+            count_launch(L);
+        }
+        ctx->fft2_P = P;
+    }
+    else
+    {
+        const uint32_t P = tmb::fft3_pieces(ctx->n);
+        ctx->fft3_X.reserve(sizeof(double2) * static_cast<size_t>(P) * tmb::kF3H);
+        ctx->fft3_shift.reserve(sizeof(double) * P);
+        ctx->fft3_norm.reserve(sizeof(double) * P);
+        for (uint32_t p0 = 0; p0 < P; p0 += B)
+        {
+            TM_CUDA(tmb::launch_fft3_pieces(ctx->clean.as<float>(), ctx->n, ctx->pcen.as<double>(), p0,
+                                            std::min<uint32_t>(B, P - p0), ctx->fft_roots.as<double2>(),
+                                            ctx->fft3_X.as<double2>(), ctx->fft3_shift.as<double>(),
+                                            ctx->fft3_norm.as<double>(), ctx->fft_scratch.as<double2>(), ctx->sms,
+                                            s));
+            count_launch(L);
+        }
+        ctx->fft3_P = P;
     }
     TM_CUDA(cudaStreamSynchronize(s));
-    int sms = 0;
-    TM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
-    ctx->sms = sms;
-    ctx->fft2_P = P;
-    ctx->fft2_ready = true;
+    (long_pieces ? ctx->fft3_ready : ctx->fft2_ready) = true;
 }
 
-// The fused FFT branch for the group's rows `rows` (templates of up to 8192 samples): their
-// spectra, then one persistent launch over the pieces their windows touch.
-static void fft2_contract(tm_ctx *ctx, Lane &L, const GroupPlan &g, const tmb::ScanArgs &a,
-                          const std::vector<int> &rows)
+// The FFT branch for the group's rows `rows` (all of up to 8192 samples, or all longer):
+// their spectra, then one persistent launch over the pieces their windows touch.
+static void fft_contract_rows(tm_ctx *ctx, Lane &L, const GroupPlan &g, const tmb::ScanArgs &a,
+                              const std::vector<int> &rows, bool long_pieces)
 {
-    ensure_fft2(ctx, L);
+    ensure_fft(ctx, L, long_pieces);
     cudaStream_t s = L.stream;
     const int nr = static_cast<int>(rows.size());
-    L.fft2_Y.reserve(sizeof(double2) * static_cast<size_t>(nr) * tmb::kF2H);
-    L.fft2_rows.reserve(sizeof(int) * static_cast<size_t>(nr));
-    TM_CUDA(cudaMemcpyAsync(L.fft2_rows.p, rows.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, s));
-    TM_CUDA(tmb::launch_fft2_templates(g.q.as<float>(), g.tp.as<TemplParam>(), L.fft2_rows.as<int>(), nr,
-                                       ctx->fft2_roots.as<double2>(), L.fft2_Y.as<double2>(), s));
+    const size_t H = long_pieces ? tmb::kF3H : tmb::kF2H;
+    const uint32_t S = long_pieces ? tmb::kF3S : tmb::kF2S;
+    DevBuf &Y = long_pieces ? L.fft3_Y : L.fft2_Y;
+    Y.reserve(sizeof(double2) * static_cast<size_t>(nr) * H);
+    L.fft_rows.reserve(sizeof(int) * static_cast<size_t>(nr));
+    TM_CUDA(cudaMemcpyAsync(L.fft_rows.p, rows.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, s));
+    if (long_pieces)
+    {
+        // the forward transform's scratch is the context's: one launch at a time
+        std::lock_guard<std::mutex> lk(ctx->fft_mu);
+        TM_CUDA(tmb::launch_fft3_templates(g.q.as<float>(), g.tp.as<TemplParam>(), L.fft_rows.as<int>(), nr,
+                                           ctx->fft_roots.as<double2>(), Y.as<double2>(),
+                                           ctx->fft_scratch.as<double2>(), ctx->sms, s));
+        TM_CUDA(cudaStreamSynchronize(s));
+    }
+    else
+        TM_CUDA(tmb::launch_fft2_templates(g.q.as<float>(), g.tp.as<TemplParam>(), L.fft_rows.as<int>(), nr,
+                                           ctx->fft_roots.as<double2>(), Y.as<double2>(), s));
     uint64_t wmax = 0;
     for (int t : rows)
         wmax = std::max<uint64_t>(wmax, g.htp[static_cast<size_t>(t)].wcount);
+    const uint32_t P = long_pieces ? ctx->fft3_P : ctx->fft2_P;
     const uint64_t first = a.w0, last = a.w0 + wmax - 1;
-    const uint32_t pa = static_cast<uint32_t>(first / tmb::kF2S);
-    const uint32_t pb = std::min<uint32_t>(static_cast<uint32_t>(last / tmb::kF2S), ctx->fft2_P - 1);
+    const uint32_t pa = static_cast<uint32_t>(first / S);
+    const uint32_t pb = std::min<uint32_t>(static_cast<uint32_t>(last / S), P - 1);
     tmb::Fft2Args f{};
-    f.X = ctx->fft2_X.as<double2>();
-    f.shifts = ctx->fft2_shift.as<double>();
-    f.norms = ctx->fft2_norm.as<double>();
+    f.X = (long_pieces ? ctx->fft3_X : ctx->fft2_X).as<double2>();
+    f.shifts = (long_pieces ? ctx->fft3_shift : ctx->fft2_shift).as<double>();
+    f.norms = (long_pieces ? ctx->fft3_norm : ctx->fft2_norm).as<double>();
     f.p_first = pa;
     f.p_count = pb >= pa ? pb - pa + 1 : 0;
-    f.Y = L.fft2_Y.as<double2>();
-    f.rows = L.fft2_rows.as<int>();
+    f.Y = Y.as<double2>();
+    f.rows = L.fft_rows.as<int>();
     f.nrows = nr;
     f.tp = g.tp.as<TemplParam>();
-    f.roots = ctx->fft2_roots.as<double2>();
+    f.roots = ctx->fft_roots.as<double2>();
     f.w0 = a.w0;
     f.W = a.W;
     f.pv = tmb::PrefixView{a.P, a.PT, a.PC};
@@ -623,39 +618,13 @@ static void fft2_contract(tm_ctx *ctx, Lane &L, const GroupPlan &g, const tmb::S
     f.cand_cap = a.cand_cap;
     f.dbg_d = a.dbg_d;
     f.dbg_e = a.dbg_e;
-    TM_CUDA(tmb::launch_fft2_corr(f, ctx->sms, s));
+    TM_CUDA(long_pieces ? tmb::launch_fft3_corr(f, ctx->sms, s) : tmb::launch_fft2_corr(f, ctx->sms, s));
     count_launch(L, 2);
 }
 
-// The lane's FFT plans and buffers.
-void ensure_lane_fft(Lane &L)
-{
-    if (L.fft_plans)
-        return;
-    int len = tmb::kFftL;
-    TM_CUFFT(cufftPlan1d(&L.fft_plan1, tmb::kFftL, CUFFT_D2Z, 1));
-    if (cufftPlanMany(&L.fft_planB, 1, &len, nullptr, 1, tmb::kFftH, nullptr, 1, tmb::kFftL, CUFFT_Z2D,
-                      static_cast<int>(tmb::kFftBatch)) != CUFFT_SUCCESS)
-    {
-        cufftDestroy(L.fft_plan1);
-        throw Failure{TM_ERR_CUDA, "cufftPlanMany (inverse FFT batch) failed"};
-    }
-    L.fft_plans = true;
-    TM_CUFFT(cufftSetStream(L.fft_plan1, L.stream));
-    TM_CUFFT(cufftSetStream(L.fft_planB, L.stream));
-    L.fft_y.reserve(sizeof(double) * tmb::kFftL);
-    L.fft_Y.reserve(sizeof(double2) * tmb::kFftH);
-    L.fft_Z.reserve(sizeof(double2) * static_cast<size_t>(tmb::kFftBatch) * tmb::kFftH);
-    L.fft_out.reserve(sizeof(double) * static_cast<size_t>(tmb::kFftBatch) * tmb::kFftL);
-}
-
-// FFT branch of a prepared mixed-length group: each template's correlation with every
-// piece its windows touch, batch by batch, into the same bucket minima and candidate
-// list as the contraction kernels (a: the launch arguments those would get).
 void fft_contract(tm_ctx *ctx, Lane &L, const GroupPlan &g, const tmb::ScanArgs &a)
 {
-    // templates of up to 8192 samples: the fused in-tree kernels; longer ones (up to 16384):
-    // pieces of 32768 samples through the toolkit's FFT
+    // templates of up to 8192 samples: pieces of 16384 samples; longer ones: pieces of 32768
     std::vector<int> short_rows, long_rows;
     for (int t = 0; t < g.T; t++)
     {
@@ -665,55 +634,9 @@ void fft_contract(tm_ctx *ctx, Lane &L, const GroupPlan &g, const tmb::ScanArgs 
         (p.m <= tmb::kF2S ? short_rows : long_rows).push_back(t);
     }
     if (!short_rows.empty())
-        fft2_contract(ctx, L, g, a, short_rows);
-    if (long_rows.empty())
-        return;
-    ensure_fft(ctx, L);
-    ensure_lane_fft(L);
-    cudaStream_t s = L.stream;
-    const uint32_t B = tmb::kFftBatch, P = ctx->fft_P;
-    for (int t : long_rows)
-    {
-        const TemplParam &p = g.htp[t];
-        TM_CUDA(tmb::launch_fft_template(g.q.as<float>() + p.q_offset, p.m, L.fft_y.as<double>(), s));
-        TM_CUFFT(cufftExecD2Z(L.fft_plan1, L.fft_y.as<cufftDoubleReal>(),
-                              reinterpret_cast<cufftDoubleComplex *>(L.fft_Y.p)));
-        const uint64_t first = a.w0, last = a.w0 + p.wcount - 1;
-        const uint32_t pa = static_cast<uint32_t>(first / tmb::kFftS), pb = static_cast<uint32_t>(last / tmb::kFftS);
-        for (uint32_t p0 = pa / B * B; p0 <= pb && p0 < P; p0 += B)
-        {
-            TM_CUDA(tmb::launch_fft_mul(ctx->fft_X.as<double2>() + static_cast<size_t>(p0) * tmb::kFftH,
-                                        L.fft_Y.as<double2>(), L.fft_Z.as<double2>(), B, s));
-            TM_CUFFT(cufftExecZ2D(L.fft_planB, reinterpret_cast<cufftDoubleComplex *>(L.fft_Z.p),
-                                  L.fft_out.as<cufftDoubleReal>()));
-            tmb::FftEpiArgs f{};
-            f.out = L.fft_out.as<double>();
-            f.p0 = p0;
-            f.count = std::min<uint32_t>(B, P - p0);
-            f.t = static_cast<uint32_t>(t);
-            f.p = g.htp[static_cast<size_t>(t)];
-            const double sm = std::sqrt(static_cast<double>(f.p.m));
-            f.e_fac = sm * (2.0 * sm + std::sqrt(static_cast<double>(tmb::kFftL)));
-            f.w0 = a.w0;
-            f.pv = tmb::PrefixView{a.P, a.PT, a.PC};
-            f.run = a.run;
-            f.raw = a.raw;
-            f.shifts = ctx->fft_shift.as<double>();
-            f.norms = ctx->fft_norm.as<double>();
-            f.bmin_u = a.bmin_u;
-            f.bmin_l = a.bmin_l;
-            f.nb = a.nb;
-            f.cand = a.cand;
-            f.cand_count = a.cand_count;
-            f.cand_cap = a.cand_cap;
-            f.dbg_d = a.dbg_d;
-            f.dbg_e = a.dbg_e;
-            f.W = a.W;
-            TM_CUDA(tmb::launch_fft_epilogue(f, s));
-            count_launch(L, 3);
-        }
-        count_launch(L, 2);
-    }
+        fft_contract_rows(ctx, L, g, a, short_rows, false);
+    if (!long_rows.empty())
+        fft_contract_rows(ctx, L, g, a, long_rows, true);
 }
 
 // Device pipeline for a mixed-length group (tensor-core kernels or the FFT branch).
