@@ -13,6 +13,7 @@
 //       the reference's distance at given windows.
 //   tmref_l2_dist / tmref_znormalize / tmref_block_order / tmref_select_knn :
 //       the inline building blocks of ZnormSearch.hpp, for bit-level pinning.
+#include <algorithm>
 #include <cfloat>
 #include <chrono>
 #include <cstdint>
@@ -119,6 +120,52 @@ extern "C"
     }
 
     void tmref_sss_destroy(void *handle) { delete static_cast<SkipSequentialScan *>(handle); }
+
+    // The reference's iSAX lower bound (SkipSequentialScan::lower_bound, the same bound as
+    // TREMOR's record-level check, SkipSequential.cpp:200-211) of one raw template against every
+    // owned window of a scan built with lower bounds: the number of windows whose bound does
+    // not exceed `bound` (the windows a skip-sequential scan must still compute), and per block
+    // of `block` consecutive windows whether any of them is such a window. For measuring how
+    // much a lower-bound skip could prune; the scan's own statistics are not needed.
+    int tmref_sss_lb_pass(void *handle, const float *query_raw, float bound, uint64_t block, uint8_t *any_pass,
+                          uint64_t *passing)
+    {
+        auto *scan = static_cast<SkipSequentialScan *>(handle);
+        if (!scan->lower_bounds || block == 0)
+            return -1;
+        try
+        {
+            std::vector<ts_type> znorm, paa;
+            std::vector<int> order;
+            scan->prepare_query(query_raw, znorm, paa, order);
+            const long long W = static_cast<long long>(scan->subsequences);
+            const long long nb = (W + static_cast<long long>(block) - 1) / static_cast<long long>(block);
+            unsigned long long count = 0;
+#pragma omp parallel for reduction(+ : count) schedule(static) num_threads(scan->threads)
+            for (long long b = 0; b < nb; b++)
+            {
+                uint8_t any = 0;
+                const long long end = std::min(W, (b + 1) * static_cast<long long>(block));
+                for (long long id = b * static_cast<long long>(block); id < end; id++)
+                {
+                    if (scan->raw[id] == TREMOR_MISSING_VALUE)
+                        continue;
+                    if (scan->lower_bound(paa.data(), id) <= bound)
+                    {
+                        count++;
+                        any = 1;
+                    }
+                }
+                any_pass[b] = any;
+            }
+            *passing = count;
+            return 0;
+        }
+        catch (const std::exception &)
+        {
+            return -1;
+        }
+    }
 
     // A sequential-mode scan (no lower bounds) over a record held in memory, with the
     // per-window statistics given instead of computed by build(): the members build() sets
