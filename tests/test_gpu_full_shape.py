@@ -6,7 +6,8 @@ bench.py) and compare with the reference's own SkipSequentialScan (sequential mo
 tremor/algos/sss/SkipSequential.cpp:296-473, built from the reference sources into
 oracle/_ref):
 
-* precision (config 3): 2^28 samples, 128 templates of 4096, kNN k=100, merge 0;
+* precision (config 3): 2^28 samples, 128 templates of 4096, kNN k=100, merge 0 (the
+  split-BF16 tensor-core kernel, which the config names);
 * threshold (config 2): 2^26 samples, 256 templates of 2048, correlation >= 0.8;
 * batching (config 4): 2^27 samples, 12 requests with lengths spread over 256-8192,
   kNN (k in {1, 10, 100}, merge m/2) and threshold (0.6-0.9), as bench.py draws them.
@@ -88,6 +89,7 @@ def test_config3_precision_full_shape():
     templates = q[:128]
     reqs = [tb.Request(t, tb.MODE_KNN, k=k, merge_offset=0) for t in templates]
     with tb.Context(x, device=0) as ctx:
+        ctx.set_kernel(tb.KERNEL_SPLIT_BF16)  # the contraction config 3 names (not the FFT branch)
         ctx.prepare_length(m)
         mean, std = ctx.window_stats(m)
         om, osd = ob.window_stats_fast(x, m)
@@ -120,6 +122,7 @@ def test_config2_threshold_full_shape():
     x, q, _ = synth.workload(n, 256, m, 500, seed=2027)
     reqs = [tb.Request(t, tb.MODE_THRESHOLD, correlation=corr, merge_offset=0) for t in q]
     with tb.Context(x, device=0) as ctx:
+        ctx.set_kernel(tb.KERNEL_SPLIT_BF16)
         ctx.profile_enable(True)
         b = ctx.batch(reqs)
         tensor = b.run(fp64=True)
@@ -170,7 +173,7 @@ def test_config4_batching_full_shape():
     assert min(lengths) <= 400 and max(lengths) >= 7000, lengths
     assert {r.mode for r in reqs} == {tb.MODE_KNN, tb.MODE_THRESHOLD}
     with tb.Context(x, device=0) as ctx:
-        auto = ctx.scan_batch(reqs, fp64=True)
+        auto = ctx.scan_batch(reqs, fp64=True)  # the planner's choice: mostly the FFT branch
         ctx.set_kernel(tb.KERNEL_SPLIT_BF16)
         ctx.set_tiles(tb.TILES_ROWS)
         rows = ctx.scan_batch(reqs)

@@ -351,8 +351,8 @@ struct tm_ctx
     int sms = 148;
     // model: the FFT branch's ms per template per 2^25 samples, for templates of up to 8192
     // samples (the fused kernels) and longer ones (B200 defaults; tm_autotune measures both)
-    double fft_ms = 0.25;
-    double fft_long_ms = 1.4;
+    double fft_ms = 0.84;
+    double fft_long_ms = 1.22;
     // the context's own memory pool for per-batch buffers (DevBuf::reserve_on); it keeps
     // up to 4 GiB of freed memory for the next batch
     cudaMemPool_t pool = nullptr;

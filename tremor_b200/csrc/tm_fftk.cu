@@ -182,24 +182,54 @@ __device__ __forceinline__ void load_roots(double2 *R, const double2 *roots)
         R[i] = roots[i];
 }
 
-// The shared epilogue of both correlation kernels for one window o of piece p (global
-// start g = piece_w + o): distance and bound from the dot product (taken from the transform
-// in shared memory by `dot_of`, evaluated only for windows that are searched), then kNN
-// bucket minima or threshold candidates. Every lane of the warp must call it; the warp's
-// windows lie within 64 consecutive positions, so in at most two buckets.
-template <class DotOf>
-__device__ __forceinline__ void corr_window(const Fft2Args &a, const TemplParam &P, int t, bool in_piece,
-                                            uint64_t g, float shift, float e_dot, int lane, DotOf dot_of)
+// What the epilogue reads from global memory for one window: its prefix sums at the start
+// and the end, its first sample and its constant run. The epilogues load these for a few
+// windows at once before evaluating any of them, so that the loads overlap (with one block
+// of 512 threads per SM there are too few warps to hide one load's latency at a time).
+struct WinIn
 {
-    const bool in_range = in_piece && g >= a.w0 && g - a.w0 < P.wcount;
+    double2 qa, qb;
+    float raw;
+    uint32_t run;
+};
+
+__device__ __forceinline__ WinIn load_window(const Fft2Args &a, int m, bool in_range, uint64_t g)
+{
+    WinIn w;
+    if (in_range)
+    {
+        w.qa = a.pv.Q[g];
+        w.qb = a.pv.Q[g + (uint64_t)m];
+        w.raw = a.raw[g];
+        w.run = a.run[g];
+    }
+    else
+    {
+        w.qa = w.qb = make_double2(0.0, 0.0);
+        w.raw = kMissing;
+        w.run = 0;
+    }
+    return w;
+}
+
+// The shared epilogue of both correlation kernels for window g (in the template's range when
+// in_range; its inputs w from load_window): distance and bound from the dot product (taken
+// from the transform in shared memory by `dot_of`, evaluated only for windows that are
+// searched), then kNN bucket minima or threshold candidates. Every lane of the warp must
+// call it; the warp's windows lie within 64 consecutive positions, so in at most two buckets.
+template <class DotOf>
+__device__ __forceinline__ void corr_window(const Fft2Args &a, const TemplParam &P, int t, bool in_range,
+                                            uint64_t g, const WinIn &w, float shift, float e_dot, int lane,
+                                            DotOf dot_of)
+{
     const uint32_t jr = in_range ? (uint32_t)(g - a.w0) : 0u;
-    const bool ok = in_range && a.raw[g] != kMissing && a.run[g] < (uint16_t)min(P.m, 65535);
+    const bool ok = in_range && w.raw != kMissing && w.run < (uint32_t)min(P.m, 65535);
     float up = inf_f(), lo = inf_f();
     bool hit = false;
     if (ok)
     {
         WindowStats ws;
-        if (window_prefix_stats(a.pv, a.pv.Q[g], a.pv.Q[g + (uint64_t)P.m], g, P.m, P.inv_m, ws) == 0)
+        if (window_prefix_stats(a.pv, w.qa, w.qb, g, P.m, P.inv_m, ws) == 0)
         {
             const double dot = dot_of();
             float d, e;
@@ -357,6 +387,7 @@ __global__ void __launch_bounds__(kF2T, 1) k_fft2_forward(const float *__restric
 __global__ void __launch_bounds__(kF2T, 1) k_fft2_corr(const Fft2Args a)
 {
     extern __shared__ double2 sm2[];
+    __shared__ TemplParam sP;
     double2 *buf = sm2, *R = sm2 + kF2Buf;
     load_roots(R, a.roots);
     const int lane = threadIdx.x & 31;
@@ -370,28 +401,52 @@ __global__ void __launch_bounds__(kF2T, 1) k_fft2_corr(const Fft2Args a)
         for (int ti = 0; ti < a.nrows; ti++)
         {
             const int t = a.rows[ti];
-            const TemplParam P = a.tp[t];
             const uint64_t piece_w = (uint64_t)p * kF2S;
             // windows of this piece in the template's range [w0, w0 + wcount)
-            if (piece_w + kF2S <= a.w0 || piece_w >= a.w0 + (uint64_t)P.wcount)
+            const uint64_t wcount = a.tp[t].wcount;
+            if (piece_w + kF2S <= a.w0 || piece_w >= a.w0 + wcount)
                 continue;
             const double2 *Y = a.Y + (size_t)ti * kF2H;
-            __syncthreads(); // the previous template's epilogue has read buf
-            for (int k = threadIdx.x; k <= kF2N / 2; k += kF2T)
+            __syncthreads(); // the previous template's epilogue has read buf and sP
+            if (threadIdx.x == 0)
+                sP = a.tp[t]; // the template's constants, read by every thread from shared memory
+            const TemplParam &P = sP;
+            // work items k = thread + 512 i (0 <= k <= N / 2), two at a time: their spectrum
+            // loads first, then the products
+            for (int i0 = 0; i0 < 10; i0 += 2)
             {
-                const int kn = kF2N - k;
-                const double2 Vk = cmul(X[k], Y[k]), Vn = cmul(X[kn], Y[kn]);
-                const double2 w = root<1>(R, 2 * k); // e^{2 pi i k / L}
-                // C[k] = E + i O with E = Vk + conj Vn, O = w (Vk - conj Vn); C[N - k] = conj E + i conj O
-                const double2 E = cadd(Vk, conj2(Vn));
-                const double2 O = cmul(csub(Vk, conj2(Vn)), w);
-                if (k == 0)
-                    buf[pidx(0)] = cadd(E, mul_si<1>(O)); // C[0] (Vn = V[N], the Nyquist bin)
-                else
+                double2 xk[2], xn[2], yk[2], yn[2];
+#pragma unroll
+                for (int j = 0; j < 2; j++)
                 {
-                    buf[pidx(k)] = cadd(E, mul_si<1>(O));
-                    if (k < kF2N / 2)
-                        buf[pidx(kn)] = cadd(conj2(E), mul_si<1>(conj2(O)));
+                    const int k = (int)threadIdx.x + kF2T * (i0 + j);
+                    if (k <= kF2N / 2)
+                    {
+                        xk[j] = X[k];
+                        xn[j] = X[kF2N - k];
+                        yk[j] = Y[k];
+                        yn[j] = Y[kF2N - k];
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < 2; j++)
+                {
+                    const int k = (int)threadIdx.x + kF2T * (i0 + j), kn = kF2N - k;
+                    if (k > kF2N / 2)
+                        continue;
+                    const double2 Vk = cmul(xk[j], yk[j]), Vn = cmul(xn[j], yn[j]);
+                    const double2 w = root<1>(R, 2 * k); // e^{2 pi i k / L}
+                    // C[k] = E + i O with E = Vk + conj Vn, O = w (Vk - conj Vn); C[N - k] = conj E + i conj O
+                    const double2 E = cadd(Vk, conj2(Vn));
+                    const double2 O = cmul(csub(Vk, conj2(Vn)), w);
+                    if (k == 0)
+                        buf[pidx(0)] = cadd(E, mul_si<1>(O)); // C[0] (Vn = V[N], the Nyquist bin)
+                    else
+                    {
+                        buf[pidx(k)] = cadd(E, mul_si<1>(O));
+                        if (k < kF2N / 2)
+                            buf[pidx(kn)] = cadd(conj2(E), mul_si<1>(conj2(O)));
+                    }
                 }
             }
             __syncthreads();
@@ -399,14 +454,27 @@ __global__ void __launch_bounds__(kF2T, 1) k_fft2_corr(const Fft2Args a)
             // epilogue: windows o = it * 512 + thread (a warp's 32 windows are consecutive)
             const double sm_ = sqrt((double)P.m);
             const float e_dot = (float)(kF2Kappa * norm * sm_ * (2.0 * sm_ + sqrt((double)kF2L)) * 1.01);
-            for (int it = 0; it < kF2S / kF2T; it++)
+            for (int it0 = 0; it0 < kF2S / kF2T; it0 += 4)
             {
-                const uint32_t o = (uint32_t)(it * kF2T) + threadIdx.x;
-                corr_window(a, P, t, true, piece_w + o, shift, e_dot, lane, [&]() {
-                    const int nn = (int)o + P.m - 1;
-                    const double2 c = final_out<1>(buf, R, nn >> 1);
-                    return ((nn & 1) ? c.y : c.x) * inv_l;
-                });
+                WinIn w[4];
+                bool inr[4];
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+                {
+                    const uint64_t g = piece_w + (uint64_t)((it0 + j) * kF2T) + threadIdx.x;
+                    inr[j] = g >= a.w0 && g - a.w0 < P.wcount;
+                    w[j] = load_window(a, P.m, inr[j], g);
+                }
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+                {
+                    const uint32_t o = (uint32_t)((it0 + j) * kF2T) + threadIdx.x;
+                    corr_window(a, P, t, inr[j], piece_w + o, w[j], shift, e_dot, lane, [&]() {
+                        const int nn = (int)o + P.m - 1;
+                        const double2 c = final_out<1>(buf, R, nn >> 1);
+                        return ((nn & 1) ? c.y : c.x) * inv_l;
+                    });
+                }
             }
         }
     }
@@ -539,6 +607,7 @@ __global__ void __launch_bounds__(kF2T, 1) k_fft3_forward(const float *__restric
 __global__ void __launch_bounds__(kF2T, 1) k_fft3_corr(const Fft2Args a)
 {
     extern __shared__ double2 sm2[];
+    __shared__ TemplParam sP;
     double2 *buf = sm2, *R = sm2 + kF2Buf;
     load_roots(R, a.roots);
     const int lane = threadIdx.x & 31;
@@ -553,54 +622,100 @@ __global__ void __launch_bounds__(kF2T, 1) k_fft3_corr(const Fft2Args a)
         for (int ti = 0; ti < a.nrows; ti++)
         {
             const int t = a.rows[ti];
-            const TemplParam P = a.tp[t];
             const uint64_t piece_w = (uint64_t)p * kF3S;
-            if (piece_w + kF3S <= a.w0 || piece_w >= a.w0 + (uint64_t)P.wcount)
+            const uint64_t wcount = a.tp[t].wcount;
+            if (piece_w + kF3S <= a.w0 || piece_w >= a.w0 + wcount)
                 continue;
             const double2 *Y = a.Y + (size_t)ti * kF3H;
+            __syncthreads(); // the previous template's epilogue has read sP
+            if (threadIdx.x == 0)
+                sP = a.tp[t]; // the template's constants, read by every thread from shared memory
+            __syncthreads();
+            const TemplParam &P = sP;
             const double sm_ = sqrt((double)P.m);
             const float e_dot = (float)(kF3Kappa * norm * sm_ * (2.0 * sm_ + sqrt((double)kF3L)) * 1.01);
             const int base = P.m - 1;
             for (int h = 0; h < 2; h++)
             {
                 __syncthreads(); // the previous half's epilogue has read buf
-                for (int u = threadIdx.x; u <= kFPts / 2; u += kF2T)
+                // work items u = thread + 512 i (0 <= u <= 4096): the eight spectrum loads of an
+                // item first, then its products
+                for (int i0 = 0; i0 < 9; i0 += 1)
                 {
-                    // C[u], C[N - u] from V[u], V[N - u]; C[u + 8192], C[8192 - u] from V[u + 8192], V[8192 - u]
-                    const double2 V1 = cmul(X[u], Y[u]), V1n = cmul(X[N - u], Y[N - u]);
-                    const double2 E1 = cadd(V1, conj2(V1n)), O1 = cmul(csub(V1, conj2(V1n)), root<1>(R, u));
-                    const double2 Cu = cadd(E1, mul_si<1>(O1)), CNu = cadd(conj2(E1), mul_si<1>(conj2(O1)));
-                    const int u2 = u + kFPts;
-                    const double2 V2 = cmul(X[u2], Y[u2]), V2n = cmul(X[N - u2], Y[N - u2]);
-                    const double2 E2 = cadd(V2, conj2(V2n)), O2 = cmul(csub(V2, conj2(V2n)), root<1>(R, u2));
-                    const double2 Cv = cadd(E2, mul_si<1>(O2)), C8u = cadd(conj2(E2), mul_si<1>(conj2(O2)));
-                    if (h == 0)
+                    double2 v[1][8];
+#pragma unroll
+                    for (int j = 0; j < 1; j++)
                     {
-                        buf[pidx(u)] = cadd(Cu, Cv);
-                        if (u > 0 && u < kFPts / 2)
-                            buf[pidx(kFPts - u)] = cadd(C8u, CNu);
+                        const int u = (int)threadIdx.x + kF2T * (i0 + j), u2 = u + kFPts;
+                        if (u <= kFPts / 2)
+                        {
+                            v[j][0] = X[u];
+                            v[j][1] = Y[u];
+                            v[j][2] = X[N - u];
+                            v[j][3] = Y[N - u];
+                            v[j][4] = X[u2];
+                            v[j][5] = Y[u2];
+                            v[j][6] = X[N - u2];
+                            v[j][7] = Y[N - u2];
+                        }
                     }
-                    else
+#pragma unroll
+                    for (int j = 0; j < 1; j++)
                     {
-                        buf[pidx(u)] = cmul(csub(Cu, Cv), root<1>(R, 2 * u));
-                        if (u > 0 && u < kFPts / 2)
-                            buf[pidx(kFPts - u)] = cmul(csub(C8u, CNu), root<1>(R, 2 * (kFPts - u)));
+                        const int u = (int)threadIdx.x + kF2T * (i0 + j), u2 = u + kFPts;
+                        if (u > kFPts / 2)
+                            continue;
+                        // C[u], C[N - u] from V[u], V[N - u]; C[u + 8192], C[8192 - u] from V[u + 8192], V[8192 - u]
+                        const double2 V1 = cmul(v[j][0], v[j][1]), V1n = cmul(v[j][2], v[j][3]);
+                        const double2 E1 = cadd(V1, conj2(V1n)), O1 = cmul(csub(V1, conj2(V1n)), root<1>(R, u));
+                        const double2 Cu = cadd(E1, mul_si<1>(O1)), CNu = cadd(conj2(E1), mul_si<1>(conj2(O1)));
+                        const double2 V2 = cmul(v[j][4], v[j][5]), V2n = cmul(v[j][6], v[j][7]);
+                        const double2 E2 = cadd(V2, conj2(V2n)), O2 = cmul(csub(V2, conj2(V2n)), root<1>(R, u2));
+                        const double2 Cv = cadd(E2, mul_si<1>(O2)), C8u = cadd(conj2(E2), mul_si<1>(conj2(O2)));
+                        if (h == 0)
+                        {
+                            buf[pidx(u)] = cadd(Cu, Cv);
+                            if (u > 0 && u < kFPts / 2)
+                                buf[pidx(kFPts - u)] = cadd(C8u, CNu);
+                        }
+                        else
+                        {
+                            buf[pidx(u)] = cmul(csub(Cu, Cv), root<1>(R, 2 * u));
+                            if (u > 0 && u < kFPts / 2)
+                                buf[pidx(kFPts - u)] = cmul(csub(C8u, CNu), root<1>(R, 2 * (kFPts - u)));
+                        }
                     }
                 }
                 __syncthreads();
                 fft8192_r16<1>(buf, R);
                 // windows of this half: v -> n0 = 4 ((v >> 1) + (base >> 2)) + 2 h + (v & 1), o = n0 - base
-                for (int it = 0; it < 17; it++)
+                for (int it0 = 0; it0 < 17; it0 += 3)
                 {
-                    const int v = it * kF2T + (int)threadIdx.x;
-                    const int n0 = 4 * ((v >> 1) + (base >> 2)) + 2 * h + (v & 1);
-                    const int o = n0 - base;
-                    const bool in_piece = o >= 0 && o < kF3S;
-                    const uint64_t g = piece_w + (uint64_t)(in_piece ? o : 0);
-                    corr_window(a, P, t, in_piece, g, shift, e_dot, lane, [&]() {
-                        const double2 c = final_out<1>(buf, R, n0 >> 2);
-                        return ((n0 & 1) ? c.y : c.x) * inv_l;
-                    });
+                    WinIn w[3];
+                    bool inr[3];
+                    uint64_t gg[3];
+                    int nn[3];
+#pragma unroll
+                    for (int j = 0; j < 3; j++)
+                    {
+                        const int v = (it0 + j) * kF2T + (int)threadIdx.x;
+                        nn[j] = 4 * ((v >> 1) + (base >> 2)) + 2 * h + (v & 1);
+                        const int o = nn[j] - base;
+                        const bool in_piece = it0 + j < 17 && o >= 0 && o < kF3S;
+                        gg[j] = piece_w + (uint64_t)(in_piece ? o : 0);
+                        inr[j] = in_piece && gg[j] >= a.w0 && gg[j] - a.w0 < P.wcount;
+                        w[j] = load_window(a, P.m, inr[j], gg[j]);
+                    }
+#pragma unroll
+                    for (int j = 0; j < 3; j++)
+                    {
+                        if (it0 + j >= 17)
+                            break; // warp-uniform
+                        corr_window(a, P, t, inr[j], gg[j], w[j], shift, e_dot, lane, [&]() {
+                            const double2 c = final_out<1>(buf, R, nn[j] >> 2);
+                            return ((nn[j] & 1) ? c.y : c.x) * inv_l;
+                        });
+                    }
                 }
             }
         }
