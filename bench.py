@@ -437,7 +437,7 @@ def run_serving(args, w):
     arrivals = np.cumsum(rng.exponential(1.0 / rate, size=count))
     ctx = tb.Context(x, device=local)
     t0 = time.time()
-    server = ctx.serve(workers=args.workers, max_batch=args.max_batch)
+    server = ctx.serve(workers=args.workers, max_batch=args.max_batch, batch_ms=args.batch_ms)
     log(f'[bench] server started (prefix sums) in {time.time() - t0:.2f} s')
     for s in range(args.warmup):  # untimed: a few batches of 8 requests
         for i in range(8):
@@ -501,7 +501,7 @@ def run_serving(args, w):
                 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'bf16x3+f32', 'data': 'synthetic',
                 'config': {'workload': args.workload, 'n': w['n'], 'templates': w['q'], 'm': w['m'],
                            'requests': count, 'arrival': f'poisson {rate} req/s', 'seed': w['seed'],
-                           'workers': args.workers, 'max_batch': args.max_batch,
+                           'workers': args.workers, 'max_batch': args.max_batch, 'batch_ms': args.batch_ms,
                            'l2': 'inputs larger than L2 (waveform 4n bytes)', 'parallelism': f'replicas x{world}',
                            'timing': 'server steady clock, first submission to last completion'},
                 'latency_ms': {'p50': pct(lat, 50), 'p99': pct(lat, 99), 'mean': float(lat.mean()),
@@ -773,6 +773,7 @@ def main():
     p.add_argument('--requests', type=int, default=0, help='serving: requests in the timed stream')
     p.add_argument('--workers', type=int, default=1, help='serving: batches in flight at once')
     p.add_argument('--max-batch', type=int, default=256, help='serving: requests per batch at most')
+    p.add_argument('--batch-ms', type=float, default=0.0, help='serving: modelled device ms per batch at most (0: none)')
     args = p.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -267,6 +267,10 @@ typedef struct tm_serve_config
                              * smaller, less efficient batches) */
     int max_batch;          /* requests per batch at most (default 256) */
     uint64_t memory_budget; /* device bytes for requests in flight; 0: a quarter of the free memory */
+    double batch_ms;        /* modelled device milliseconds of a batch at most (the planner's model,
+                             * tm_autotune): admission stops there, so a request arriving during a
+                             * batch waits for a bounded one; 0: no limit (a first request alone is
+                             * always admitted) */
 } tm_serve_config;
 
 typedef struct tm_completion

@@ -106,3 +106,36 @@ def test_serving_state_rules():
         pending, in_flight, nbytes, launches = server.status()
         assert (pending, in_flight, nbytes) == (0, 0, 0) and launches > 0
     _check(x, reqs, [got[i].answers for i in t])
+
+
+def test_batch_time_budget():
+    """batch_ms bounds a batch's modelled device time: below any one request's estimate
+    every batch holds one request (a first request alone is always admitted), and the
+    answers are those of the requests alone."""
+    x = _waveform(1 << 16, 27)
+    rng = np.random.default_rng(28)
+    reqs = _requests(x, rng, [64, 96, 150, 300, 64, 500, 128, 40])
+    with tb.Context(x) as ctx:
+        with ctx.serve(workers=1, max_batch=8, batch_ms=1e-9) as server:
+            ticket = {server.submit(r): i for i, r in enumerate(reqs)}
+            got = _collect(server, len(reqs))
+    assert sorted(c.batch_size for c in got.values()) == [1] * len(reqs)
+    served = [None] * len(reqs)
+    for t, c in got.items():
+        served[ticket[t]] = c.answers
+    _check(x, reqs, served)
+
+
+def test_poll_without_limit_returns_once_stopped():
+    """tm_poll with no time limit returns (empty) once the server is stopped and nothing is
+    left to complete, instead of waiting for good."""
+    x = _waveform(1 << 15, 29)
+    with tb.Context(x) as ctx:
+        server = ctx.serve()
+        server.stop()
+        out = []
+        th = threading.Thread(target=lambda: out.append(server.poll(8, timeout_ms=-1)), daemon=True)
+        th.start()
+        th.join(timeout=10.0)
+        assert not th.is_alive(), 'poll without a limit did not return after stop'
+        assert out == [[]]

@@ -51,7 +51,8 @@ class _Request(ctypes.Structure):
 
 
 class _ServeConfig(ctypes.Structure):
-    _fields_ = [('workers', ctypes.c_int32), ('max_batch', ctypes.c_int32), ('memory_budget', ctypes.c_uint64)]
+    _fields_ = [('workers', ctypes.c_int32), ('max_batch', ctypes.c_int32), ('memory_budget', ctypes.c_uint64),
+                ('batch_ms', ctypes.c_double)]
 
 
 class _Completion(ctypes.Structure):
@@ -251,9 +252,10 @@ class Context:
         self._check(self._lib.tm_scan_batch(self._h, arr, len(requests), ctypes.byref(res)))
         return self._take(res, len(requests), requests if fp64 else None)
 
-    def serve(self, workers: int = 1, max_batch: int = 256, memory_budget: int = 0) -> 'Server':
-        """Starts continuous batching over this context's waveform (tm_serve_start)."""
-        return Server(self, workers, max_batch, memory_budget)
+    def serve(self, workers: int = 1, max_batch: int = 256, memory_budget: int = 0, batch_ms: float = 0.0) -> 'Server':
+        """Starts continuous batching over this context's waveform (tm_serve_start); batch_ms
+        bounds a batch's modelled device time (0: no bound)."""
+        return Server(self, workers, max_batch, memory_budget, batch_ms)
 
     def scan_knn(self, template: np.ndarray, k: int, merge_offset: int = 0, bound: float = float('inf')):
         """(positions, distances) of one template's k answers (tm_scan_knn); answers above
@@ -405,9 +407,10 @@ class Server:
     """Continuous batching over a context's resident waveform (tm_serve_*): submit() from
     any thread, poll() from one."""
 
-    def __init__(self, ctx: Context, workers: int = 1, max_batch: int = 256, memory_budget: int = 0):
+    def __init__(self, ctx: Context, workers: int = 1, max_batch: int = 256, memory_budget: int = 0,
+                 batch_ms: float = 0.0):
         self.ctx = ctx
-        cfg = _ServeConfig(workers, max_batch, memory_budget)
+        cfg = _ServeConfig(workers, max_batch, memory_budget, batch_ms)
         ctx._check(ctx._lib.tm_serve_start(ctx._h, ctypes.byref(cfg)))
         self._running = True
 

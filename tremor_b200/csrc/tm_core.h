@@ -460,6 +460,7 @@ void prepare_group(tm_ctx *ctx, Lane &L, int m, const std::vector<int> &idx, con
 void prepare_group_mixed(tm_ctx *ctx, Lane &L, const std::vector<int> &idx_in, const tm_request *reqs, GroupPlan &g,
                          uint64_t &h2d, int col_tile = 0);
 int plan_col_tile(const tm_ctx *ctx, const tm_request *reqs, const std::vector<int> &idx, double *cost = nullptr);
+double tile_time(const tm_ctx *ctx, bool mixed, int v, double k);
 void create_batch(tm_ctx *ctx, Lane &L, const tm_request *requests, int count, tm_batch &b, bool serving = false);
 
 // tm_serve.cu

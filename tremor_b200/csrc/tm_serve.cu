@@ -21,7 +21,8 @@ struct ServeItem
     uint64_t ticket = 0;
     std::vector<float> templ; // owned copy
     tm_request req{};
-    uint64_t bytes = 0; // admission estimate
+    uint64_t bytes = 0;   // admission estimate of its device memory
+    double cost_ms = 0.0; // and of its device time (serve_cost)
     double submit_ms = 0.0;
 };
 
@@ -63,26 +64,46 @@ static uint64_t serve_bytes(const tm_ctx *ctx, const tm_request &r)
     return row + 48ull * cands;
 }
 
+// Modelled device milliseconds of a request: the cheaper of the FFT branch (a constant per
+// template, by kind) and its share of a full 128-row tile of mixed lengths at its own K, from
+// the planner's model (ms per 2^25 windows), scaled to the record's windows.
+static double serve_cost(const tm_ctx *ctx, const tm_request &r)
+{
+    const double scale = static_cast<double>(ctx->n - static_cast<uint64_t>(r.m) + 1) / 33554432.0;
+    const double fft = r.m <= tmb::kF2S ? ctx->fft_ms : ctx->fft_long_ms;
+    const double row = tile_time(ctx, true, 0, static_cast<double>((r.m + 63) & ~63)) / 128.0;
+    return std::min(fft, row) * scale;
+}
+
 // Admission (under the server's lock). A batch is built a tile at a time: the 128 rows of
 // a contraction tile share one K extent, their longest template, so rows not longer than
 // that cost nothing extra. Each tile opens with the oldest pending request (so every batch
 // admits the oldest, and later arrivals never hold a request back indefinitely) and fills
 // with the longest pending requests not longer than it; with a long queue the tiles hold
 // similar lengths.
-// Stops at max_batch or at the memory budget (a first request alone is always admitted).
+// Stops at max_batch, at the memory budget or at the batch's modelled time (batch_ms); a
+// first request alone is always admitted.
 static void admit(Server *sv, std::vector<ServeItem> &batch, uint64_t &bytes)
 {
-    auto fits = [&](uint64_t b) {
-        return (sv->in_flight_bytes == 0 && batch.empty()) || sv->in_flight_bytes + bytes + b <= sv->cfg.memory_budget;
+    double ms = 0.0;
+    for (const ServeItem &it : batch)
+        ms += it.cost_ms;
+    auto fits = [&](const ServeItem &it) {
+        if (batch.empty() && sv->in_flight_bytes == 0)
+            return true;
+        if (sv->cfg.batch_ms > 0.0 && !batch.empty() && ms + it.cost_ms > sv->cfg.batch_ms)
+            return false;
+        return sv->in_flight_bytes + bytes + it.bytes <= sv->cfg.memory_budget;
     };
     std::vector<size_t> order;
     std::vector<char> chosen;
     while (!sv->pending.empty() && static_cast<int>(batch.size()) < sv->cfg.max_batch)
     {
-        if (!fits(sv->pending.front().bytes))
+        if (!fits(sv->pending.front()))
             return;
         const int cap_m = sv->pending.front().req.m;
         bytes += sv->pending.front().bytes;
+        ms += sv->pending.front().cost_ms;
         batch.push_back(std::move(sv->pending.front()));
         sv->pending.pop_front();
         const size_t room = std::min<size_t>(127, static_cast<size_t>(sv->cfg.max_batch) - batch.size());
@@ -96,9 +117,10 @@ static void admit(Server *sv, std::vector<ServeItem> &batch, uint64_t &bytes)
         size_t taken = 0;
         for (size_t i : order)
         {
-            if (taken == room || !fits(sv->pending[i].bytes))
+            if (taken == room || !fits(sv->pending[i]))
                 break;
             bytes += sv->pending[i].bytes;
+            ms += sv->pending[i].cost_ms;
             batch.push_back(std::move(sv->pending[i]));
             chosen[i] = 1;
             taken++;
@@ -260,10 +282,10 @@ int tm_serve_start(tm_ctx *ctx, const tm_serve_config *config)
         return TM_ERR_ARGUMENT;
     if (serving(ctx))
         return TM_ERR_STATE;
-    tm_serve_config cfg{1, 256, 0};
+    tm_serve_config cfg{1, 256, 0, 0.0};
     if (config)
         cfg = *config;
-    if (cfg.workers < 1 || cfg.workers > 8 || cfg.max_batch < 1)
+    if (cfg.workers < 1 || cfg.workers > 8 || cfg.max_batch < 1 || !(cfg.batch_ms >= 0.0))
         return TM_ERR_ARGUMENT;
     return guarded(ctx, [&] {
         TM_CUDA(cudaSetDevice(ctx->device));
@@ -318,6 +340,7 @@ int tm_submit(tm_ctx *ctx, const tm_request *request, uint64_t *ticket)
     }
     it.req = *request;
     it.bytes = serve_bytes(ctx, *request);
+    it.cost_ms = serve_cost(ctx, *request);
     {
         std::lock_guard<std::mutex> lk(sv->mu);
         if (sv->stopping)
