@@ -215,70 +215,115 @@ __device__ __forceinline__ WinIn load_window(const Fft2Args &a, int m, bool in_r
 // The shared epilogue of both correlation kernels for window g (in the template's range when
 // in_range; its inputs w from load_window): distance and bound from the dot product (taken
 // from the transform in shared memory by `dot_of`, evaluated only for windows that are
-// searched), then kNN bucket minima or threshold candidates. Every lane of the warp must
-// call it; the warp's windows lie within 64 consecutive positions, so in at most two buckets.
+// searched) into up = d + e and lo = d - e (+inf for windows not searched; lo = -inf when the
+// statistics are not trusted), and hit = lo <= the threshold distance.
 template <class DotOf>
-__device__ __forceinline__ void corr_window(const Fft2Args &a, const TemplParam &P, int t, bool in_range,
-                                            uint64_t g, const WinIn &w, float shift, float e_dot, int lane,
-                                            DotOf dot_of)
+__device__ __forceinline__ void corr_eval(const Fft2Args &a, const TemplParam &P, int t, bool in_range, uint64_t g,
+                                          const WinIn &w, float shift, float e_dot, DotOf dot_of, float &up,
+                                          float &lo, bool &hit)
 {
-    const uint32_t jr = in_range ? (uint32_t)(g - a.w0) : 0u;
-    const bool ok = in_range && w.raw != kMissing && w.run < (uint32_t)min(P.m, 65535);
-    float up = inf_f(), lo = inf_f();
-    bool hit = false;
-    if (ok)
+    up = inf_f();
+    lo = inf_f();
+    hit = false;
+    if (!(in_range && w.raw != kMissing && w.run < (uint32_t)min(P.m, 65535)))
+        return;
+    WindowStats ws;
+    if (window_prefix_stats(a.pv, w.qa, w.qb, g, P.m, P.inv_m, ws) == 0)
     {
-        WindowStats ws;
-        if (window_prefix_stats(a.pv, w.qa, w.qb, g, P.m, P.inv_m, ws) == 0)
+        const double dot = dot_of();
+        float d, e;
+        fast_distance_mixed(P, P.a1_main, (float)dot, ws.mu, ws.iv, shift, stats_error(ws, P.m, P.qs, P.s1), d, e);
+        e += 2.0f * e_dot * ws.iv * 1.01f;
+        if (a.dbg_d != nullptr)
         {
-            const double dot = dot_of();
-            float d, e;
-            fast_distance_mixed(P, P.a1_main, (float)dot, ws.mu, ws.iv, shift, stats_error(ws, P.m, P.qs, P.s1), d,
-                                e);
-            e += 2.0f * e_dot * ws.iv * 1.01f;
-            if (a.dbg_d != nullptr)
-            {
-                a.dbg_d[(size_t)t * a.W + jr] = d;
-                a.dbg_e[(size_t)t * a.W + jr] = e;
-            }
-            up = d + e;
-            lo = d - e;
-            hit = lo <= P.thr_ed;
+            const uint32_t jr = (uint32_t)(g - a.w0);
+            a.dbg_d[(size_t)t * a.W + jr] = d;
+            a.dbg_e[(size_t)t * a.W + jr] = e;
+        }
+        up = d + e;
+        lo = d - e;
+        hit = lo <= P.thr_ed;
+    }
+    else
+    {
+        lo = -inf_f();
+        hit = true;
+    }
+}
+
+// kNN bucket minima of a group of J windows per lane (windows jr[j] relative to w0, those
+// with inr[j] in the template's range) whose warp-wide span is under a bucket, so they lie in
+// at most two buckets B and B + 1: per-lane minima first, then one warp reduction per bucket
+// and key, and one atomic per bucket and key (skipped for buckets with no searched window,
+// whose minima stay at +inf's key). Every lane of the warp must call it.
+template <int J>
+__device__ __forceinline__ void bucket_minima(const Fft2Args &a, int t, int lane, const bool (&inr)[J],
+                                              const uint32_t (&jr)[J], const float (&up)[J], const float (&lo)[J])
+{
+    uint32_t bmin = 0xffffffffu;
+#pragma unroll
+    for (int j = 0; j < J; j++)
+        if (inr[j])
+            bmin = min(bmin, jr[j] / (uint32_t)kBucket);
+    const uint32_t B = __reduce_min_sync(0xffffffffu, bmin);
+    if (B == 0xffffffffu)
+        return; // no window of the warp in the range
+    uint32_t uA = 0xffffffffu, lA = 0xffffffffu, uB = 0xffffffffu, lB = 0xffffffffu;
+#pragma unroll
+    for (int j = 0; j < J; j++)
+    {
+        if (!inr[j])
+            continue;
+        const uint32_t ku = float_key(up[j]), kl = float_key(lo[j]);
+        if (jr[j] / (uint32_t)kBucket == B)
+        {
+            uA = min(uA, ku);
+            lA = min(lA, kl);
         }
         else
         {
-            lo = -inf_f();
-            hit = true;
+            uB = min(uB, ku);
+            lB = min(lB, kl);
         }
     }
-    if (P.mode == TM_MODE_KNN)
+    uA = __reduce_min_sync(0xffffffffu, uA);
+    lA = __reduce_min_sync(0xffffffffu, lA);
+    uB = __reduce_min_sync(0xffffffffu, uB);
+    lB = __reduce_min_sync(0xffffffffu, lB);
+    const uint32_t none = float_key(inf_f());
+    if (lane == 0)
     {
-        const uint32_t bucket = jr / kBucket;
-        const unsigned act = __ballot_sync(0xffffffffu, in_range);
-        if (act == 0u)
-            return;
-        const uint32_t b0 = __shfl_sync(0xffffffffu, bucket, __ffs(act) - 1);
-        const unsigned same = __ballot_sync(0xffffffffu, in_range && bucket == b0);
-        const unsigned other = act & ~same;
-        const uint32_t ku = float_key(up), kl = float_key(lo);
-        const uint32_t u0 = __reduce_min_sync(0xffffffffu, same & (1u << lane) ? ku : 0xffffffffu);
-        const uint32_t l0 = __reduce_min_sync(0xffffffffu, same & (1u << lane) ? kl : 0xffffffffu);
-        const uint32_t u1 = __reduce_min_sync(0xffffffffu, other & (1u << lane) ? ku : 0xffffffffu);
-        const uint32_t l1 = __reduce_min_sync(0xffffffffu, other & (1u << lane) ? kl : 0xffffffffu);
-        const uint32_t none = float_key(inf_f());
-        if (lane == __ffs(act) - 1 && (u0 != none || l0 != none) && u0 != 0xffffffffu)
+        if (uA != 0xffffffffu && (uA != none || lA != none))
         {
-            atomicMin(&a.bmin_u[(size_t)t * a.nb + b0], u0);
-            atomicMin(&a.bmin_l[(size_t)t * a.nb + b0], l0);
+            atomicMin(&a.bmin_u[(size_t)t * a.nb + B], uA);
+            atomicMin(&a.bmin_l[(size_t)t * a.nb + B], lA);
         }
-        if (other != 0u && lane == __ffs(other) - 1 && (u1 != none || l1 != none))
+        if (uB != 0xffffffffu && (uB != none || lB != none))
         {
-            atomicMin(&a.bmin_u[(size_t)t * a.nb + bucket], u1);
-            atomicMin(&a.bmin_l[(size_t)t * a.nb + bucket], l1);
+            atomicMin(&a.bmin_u[(size_t)t * a.nb + B + 1], uB);
+            atomicMin(&a.bmin_l[(size_t)t * a.nb + B + 1], lB);
         }
     }
-    else
-        emit_candidates(hit ? 1u : 0u, lane, (uint32_t)t, jr, a.cand, a.cand_count, a.cand_cap);
+}
+
+// Threshold candidates of one window per lane: one ballot, one atomic per warp with hits.
+// Entries past the capacity are counted, not written. Every lane of the warp must call it.
+__device__ __forceinline__ void emit_hits(const Fft2Args &a, int t, int lane, bool hit, uint32_t jr)
+{
+    const unsigned b = __ballot_sync(0xffffffffu, hit);
+    if (b == 0u)
+        return;
+    const int leader = __ffs(b) - 1;
+    uint32_t base = 0;
+    if (lane == leader)
+        base = atomicAdd(a.cand_count, (uint32_t)__popc(b));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (hit)
+    {
+        const uint32_t pos = base + (uint32_t)__popc(b & ((1u << lane) - 1u));
+        if (pos < a.cand_cap)
+            a.cand[pos] = Candidate{(uint32_t)t, jr};
+    }
 }
 
 // Forward real FFT of one piece of the record (blockIdx.x < pieces) or one template row
@@ -457,24 +502,33 @@ __global__ void __launch_bounds__(kF2T, 1) k_fft2_corr(const Fft2Args a)
             for (int it0 = 0; it0 < kF2S / kF2T; it0 += 4)
             {
                 WinIn w[4];
-                bool inr[4];
+                bool inr[4], hit[4];
+                uint32_t jr[4];
+                float up[4], lo[4];
 #pragma unroll
                 for (int j = 0; j < 4; j++)
                 {
                     const uint64_t g = piece_w + (uint64_t)((it0 + j) * kF2T) + threadIdx.x;
                     inr[j] = g >= a.w0 && g - a.w0 < P.wcount;
+                    jr[j] = inr[j] ? (uint32_t)(g - a.w0) : 0u;
                     w[j] = load_window(a, P.m, inr[j], g);
                 }
 #pragma unroll
                 for (int j = 0; j < 4; j++)
                 {
                     const uint32_t o = (uint32_t)((it0 + j) * kF2T) + threadIdx.x;
-                    corr_window(a, P, t, inr[j], piece_w + o, w[j], shift, e_dot, lane, [&]() {
+                    corr_eval(a, P, t, inr[j], piece_w + o, w[j], shift, e_dot, [&]() {
                         const int nn = (int)o + P.m - 1;
                         const double2 c = final_out<1>(buf, R, nn >> 1);
                         return ((nn & 1) ? c.y : c.x) * inv_l;
-                    });
+                    }, up[j], lo[j], hit[j]);
                 }
+                if (P.mode == TM_MODE_KNN)
+                    bucket_minima<4>(a, t, lane, inr, jr, up, lo); // the group spans 3 x 512 + 32 windows
+                else
+#pragma unroll
+                    for (int j = 0; j < 4; j++)
+                        emit_hits(a, t, lane, hit[j], jr[j]);
             }
         }
     }
@@ -689,14 +743,16 @@ __global__ void __launch_bounds__(kF2T, 1) k_fft3_corr(const Fft2Args a)
                 __syncthreads();
                 fft8192_r16<1>(buf, R);
                 // windows of this half: v -> n0 = 4 ((v >> 1) + (base >> 2)) + 2 h + (v & 1), o = n0 - base
-                for (int it0 = 0; it0 < 17; it0 += 3)
+                for (int it0 = 0; it0 < 17; it0 += 2)
                 {
-                    WinIn w[3];
-                    bool inr[3];
-                    uint64_t gg[3];
-                    int nn[3];
+                    WinIn w[2];
+                    bool inr[2], hit[2];
+                    uint32_t jr[2];
+                    float up[2], lo[2];
+                    uint64_t gg[2];
+                    int nn[2];
 #pragma unroll
-                    for (int j = 0; j < 3; j++)
+                    for (int j = 0; j < 2; j++)
                     {
                         const int v = (it0 + j) * kF2T + (int)threadIdx.x;
                         nn[j] = 4 * ((v >> 1) + (base >> 2)) + 2 * h + (v & 1);
@@ -704,18 +760,21 @@ __global__ void __launch_bounds__(kF2T, 1) k_fft3_corr(const Fft2Args a)
                         const bool in_piece = it0 + j < 17 && o >= 0 && o < kF3S;
                         gg[j] = piece_w + (uint64_t)(in_piece ? o : 0);
                         inr[j] = in_piece && gg[j] >= a.w0 && gg[j] - a.w0 < P.wcount;
+                        jr[j] = inr[j] ? (uint32_t)(gg[j] - a.w0) : 0u;
                         w[j] = load_window(a, P.m, inr[j], gg[j]);
                     }
 #pragma unroll
-                    for (int j = 0; j < 3; j++)
-                    {
-                        if (it0 + j >= 17)
-                            break; // warp-uniform
-                        corr_window(a, P, t, inr[j], gg[j], w[j], shift, e_dot, lane, [&]() {
+                    for (int j = 0; j < 2; j++)
+                        corr_eval(a, P, t, inr[j], gg[j], w[j], shift, e_dot, [&]() {
                             const double2 c = final_out<1>(buf, R, nn[j] >> 2);
                             return ((nn[j] & 1) ? c.y : c.x) * inv_l;
-                        });
-                    }
+                        }, up[j], lo[j], hit[j]);
+                    if (P.mode == TM_MODE_KNN)
+                        bucket_minima<2>(a, t, lane, inr, jr, up, lo); // the group spans 1024 + 64 windows
+                    else
+#pragma unroll
+                        for (int j = 0; j < 2; j++)
+                            emit_hits(a, t, lane, hit[j], jr[j]);
                 }
             }
         }
