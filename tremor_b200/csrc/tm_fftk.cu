@@ -75,10 +75,15 @@ template <int S> __device__ __forceinline__ double2 mul_si(double2 a)
     return S > 0 ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
 }
 
+// Position of R1[a] in shared memory: the low three bits XOR-ed with bits 3-5, so that the
+// lookups of a quarter warp at strides 1, 2, 4 or 8 (the passes' and epilogue's patterns)
+// fall in distinct banks.
+__device__ __forceinline__ int r1_slot(int a) { return a ^ ((a >> 3) & 7); }
+
 // e^{S 2 pi i e / 32768}, 0 <= e < 32768, from the shared tables R (R1 then R2).
 template <int S> __device__ __forceinline__ double2 root(const double2 *R, int e)
 {
-    const double2 w = cmul(R[128 + (e >> 7)], R[e & 127]);
+    const double2 w = cmul(R[128 + (e >> 7)], R[r1_slot(e & 127)]);
     return S > 0 ? w : conj2(w);
 }
 
@@ -179,7 +184,7 @@ template <int S> __device__ __forceinline__ double2 final_out(const double2 *buf
 __device__ __forceinline__ void load_roots(double2 *R, const double2 *roots)
 {
     for (int i = threadIdx.x; i < kFRoots; i += blockDim.x)
-        R[i] = roots[i];
+        R[i < 128 ? r1_slot(i) : i] = roots[i];
 }
 
 // What the epilogue reads from global memory for one window: its prefix sums at the start
