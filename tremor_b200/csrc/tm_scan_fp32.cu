@@ -14,7 +14,10 @@
 //
 // Tile: 256 windows x 64 templates per CTA, 8 warps; a warp owns 8 templates and a
 // lane 8 consecutive windows (64 FP32 accumulators). K advances in stages of 64
-// samples, double-buffered with cp.async.
+// samples, double-buffered with cp.async. The stage's waveform slice is stored with 4
+// floats of padding after every 32 (xpos), so that the float4 loads of a quarter warp
+// (lanes 8 floats apart) fall in distinct shared-memory banks; a float4 never straddles
+// a pad because the loads start at multiples of 4 floats.
 #include "tm_internal.cuh"
 #include "tm_epilogue.cuh"
 
@@ -22,6 +25,9 @@ namespace tmb {
 
 constexpr int F_WIN = 256, F_TPL = 64, F_K = 64, F_THREADS = 256;
 constexpr int F_XS = F_WIN + F_K + 16;
+constexpr int F_XS_PAD = F_XS + ((F_XS + 31) >> 5) * 4; // F_XS floats with their padding
+
+__device__ __forceinline__ int xpos(int i) { return i + ((i >> 5) << 2); }
 
 __device__ __forceinline__ void cp_async4(void *smem, const void *gmem)
 {
@@ -38,7 +44,7 @@ template <int N> __device__ __forceinline__ void cp_wait() { asm volatile("cp.as
 
 __global__ void __launch_bounds__(F_THREADS, 2) k_scan_fp32(ScanArgs a)
 {
-    __shared__ __align__(16) float xs[2][F_XS];
+    __shared__ __align__(16) float xs[2][F_XS_PAD];
     __shared__ __align__(16) float qs[2][F_TPL][F_K];
     __shared__ TemplParam tps[F_TPL];
 
@@ -54,7 +60,7 @@ __global__ void __launch_bounds__(F_THREADS, 2) k_scan_fp32(ScanArgs a)
 
     auto load_stage = [&](int buf, int k0) {
         for (int i = tid; i < F_XS; i += F_THREADS)
-            cp_async4(&xs[buf][i], xg + k0 + i);
+            cp_async4(&xs[buf][xpos(i)], xg + k0 + i);
         for (int i = tid; i < F_TPL * F_K / 4; i += F_THREADS)
         {
             const int t = i / (F_K / 4), c = i % (F_K / 4);
@@ -84,16 +90,17 @@ __global__ void __launch_bounds__(F_THREADS, 2) k_scan_fp32(ScanArgs a)
             cp_wait<0>();
         __syncthreads();
         for (int i = tid; i < F_XS; i += F_THREADS)
-            xs[cur][i] -= shift;
+            xs[cur][xpos(i)] -= shift;
         __syncthreads();
-        const float *xw = &xs[cur][8 * lane];
+        const float *xw = &xs[cur][0];
         const float *qw = &qs[cur][8 * warp][0];
 #pragma unroll 4
         for (int kk = 0; kk < F_K; kk += 4)
         {
-            const float4 xa = *reinterpret_cast<const float4 *>(xw + kk);
-            const float4 xb = *reinterpret_cast<const float4 *>(xw + kk + 4);
-            const float4 xc = *reinterpret_cast<const float4 *>(xw + kk + 8);
+            const int x0 = 8 * lane + kk;
+            const float4 xa = *reinterpret_cast<const float4 *>(xw + xpos(x0));
+            const float4 xb = *reinterpret_cast<const float4 *>(xw + xpos(x0 + 4));
+            const float4 xc = *reinterpret_cast<const float4 *>(xw + xpos(x0 + 8));
             const float xr[12] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y, xb.z, xb.w, xc.x, xc.y, xc.z, xc.w};
 #pragma unroll
             for (int t = 0; t < 8; t++)
