@@ -39,6 +39,7 @@ struct Fft2Args
     Candidate *cand;
     uint32_t *cand_count, cand_cap;
     float *dbg_d, *dbg_e; // diagnostics: d and e of every window, [t][W]; null in searches
+    float4 *stats;        // per block, kF3S windows' statistics of the current piece (a lane's scratch)
 };
 
 constexpr int kFftRoots = 384; // entries of the twiddle tables

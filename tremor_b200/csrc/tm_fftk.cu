@@ -217,24 +217,44 @@ __device__ __forceinline__ WinIn load_window(const Fft2Args &a, int m, bool in_r
     return w;
 }
 
-// The shared epilogue of both correlation kernels for window g (in the template's range when
-// in_range; its inputs w from load_window): distance and bound from the dot product (taken
-// from the transform in shared memory by `dot_of`, evaluated only for windows that are
-// searched) into up = d + e and lo = d - e (+inf for windows not searched; lo = -inf when the
-// statistics are not trusted), and hit = lo <= the threshold distance.
+// A window's statistics as the epilogue uses them, for one template length: x = mean,
+// y = 1 / std, z and w the two factors of its error term (WindowStats::rel_sd, e_mu);
+// y == 0: the window is not searched (outside the range, first sample missing, constant);
+// y < 0: its statistics are not trusted (it is re-scored exactly whatever its distance).
+// They do not depend on the template, so the epilogues keep them in the block's slice of a
+// global scratch (L2-resident) for the next template of the same length in the same piece.
+__device__ __forceinline__ float4 window_stats4(const Fft2Args &a, int m, double inv_m, bool in_range, uint64_t g,
+                                                const WinIn &w)
+{
+    if (!(in_range && w.raw != kMissing && w.run < (uint32_t)min(m, 65535)))
+        return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    WindowStats ws;
+    if (window_prefix_stats(a.pv, w.qa, w.qb, g, m, inv_m, ws) != 0)
+        return make_float4(0.0f, -1.0f, 0.0f, 0.0f);
+    return make_float4(ws.mu, ws.iv, ws.rel_sd, ws.e_mu);
+}
+
+// The shared epilogue of both correlation kernels for window g with statistics st
+// (window_stats4): distance and bound from the dot product (taken from the transform in
+// shared memory by `dot_of`, evaluated only for windows that are searched) into up = d + e
+// and lo = d - e (+inf for windows not searched; lo = -inf when the statistics are not
+// trusted), and hit = lo <= the threshold distance.
 template <class DotOf>
-__device__ __forceinline__ void corr_eval(const Fft2Args &a, const TemplParam &P, int t, bool in_range, uint64_t g,
-                                          const WinIn &w, float shift, float e_dot, DotOf dot_of, float &up,
-                                          float &lo, bool &hit)
+__device__ __forceinline__ void corr_eval(const Fft2Args &a, const TemplParam &P, int t, uint64_t g, const float4 &st,
+                                          float shift, float e_dot, DotOf dot_of, float &up, float &lo, bool &hit)
 {
     up = inf_f();
     lo = inf_f();
     hit = false;
-    if (!(in_range && w.raw != kMissing && w.run < (uint32_t)min(P.m, 65535)))
+    if (st.y == 0.0f)
         return;
-    WindowStats ws;
-    if (window_prefix_stats(a.pv, w.qa, w.qb, g, P.m, P.inv_m, ws) == 0)
+    if (st.y > 0.0f)
     {
+        WindowStats ws;
+        ws.mu = st.x;
+        ws.iv = st.y;
+        ws.rel_sd = st.z;
+        ws.e_mu = st.w;
         const double dot = dot_of();
         float d, e;
         fast_distance_mixed(P, P.a1_main, (float)dot, ws.mu, ws.iv, shift, stats_error(ws, P.m, P.qs, P.s1), d, e);
@@ -442,8 +462,10 @@ __global__ void __launch_bounds__(kF2T, 1) k_fft2_corr(const Fft2Args a)
     load_roots(R, a.roots);
     const int lane = threadIdx.x & 31;
     const double inv_l = 1.0 / (double)kF2L;
+    float4 *cache = a.stats + (size_t)blockIdx.x * kF3S; // this block's statistics cache
     for (uint32_t pi = blockIdx.x; pi < a.p_count; pi += gridDim.x)
     {
+        int cached_m = -1; // the length whose statistics of this piece the cache holds
         const uint32_t p = a.p_first + pi;
         const double2 *X = a.X + (size_t)p * kF2H;
         const float shift = (float)a.shifts[p];
@@ -504,9 +526,12 @@ __global__ void __launch_bounds__(kF2T, 1) k_fft2_corr(const Fft2Args a)
             // epilogue: windows o = it * 512 + thread (a warp's 32 windows are consecutive)
             const double sm_ = sqrt((double)P.m);
             const float e_dot = (float)(kF2Kappa * norm * sm_ * (2.0 * sm_ + sqrt((double)kF2L)) * 1.01);
+            // the windows' statistics: computed for the first template of a length in this
+            // piece, then read back from the block's cache (each thread reads what it wrote)
+            const bool cached = P.m == cached_m;
             for (int it0 = 0; it0 < kF2S / kF2T; it0 += 4)
             {
-                WinIn w[4];
+                float4 st[4];
                 bool inr[4], hit[4];
                 uint32_t jr[4];
                 float up[4], lo[4];
@@ -516,13 +541,32 @@ __global__ void __launch_bounds__(kF2T, 1) k_fft2_corr(const Fft2Args a)
                     const uint64_t g = piece_w + (uint64_t)((it0 + j) * kF2T) + threadIdx.x;
                     inr[j] = g >= a.w0 && g - a.w0 < P.wcount;
                     jr[j] = inr[j] ? (uint32_t)(g - a.w0) : 0u;
-                    w[j] = load_window(a, P.m, inr[j], g);
+                }
+                if (cached)
+                {
+#pragma unroll
+                    for (int j = 0; j < 4; j++)
+                        st[j] = cache[(it0 + j) * kF2T + threadIdx.x];
+                }
+                else
+                {
+                    WinIn w[4];
+#pragma unroll
+                    for (int j = 0; j < 4; j++)
+                        w[j] = load_window(a, P.m, inr[j], piece_w + (uint64_t)((it0 + j) * kF2T) + threadIdx.x);
+#pragma unroll
+                    for (int j = 0; j < 4; j++)
+                    {
+                        st[j] = window_stats4(a, P.m, P.inv_m, inr[j],
+                                              piece_w + (uint64_t)((it0 + j) * kF2T) + threadIdx.x, w[j]);
+                        cache[(it0 + j) * kF2T + threadIdx.x] = st[j];
+                    }
                 }
 #pragma unroll
                 for (int j = 0; j < 4; j++)
                 {
                     const uint32_t o = (uint32_t)((it0 + j) * kF2T) + threadIdx.x;
-                    corr_eval(a, P, t, inr[j], piece_w + o, w[j], shift, e_dot, [&]() {
+                    corr_eval(a, P, t, piece_w + o, st[j], shift, e_dot, [&]() {
                         const int nn = (int)o + P.m - 1;
                         const double2 c = final_out<1>(buf, R, nn >> 1);
                         return ((nn & 1) ? c.y : c.x) * inv_l;
@@ -535,6 +579,7 @@ __global__ void __launch_bounds__(kF2T, 1) k_fft2_corr(const Fft2Args a)
                     for (int j = 0; j < 4; j++)
                         emit_hits(a, t, lane, hit[j], jr[j]);
             }
+            cached_m = P.m;
         }
     }
 }
@@ -672,8 +717,10 @@ __global__ void __launch_bounds__(kF2T, 1) k_fft3_corr(const Fft2Args a)
     const int lane = threadIdx.x & 31;
     const double inv_l = 1.0 / (double)kF3L;
     constexpr int N = kF3N;
+    float4 *cache = a.stats + (size_t)blockIdx.x * kF3S; // this block's statistics cache
     for (uint32_t pi = blockIdx.x; pi < a.p_count; pi += gridDim.x)
     {
+        int cached_m = -1; // the length whose statistics of this piece the cache holds
         const uint32_t p = a.p_first + pi;
         const double2 *X = a.X + (size_t)p * kF3H;
         const float shift = (float)a.shifts[p];
@@ -694,6 +741,7 @@ __global__ void __launch_bounds__(kF2T, 1) k_fft3_corr(const Fft2Args a)
             const double sm_ = sqrt((double)P.m);
             const float e_dot = (float)(kF3Kappa * norm * sm_ * (2.0 * sm_ + sqrt((double)kF3L)) * 1.01);
             const int base = P.m - 1;
+            const bool cached = P.m == cached_m; // (each thread reads back only what it wrote)
             for (int h = 0; h < 2; h++)
             {
                 __syncthreads(); // the previous half's epilogue has read buf
@@ -750,12 +798,12 @@ __global__ void __launch_bounds__(kF2T, 1) k_fft3_corr(const Fft2Args a)
                 // windows of this half: v -> n0 = 4 ((v >> 1) + (base >> 2)) + 2 h + (v & 1), o = n0 - base
                 for (int it0 = 0; it0 < 17; it0 += 2)
                 {
-                    WinIn w[2];
+                    float4 st[2];
                     bool inr[2], hit[2];
                     uint32_t jr[2];
                     float up[2], lo[2];
                     uint64_t gg[2];
-                    int nn[2];
+                    int nn[2], oo[2];
 #pragma unroll
                     for (int j = 0; j < 2; j++)
                     {
@@ -763,14 +811,34 @@ __global__ void __launch_bounds__(kF2T, 1) k_fft3_corr(const Fft2Args a)
                         nn[j] = 4 * ((v >> 1) + (base >> 2)) + 2 * h + (v & 1);
                         const int o = nn[j] - base;
                         const bool in_piece = it0 + j < 17 && o >= 0 && o < kF3S;
+                        oo[j] = in_piece ? o : -1;
                         gg[j] = piece_w + (uint64_t)(in_piece ? o : 0);
                         inr[j] = in_piece && gg[j] >= a.w0 && gg[j] - a.w0 < P.wcount;
                         jr[j] = inr[j] ? (uint32_t)(gg[j] - a.w0) : 0u;
-                        w[j] = load_window(a, P.m, inr[j], gg[j]);
+                    }
+                    if (cached)
+                    {
+#pragma unroll
+                        for (int j = 0; j < 2; j++)
+                            st[j] = oo[j] >= 0 ? cache[oo[j]] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                    }
+                    else
+                    {
+                        WinIn w[2];
+#pragma unroll
+                        for (int j = 0; j < 2; j++)
+                            w[j] = load_window(a, P.m, inr[j], gg[j]);
+#pragma unroll
+                        for (int j = 0; j < 2; j++)
+                        {
+                            st[j] = window_stats4(a, P.m, P.inv_m, inr[j], gg[j], w[j]);
+                            if (oo[j] >= 0)
+                                cache[oo[j]] = st[j];
+                        }
                     }
 #pragma unroll
                     for (int j = 0; j < 2; j++)
-                        corr_eval(a, P, t, inr[j], gg[j], w[j], shift, e_dot, [&]() {
+                        corr_eval(a, P, t, gg[j], st[j], shift, e_dot, [&]() {
                             const double2 c = final_out<1>(buf, R, nn[j] >> 2);
                             return ((nn[j] & 1) ? c.y : c.x) * inv_l;
                         }, up[j], lo[j], hit[j]);
@@ -782,6 +850,7 @@ __global__ void __launch_bounds__(kF2T, 1) k_fft3_corr(const Fft2Args a)
                             emit_hits(a, t, lane, hit[j], jr[j]);
                 }
             }
+            cached_m = P.m;
         }
     }
 }

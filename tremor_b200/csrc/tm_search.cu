@@ -574,6 +574,7 @@ static void fft_contract_rows(tm_ctx *ctx, Lane &L, const GroupPlan &g, const tm
     DevBuf &Y = long_pieces ? L.fft3_Y : L.fft2_Y;
     Y.reserve(sizeof(double2) * static_cast<size_t>(nr) * H);
     L.fft_rows.reserve(sizeof(int) * static_cast<size_t>(nr));
+    L.fft_stats.reserve(sizeof(float4) * static_cast<size_t>(ctx->sms) * tmb::kF3S);
     TM_CUDA(cudaMemcpyAsync(L.fft_rows.p, rows.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, s));
     if (long_pieces)
     {
@@ -618,6 +619,7 @@ static void fft_contract_rows(tm_ctx *ctx, Lane &L, const GroupPlan &g, const tm
     f.cand_cap = a.cand_cap;
     f.dbg_d = a.dbg_d;
     f.dbg_e = a.dbg_e;
+    f.stats = L.fft_stats.as<float4>();
     TM_CUDA(long_pieces ? tmb::launch_fft3_corr(f, ctx->sms, s) : tmb::launch_fft2_corr(f, ctx->sms, s));
     count_launch(L, 2);
 }
