@@ -19,7 +19,8 @@ path needs no exchange); time is the max over ranks.
 After the timed legs, untimed: every answer of one step is recomputed in FP64
 (`fp64_error`: the error against FP64 stated per result, summarised), and the plain FP32
 kernel runs the same batches (`plain_fp32`, at most 3 steps); `vs_baseline` is value over
-that FP32 rate, the metric's own comparison.
+that FP32 rate, the metric's own comparison. Then a short serving leg (`serving`: config 5's
+2^29-sample record, 150 requests at 200 req/s, p50/p99 latency and the achieved rate).
 
 --impl reference: the reference's own CPU scan (SkipSequentialScan, sequential mode,
 built from the reference sources into oracle/_ref) on a bounded sample of the same
@@ -50,7 +51,7 @@ WORKLOADS = {
     # precision = config 3, plain_knn = config 1, threshold = config 2
     # config 3 names the contraction: split-BF16 tensor cores (the default kernel here)
     'precision': dict(n=1 << 28, q=1024, m=4096, events=2000, mode='knn', k=100, merge=0, corr=0.0,
-                      per_step=128, seed=2028, kernel='bf16'),
+                      per_step=128, seed=2028, kernel='bf16', serving_leg=True),
     'plain_knn': dict(n=1 << 22, q=16, m=1024, events=50, mode='knn', k=10, merge=512, corr=0.0,
                       per_step=16, seed=2026),
     # the precision workload's kernel on 2^25 samples (> L2) and 64 templates: ncu captures
@@ -522,6 +523,59 @@ def run_serving(args, w):
         dist.destroy_process_group()
 
 
+def serving_leg(local, rate=200.0, count=150, batch_ms=0.0):
+    """Config 5 in brief, for the default bench line: the serving workload's record (2^29
+    samples, resident with its prefix sums) and a Poisson stream of `count` requests at `rate`
+    req/s (lengths log-uniform 128-16384, 50/50 kNN / threshold), after 8 untimed warm-up
+    requests. Latency is completion minus submission (the server's steady clock); throughput
+    is all pairs over the span from the first submission to the last completion."""
+    import threading as th
+    import tremor_b200 as tb
+    w = WORKLOADS['serving']
+    x, q = make_workload(w)
+    reqs = requests_for(w, q)
+    rng = np.random.default_rng(w['seed'] + 2)
+    pick = rng.integers(0, len(reqs), size=count)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=count))
+    with tb.Context(x, device=local) as ctx:
+        server = ctx.serve(batch_ms=batch_ms)
+        for i in range(8):
+            server.submit(reqs[i])
+        got = 0
+        while got < 8:
+            got += len(server.poll(64, 1000))
+        tickets = {}
+
+        def submitter():
+            start = time.perf_counter()
+            for i in range(count):
+                delay = arrivals[i] - (time.perf_counter() - start)
+                if delay > 0:
+                    time.sleep(delay)
+                tickets[server.submit(reqs[pick[i]])] = i
+
+        sub = th.Thread(target=submitter)
+        sub.start()
+        done = {}
+        while len(done) < count:
+            for c in server.poll(256, 500):
+                done[c.ticket] = c
+        sub.join()
+        server.stop()
+    comps = list(done.values())
+    if any(c.status != 0 for c in comps):
+        raise RuntimeError('a served request failed')
+    span_ms = max(c.done_ms for c in comps) - min(c.submit_ms for c in comps)
+    lens = [len(reqs[pick[tickets[c.ticket]]].template) for c in comps]
+    lat = np.array([c.done_ms - c.submit_ms for c in comps])
+    return {'workload': 'serving (config 5): 2^29 samples, lengths 128-16384, 50/50 kNN / threshold',
+            'requests': count, 'offered_rate_rps': rate, 'achieved_rate_rps': count / (span_ms / 1e3),
+            'value': sum(w['n'] - m + 1 for m in lens) / (span_ms / 1e3) / 1e9, 'unit': UNIT,
+            'latency_ms': {'p50': float(np.percentile(lat, 50)), 'p99': float(np.percentile(lat, 99)),
+                           'mean': float(lat.mean())},
+            'batch_size_mean': float(np.mean([c.batch_size for c in comps])), 'batch_ms': batch_ms}
+
+
 def run_ours(args, w):
     import torch
     import tremor_b200 as tb
@@ -748,10 +802,16 @@ def run_ours(args, w):
                 'candidates_last_step': ctx.last_candidates(),
                 'phases_ms_per_step': phase_ms,
                 'step_ms': [round(a.elapsed_time(b), 3) for a, b in zip(step_ev, step_ev[1:])]}
-        print(json.dumps(line), flush=True)
     for b in batches:
         b.close()
     ctx.close()
+    if rank == 0:
+        if w.get('serving_leg') and world == 1 and not args.no_serving:
+            try:
+                line['serving'] = serving_leg(local, batch_ms=args.batch_ms)
+            except Exception as exc:  # an informative leg
+                line['serving'] = {'error': str(exc)[:300]}
+        print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
 
@@ -769,6 +829,7 @@ def main():
                    help='tile shape of mixed-length groups (TILES_*)')
     p.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline leg')
     p.add_argument('--no-fp32', action='store_true', help='skip the plain FP32 kernel leg')
+    p.add_argument('--no-serving', action='store_true', help='skip the short serving leg of the default workload')
     p.add_argument('--rate', type=float, default=0.0, help='serving: Poisson arrival rate (req/s)')
     p.add_argument('--requests', type=int, default=0, help='serving: requests in the timed stream')
     p.add_argument('--workers', type=int, default=1, help='serving: batches in flight at once')
