@@ -75,11 +75,12 @@ template <bool MIXED> struct SmemT
     double wl_inv[WL][32];     //   their inverses
     float4 wl_c[WL][32];       //   maxima over their rows of a1, a5, a6 and 1.25 (4 m + 2 qs)
     float wl_b[WL][32];        //   and of 2.5 |s1|
-    float4 win4[W2][TN];       // single-length tiles: window terms (win_terms)
+    float4 win4[W2][TN];       // single-length tiles: window terms (win_terms), then (1/sigma, mu - shift, eb, Q)
     float win_h[W2][TN];
+    float4 coef[8];            // single-length tiles: per epilogue warp, maxima over its rows of (a1, a45, a6, c24)
     Candidate stage[8][STAGE]; // per epilogue warp: candidates before their flush
     uint64_t full_a[S], full_b[S], empty[S];
-    uint64_t acc_full[2], acc_empty[2], win_ready[2], drain;
+    uint64_t acc_full[2], acc_empty[2], win_ready[2], eb_ready[2], drain;
     uint32_t tmem_base;
     int abort;
 };
@@ -350,6 +351,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             mbar_init(&sm.acc_full[b], 1);
             mbar_init(&sm.acc_empty[b], EPI);
             mbar_init(&sm.win_ready[b], EPI);
+            mbar_init(&sm.eb_ready[b], EPI);
         }
         mbar_init(&sm.drain, 1);
         sm.abort = 0;
@@ -506,17 +508,6 @@ __global__ void __launch_bounds__(THREADS, 1)
             const int buf = tc & 1;
             const int tt = (int)(tile / ua.w_tiles);
             const uint32_t j0 = (uint32_t)(tile % ua.w_tiles) * TN;
-            if (!MIXED)
-            {
-                const uint32_t j = j0 + et; // one window per epilogue thread
-                float h;
-                sm.win4[buf & (Sm::W2 - 1)][et] =
-                    j < a.W ? win_terms(a.mean[j], a.inv[j], tile_shift<false>(a, j0), h) : skip_terms(h);
-                sm.win_h[buf & (Sm::W2 - 1)][et] = h;
-                mbar_arrive(&sm.win_ready[buf]);
-                if (!mbar_wait_warp(&sm.win_ready[buf], (tc >> 1) & 1, sm.abort, ua.err, 7))
-                    goto done;
-            }
             const float shift = tile_shift<MIXED>(a, j0);
             const int t = tt * TM + row;
             TemplParam p;
@@ -530,6 +521,38 @@ __global__ void __launch_bounds__(THREADS, 1)
             {
                 p = TemplParam{};
                 p.thr_ed = -kFltMax;
+            }
+            if (!MIXED)
+            {
+                // the window part of the bound once per window, with the maxima over the
+                // tile's rows of its coefficients (all >= 0, so the maxima bound every row's):
+                // each warp reduces its rows, the window terms are staged, and after the
+                // barrier each thread folds the 8 warps' maxima into its window's eb
+                const int wb = buf & (Sm::W2 - 1);
+                const float c1 = warp_max_nonneg(valid, p.a1_main), c45 = warp_max_nonneg(valid, 2.0f * p.a4 + p.a5);
+                const float c6 = warp_max_nonneg(valid, p.a6), c24 = warp_max_nonneg(valid, p.a2 + p.a4);
+                if (lane == 0)
+                    sm.coef[ew] = make_float4(c1, c45, c6, c24);
+                const uint32_t j = j0 + et; // one window per epilogue thread
+                float h;
+                sm.win4[wb][et] = j < a.W ? win_terms(a.mean[j], a.inv[j], shift, h) : skip_terms(h);
+                sm.win_h[wb][et] = h;
+                mbar_arrive(&sm.win_ready[buf]);
+                if (!mbar_wait_warp(&sm.win_ready[buf], (tc >> 1) & 1, sm.abort, ua.err, 7))
+                    goto done;
+                float4 cm = sm.coef[0];
+#pragma unroll
+                for (int w = 1; w < 8; w++)
+                {
+                    const float4 c = sm.coef[w];
+                    cm = make_float4(fmaxf(cm.x, c.x), fmaxf(cm.y, c.y), fmaxf(cm.z, c.z), fmaxf(cm.w, c.w));
+                }
+                float4 wt = sm.win4[wb][et]; // each thread rewrites only its own window's entry
+                wt.z = fmaf(cm.x, wt.z, fmaf(cm.y, wt.w, fmaf(cm.z, sm.win_h[wb][et], cm.w))); // eb (NaN: not searched)
+                sm.win4[wb][et] = wt;
+                mbar_arrive(&sm.eb_ready[buf]);
+                if (!mbar_wait_warp(&sm.eb_ready[buf], (tc >> 1) & 1, sm.abort, ua.err, 8))
+                    goto done;
             }
             // mixed: the distinct lengths of this warp's rows (at most 32), found while the
             // tile's MMAs run; my_d is the lane's entry
@@ -642,17 +665,46 @@ __global__ void __launch_bounds__(THREADS, 1)
             {
                 const int wb = buf & (Sm::W2 - 1);
                 const LaneTerms lt = lane_terms(p, valid);
+                // a warp whose rows are all kNN (or padding) needs only the minima, one whose
+                // rows are all threshold rows only the mask
+                const bool all_knn = __all_sync(0xffffffffu, !valid || p.mode == 1);
+                const bool all_thr = __all_sync(0xffffffffu, !valid || p.mode != 1);
                 for (int c = 8 * half; c < 8 * half + 8; c++) // this warp's 128 of the 256 columns
                 {
                     float v[16];
                     tmem_ld16(taddr + c * 16, v);
                     uint32_t mask = 0;
-#pragma unroll
-                    for (int i = 0; i < 16; i++)
+                    if (all_knn)
                     {
-                        const float4 w = sm.win4[wb][c * 16 + i];
-                        const float eb = fmaf(lt.a1, w.z, fmaf(lt.a45, w.w, fmaf(lt.a6, sm.win_h[wb][c * 16 + i], lt.c24)));
-                        pair_update(lt, v[i], w.x, w.y, eb, i, mask, umin, lmin);
+#pragma unroll
+                        for (int i = 0; i < 16; i++)
+                        {
+                            const float4 w = sm.win4[wb][c * 16 + i];
+                            float d, e;
+                            pair_bound(lt, v[i], w.x, w.y, w.z, d, e);
+                            umin = fminf(umin, d + e);
+                            lmin = fminf(lmin, d - e);
+                        }
+                    }
+                    else if (all_thr)
+                    {
+#pragma unroll
+                        for (int i = 0; i < 16; i++)
+                        {
+                            const float4 w = sm.win4[wb][c * 16 + i];
+                            float d, e;
+                            pair_bound(lt, v[i], w.x, w.y, w.z, d, e);
+                            mask |= (d - e <= lt.thr ? 1u : 0u) << i;
+                        }
+                    }
+                    else
+                    {
+#pragma unroll
+                        for (int i = 0; i < 16; i++)
+                        {
+                            const float4 w = sm.win4[wb][c * 16 + i];
+                            pair_update(lt, v[i], w.x, w.y, w.z, i, mask, umin, lmin);
+                        }
                     }
                     if (a.dbg_d != nullptr && valid)
                         for (int i = 0; i < 16; i++)
@@ -660,16 +712,15 @@ __global__ void __launch_bounds__(THREADS, 1)
                             const float4 w = sm.win4[wb][c * 16 + i];
                             if (w.x == 0.0f)
                                 continue;
-                            const float eb =
-                                fmaf(lt.a1, w.z, fmaf(lt.a45, w.w, fmaf(lt.a6, sm.win_h[wb][c * 16 + i], lt.c24)));
                             float dd, e;
-                            pair_bound(lt, v[i], w.x, w.y, eb, dd, e);
+                            pair_bound(lt, v[i], w.x, w.y, w.z, dd, e);
                             const size_t at = (size_t)t * a.W + j0 + c * 16 + i;
                             a.dbg_d[at] = dd;
                             a.dbg_e[at] = e;
                         }
-                    stage_emit<STAGE>(mask, lane, (uint32_t)t, j0 + c * 16, sm.stage[ew], staged, a.cand, a.cand_count,
-                                      a.cand_cap);
+                    if (!all_knn)
+                        stage_emit<STAGE>(mask, lane, (uint32_t)t, j0 + c * 16, sm.stage[ew], staged, a.cand,
+                                          a.cand_count, a.cand_cap);
                 }
             }
             tc_fence_before();
