@@ -34,6 +34,14 @@ struct WindowStats
     float e_mu;   // bound on the absolute error of the mean
 };
 
+// An upper bound on sqrt(x) for x >= 0 (0 for x = 0) from the fast reciprocal square root:
+// its relative error is below 2^-21, so the factor 1 + 2^-19 keeps the result above sqrt(x).
+// For the error-bound terms only (never for a value).
+__device__ __forceinline__ float sqrt_up(float x)
+{
+    return x > 0.0f ? x * rsqrtf(x) * (1.0f + 1.9073486e-06f) : 0.0f;
+}
+
 // Bound on the distance error that statistics with these error bounds can cause, for a
 // template of length m with |q| sqrt(m) = qs and sum q = s1q (added to e).
 __device__ __forceinline__ float stats_error(const WindowStats &w, int m, float qs, float s1q)
@@ -71,7 +79,8 @@ __device__ __forceinline__ int window_prefix_stats(const PrefixView &pv, double2
         s2 = Qb.y - Qa.y;
         const float nb = (float)(e - (b1 << kPrefixBlockLog));
         e_s2 = fg * (qa + qb);
-        e_s1 = 1.001f * fg * (sqrtf(na * qa) + sqrtf(nb * qb));
+        // sqrt(na qa) + sqrt(nb qb) <= sqrt(2 (na qa + nb qb)) (Cauchy-Schwarz)
+        e_s1 = 1.001f * fg * sqrt_up(2.0f * (na * qa + nb * qb));
     }
     else
     {
@@ -82,10 +91,10 @@ __device__ __forceinline__ int window_prefix_stats(const PrefixView &pv, double2
         s2 = (t.y - Qa.y) + (Qb.y + (2.0 * d * Qb.x + n2 * d * d));
         const float tq = (float)t.y, fd = fabsf((float)d), fn2 = (float)n2, q1b = fabsf((float)Qb.x);
         const float nt = (float)kPrefixBlock;
-        const float eq1b = 1.001f * fg * sqrtf(fn2 * qb);
+        const float eq1b = 1.001f * fg * sqrt_up(fn2 * qb);
         e_s2 = fg * (tq + qa + qb) + 2.0f * fd * eq1b + 8.0f * fe * (2.0f * fd * q1b + fn2 * fd * fd) +
                4.0f * fe * fd * (q1b + fn2 * fd);
-        e_s1 = 1.001f * fg * (sqrtf(nt * tq) + sqrtf(na * qa)) + eq1b + 4.0f * fe * fn2 * fd +
+        e_s1 = 1.001f * fg * sqrt_up(2.0f * (nt * tq + na * qa)) + eq1b + 4.0f * fe * fn2 * fd +
                4.0f * fe * (fabsf((float)t.x) + fabsf((float)Qa.x) + q1b + fn2 * fd);
     }
     const double mu_c = s1 * inv_m;
@@ -94,7 +103,8 @@ __device__ __forceinline__ int window_prefix_stats(const PrefixView &pv, double2
     if (!(var > 1e-22) || !(var < 1e36))
         return 2;
     const float fvar = (float)var, fmu = (float)mu_c;
-    const float fm = (float)m, fim = 1.0f / fm;
+    // 1 / m from the caller's FP64 inverse, rounded up (a factor for the bounds only)
+    const float fm = (float)m, fim = (float)inv_m * (1.0f + 1.1920929e-07f);
     const float fs2 = fm * (fvar + fmu * fmu) * 1.0001f;
     e_s2 += 4.0f * fe * fs2;
     e_s1 += 4.0f * fe * fm * fabsf(fmu);
