@@ -12,7 +12,7 @@ from tests import oracle_bindings as ob
 pytestmark = pytest.mark.gpu
 
 # every branch of the mixed-length contraction: 128-template row tiles (k_scan_umma),
-# column tiles of 128 / 64 / 32 templates (k_scan_wm), the FP64 FFT branch (tm_fft.cu)
+# column tiles of 128 / 64 / 32 templates (k_scan_wm), the FP64 FFT branch (tm_fftk.cu)
 TILES = [tb.TILES_ROWS, tb.TILES_COLS_128, tb.TILES_COLS_64, tb.TILES_COLS_32, tb.TILES_FFT]
 
 
