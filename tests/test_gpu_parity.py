@@ -138,6 +138,38 @@ def test_window_range_is_a_partition(kernel):
         assert np.array_equal(D.view(np.uint32), Do.view(np.uint32))
 
 
+@pytest.mark.parametrize('merge', [0, 64, 700])
+def test_partitioned_knn_equals_whole_record(merge):
+    """kNN over three window partitions (one context each, as three ranks would hold
+    them): every partition's candidates (replicas.knn_candidates, two device searches)
+    and the canonical selection over their union equal the whole record's kNN, with
+    near-copies of a template planted on both sides of each partition boundary."""
+    from tremor_b200 import replicas
+    x = _waveform(1 << 16, 23)
+    m, k = 128, 10
+    rng = np.random.default_rng(24)
+    q = _templates(x, m, rng, 3)
+    W = len(x) - m + 1
+    parts = [replicas.partition(W, 3, r) for r in range(3)]
+    for first, _ in parts[1:]:  # m + 5 apart, one on each side of the boundary
+        for off, eps in ((-m - 3, 0.02), (2, 0.005)):
+            x[first + off:first + off + m] = q[0] + eps * np.std(q[0]) * rng.normal(size=m).astype(np.float32)
+    with tb.Context(x) as whole:
+        I, D = whole.search_knn(q, k, merge)
+    cands = []
+    for first, count in parts:
+        with tb.Context(x) as ctx:
+            ctx.set_window_range(first, count)
+            cands.append(replicas.knn_candidates(ctx, list(q), k, merge))
+    for i in range(len(q)):
+        p = np.concatenate([c[i][0] for c in cands])
+        d = np.concatenate([c[i][1] for c in cands])
+        Ip, Dp = replicas.select_knn(p, d, k, merge)
+        assert np.array_equal(Ip, I[i]) and np.array_equal(Dp.view(np.uint32), D[i].view(np.uint32)), (merge, i)
+    for first, _ in parts[1:]:
+        assert first + 2 in I[0] and (first - m - 3 in I[0]) == (merge <= m + 5)
+
+
 @pytest.mark.parametrize('kernel', KERNELS)
 def test_config1_shape_self_match_and_oracle(kernel):
     """The plain kNN workload's shape (2^22 samples, m=1024, k=10, merge m/2): planted
