@@ -10,8 +10,9 @@ constant) for every answer of the golden fixtures and of a record with constant 
   (plus 1e-9 absolute, for distances near 0) of NumPy's;
 * padding (kNN slots the exclusion zone leaves empty, distance FLT_MAX, as the 'sparse'
   fixture has): +inf;
-* the returned FP32 distance within the north-star tolerance (1e-4 relative) of FP64
-  wherever FP64 is finite.
+* the returned FP32 distance within the FP32 error model of FP64 wherever FP64 is finite:
+  |D - D64| <= 1e-4 D64 + 2^-20 sqrt(m D64) + m 2^-44 (1e-4 relative away from 0; exact
+  copies of a template, distance near 0, are held to the absolute terms).
 """
 import numpy as np
 import pytest
@@ -53,8 +54,11 @@ def _check(x, requests, answers, what):
         got = d64[~pad]
         assert np.all(np.isfinite(ref)), f'{what}: an answer on a constant window'
         assert np.all(np.abs(got - ref) <= 1e-12 * ref + 1e-9), (what, np.max(np.abs(got - ref)))
-        rel = tb.Context.relative_error(dist[~pad], got)
-        assert np.all(rel[np.isfinite(rel)] <= 1e-4), (what, np.nanmax(rel))
+        # the FP32 error model of the reference's distance (exact copies have distances near 0,
+        # where its absolute error of a few ulps of the per-sample terms dominates)
+        m = len(r.template)
+        err = np.abs(dist[~pad].astype(np.float64) - got)
+        assert np.all(err <= 1e-4 * got + 2.0 ** -20 * np.sqrt(m * got) + m * 2.0 ** -44), (what, err.max())
     return padded
 
 
