@@ -269,7 +269,7 @@ struct Lane
     HostBuf h_split, h_q, h_order, h_slots, h_counters;
     uint32_t cand_cap = 1u << 22, list_cap = 1u << 20;
     // FFT branch: the template spectra and rows of a launch (both piece lengths)
-    DevBuf fft2_Y, fft3_Y, fft_rows, fft_stats; // (fft_stats: the correlation kernels' per-block statistics cache)
+    DevBuf fft2_Y, fft3_Y, fft_rows, fft_stats, fft_gmax; // (fft_stats: the correlation kernels' per-block statistics cache; fft_gmax: per row, its length's largest bound coefficients)
     // instrumentation
     bool profile = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr, ev4 = nullptr;
@@ -293,7 +293,7 @@ struct Lane
         if (stream)
             cudaStreamSynchronize(stream);
         for (DevBuf *b : {&tkey, &bmin_u, &bmin_l, &list, &counters, &cand, &dist, &akeys, &avals, &avals64, &sort_tmp,
-                          &segs, &fft2_Y, &fft3_Y, &fft_rows, &fft_stats})
+                          &segs, &fft2_Y, &fft3_Y, &fft_rows, &fft_stats, &fft_gmax})
             b->release();
         for (HostBuf *b : {&h_split, &h_q, &h_order, &h_slots, &h_counters})
             b->release();

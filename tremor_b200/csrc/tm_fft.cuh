@@ -39,8 +39,16 @@ struct Fft2Args
     Candidate *cand;
     uint32_t *cand_count, cand_cap;
     float *dbg_d, *dbg_e; // diagnostics: d and e of every window, [t][W]; null in searches
-    float4 *stats;        // per block, kF3S windows' statistics of the current piece (a lane's scratch)
+    float4 *stats;        // per block, kFftCache windows' folded statistics of the current piece (a lane's scratch)
+    // per template row t, the largest bound coefficients of the launch's templates of its
+    // length: gmax[2 t] = (a1_main, a2, a5, a6), gmax[2 t + 1] = (qs, |s1|, 0, 0)
+    const float4 *gmax;
 };
+
+// Work items of one half of a kF3 piece's epilogue (one complex output each, two windows),
+// rounded up; a block's statistics cache holds two windows per item of both halves.
+constexpr int kF3Items = 4104;
+constexpr int kFftCache = 4 * kF3Items;
 
 constexpr int kFftRoots = 384; // entries of the twiddle tables
 constexpr int kFftScratchPts = 8192; // complex points of a block's slice of the forward scratch

@@ -221,8 +221,9 @@ __device__ __forceinline__ WinIn load_window(const Fft2Args &a, int m, bool in_r
 // y = 1 / std, z and w the two factors of its error term (WindowStats::rel_sd, e_mu);
 // y == 0: the window is not searched (outside the range, first sample missing, constant);
 // y < 0: its statistics are not trusted (it is re-scored exactly whatever its distance).
-// They do not depend on the template, so the epilogues keep them in the block's slice of a
-// global scratch (L2-resident) for the next template of the same length in the same piece.
+// They do not depend on the template: the epilogues fold them (fold_window) and keep them in
+// the block's slice of a global scratch (L2-resident) for the next template of the same
+// length in the same piece.
 __device__ __forceinline__ float4 window_stats4(const Fft2Args &a, int m, double inv_m, bool in_range, uint64_t g,
                                                 const WinIn &w)
 {
@@ -234,14 +235,36 @@ __device__ __forceinline__ float4 window_stats4(const Fft2Args &a, int m, double
     return make_float4(ws.mu, ws.iv, ws.rel_sd, ws.e_mu);
 }
 
-// The shared epilogue of both correlation kernels for window g with statistics st
-// (window_stats4): distance and bound from the dot product (taken from the transform in
-// shared memory by `dot_of`, evaluated only for windows that are searched) into up = d + e
-// and lo = d - e (+inf for windows not searched; lo = -inf when the statistics are not
-// trusted), and hit = lo <= the threshold distance.
-template <class DotOf>
-__device__ __forceinline__ void corr_eval(const Fft2Args &a, const TemplParam &P, int t, uint64_t g, const float4 &st,
-                                          float shift, float e_dot, DotOf dot_of, float &up, float &lo, bool &hit)
+// The folded statistics of a window for the templates of one length in one piece (what the
+// block's cache holds): x = mu - shift, y = 1 / std as in window_stats4 (0: not searched;
+// < 0: statistics not trusted), z = every term of the distance bound that does not depend
+// on the dot product's distance: fast_distance_mixed's bound without its a3 max(d, 0) term,
+// with the largest coefficients c0 = (a1, a2, a5, a6), c1 = (qs, |s1|) of the launch's
+// templates of this length (so it bounds each of them), plus the transform's error
+// 2 e_dot / std.
+__device__ __forceinline__ float4 fold_window(const float4 &st, const float4 &c0, const float4 &c1, int m, float shift,
+                                              float e_dot)
+{
+    if (!(st.y > 0.0f))
+        return make_float4(0.0f, st.y, 0.0f, 0.0f);
+    const float mu = st.x, iv = st.y, ms = mu - shift;
+    const float r = ms * iv, r0 = mu * iv;
+    WindowStats ws;
+    ws.mu = mu;
+    ws.iv = iv;
+    ws.rel_sd = st.z;
+    ws.e_mu = st.w;
+    const float ew = c0.x * sqrtf(1.0f + r * r) + c0.y + c0.z * r0 * r0 + c0.w * (fabsf(mu) + fabsf(shift)) * iv +
+                     stats_error(ws, m, c1.x, c1.y) + 2.0f * e_dot * iv * 1.01f;
+    return make_float4(ms, iv, ew, 0.0f);
+}
+
+// The per-template epilogue of window jr (relative to w0) with folded statistics st and dot
+// product dot: d as fast_distance_mixed, up = d + e and lo = d - e (+inf for windows not
+// searched; lo = -inf when the statistics are not trusted), hit = lo <= the threshold
+// distance.
+__device__ __forceinline__ void corr_eval(const Fft2Args &a, const TemplParam &P, int t, uint32_t jr, const float4 &st,
+                                          double dot, float &up, float &lo, bool &hit)
 {
     up = inf_f();
     lo = inf_f();
@@ -250,18 +273,11 @@ __device__ __forceinline__ void corr_eval(const Fft2Args &a, const TemplParam &P
         return;
     if (st.y > 0.0f)
     {
-        WindowStats ws;
-        ws.mu = st.x;
-        ws.iv = st.y;
-        ws.rel_sd = st.z;
-        ws.e_mu = st.w;
-        const double dot = dot_of();
-        float d, e;
-        fast_distance_mixed(P, P.a1_main, (float)dot, ws.mu, ws.iv, shift, stats_error(ws, P.m, P.qs, P.s1), d, e);
-        e += 2.0f * e_dot * ws.iv * 1.01f;
+        const float cross = ((float)dot - st.x * P.s1) * st.y;
+        const float d = P.c_lin - 2.0f * cross;
+        const float e = st.z + P.a3 * fmaxf(d, 0.0f);
         if (a.dbg_d != nullptr)
         {
-            const uint32_t jr = (uint32_t)(g - a.w0);
             a.dbg_d[(size_t)t * a.W + jr] = d;
             a.dbg_e[(size_t)t * a.W + jr] = e;
         }
@@ -462,7 +478,7 @@ __global__ void __launch_bounds__(kF2T, 1) k_fft2_corr(const Fft2Args a)
     load_roots(R, a.roots);
     const int lane = threadIdx.x & 31;
     const double inv_l = 1.0 / (double)kF2L;
-    float4 *cache = a.stats + (size_t)blockIdx.x * kF3S; // this block's statistics cache
+    float4 *cache = a.stats + (size_t)blockIdx.x * kFftCache; // this block's statistics cache
     for (uint32_t pi = blockIdx.x; pi < a.p_count; pi += gridDim.x)
     {
         int cached_m = -1; // the length whose statistics of this piece the cache holds
@@ -523,14 +539,25 @@ __global__ void __launch_bounds__(kF2T, 1) k_fft2_corr(const Fft2Args a)
             }
             __syncthreads();
             fft8192_r16<1>(buf, R);
-            // epilogue: windows o = it * 512 + thread (a warp's 32 windows are consecutive)
+            // epilogue: work item u = it * 512 + thread takes output i = (base >> 1) + u of the
+            // final pass (base = m - 1), whose real and imaginary parts are the dot products of
+            // windows o = 2 u - odd and 2 u - odd + 1 (odd = base & 1; with odd base, item 0
+            // has only window 0 and item 4096 only window 8191). Window o is in the template's
+            // range when o_lo <= o < o_hi; jr = rel + o is its index relative to w0.
+            const int base = P.m - 1, odd = base & 1, nitems = kF2S / 2 + odd;
+            const int64_t rel = (int64_t)piece_w - (int64_t)a.w0;
+            const int o_lo = (int)(rel < 0 ? -rel : 0);
+            const int o_hi = (int)((int64_t)P.wcount - rel < (int64_t)kF2S ? (int64_t)P.wcount - rel : (int64_t)kF2S);
             const double sm_ = sqrt((double)P.m);
             const float e_dot = (float)(kF2Kappa * norm * sm_ * (2.0 * sm_ + sqrt((double)kF2L)) * 1.01);
-            // the windows' statistics: computed for the first template of a length in this
-            // piece, then read back from the block's cache (each thread reads what it wrote)
+            // the windows' folded statistics: computed for the first template of a length in
+            // this piece, then read back from the block's cache (each thread reads what it wrote)
             const bool cached = P.m == cached_m;
-            for (int it0 = 0; it0 < kF2S / kF2T; it0 += 4)
+            const float4 c0 = a.gmax[2 * t], c1 = a.gmax[2 * t + 1];
+            for (int it0 = 0; it0 < 10; it0 += 2)
             {
+                if (it0 * kF2T + (int)(threadIdx.x & ~31u) >= nitems)
+                    continue; // no item of this warp (uniform across the warp)
                 float4 st[4];
                 bool inr[4], hit[4];
                 uint32_t jr[4];
@@ -538,42 +565,46 @@ __global__ void __launch_bounds__(kF2T, 1) k_fft2_corr(const Fft2Args a)
 #pragma unroll
                 for (int j = 0; j < 4; j++)
                 {
-                    const uint64_t g = piece_w + (uint64_t)((it0 + j) * kF2T) + threadIdx.x;
-                    inr[j] = g >= a.w0 && g - a.w0 < P.wcount;
-                    jr[j] = inr[j] ? (uint32_t)(g - a.w0) : 0u;
+                    const int u = (it0 + (j >> 1)) * kF2T + (int)threadIdx.x;
+                    const int o = 2 * u - odd + (j & 1);
+                    inr[j] = u < nitems && o >= o_lo && o < o_hi;
+                    jr[j] = (uint32_t)rel + (uint32_t)o;
                 }
                 if (cached)
                 {
 #pragma unroll
                     for (int j = 0; j < 4; j++)
-                        st[j] = cache[(it0 + j) * kF2T + threadIdx.x];
+                        st[j] = inr[j] ? cache[2 * ((it0 + (j >> 1)) * kF2T + (int)threadIdx.x) + (j & 1)]
+                                       : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                 }
                 else
                 {
                     WinIn w[4];
 #pragma unroll
                     for (int j = 0; j < 4; j++)
-                        w[j] = load_window(a, P.m, inr[j], piece_w + (uint64_t)((it0 + j) * kF2T) + threadIdx.x);
+                        w[j] = load_window(a, P.m, inr[j], (uint64_t)((int64_t)a.w0 + (int64_t)jr[j]));
 #pragma unroll
                     for (int j = 0; j < 4; j++)
                     {
-                        st[j] = window_stats4(a, P.m, P.inv_m, inr[j],
-                                              piece_w + (uint64_t)((it0 + j) * kF2T) + threadIdx.x, w[j]);
-                        cache[(it0 + j) * kF2T + threadIdx.x] = st[j];
+                        st[j] = fold_window(window_stats4(a, P.m, P.inv_m, inr[j],
+                                                          (uint64_t)((int64_t)a.w0 + (int64_t)jr[j]), w[j]),
+                                            c0, c1, P.m, shift, e_dot);
+                        if (inr[j])
+                            cache[2 * ((it0 + (j >> 1)) * kF2T + (int)threadIdx.x) + (j & 1)] = st[j];
                     }
                 }
 #pragma unroll
-                for (int j = 0; j < 4; j++)
+                for (int j = 0; j < 4; j += 2)
                 {
-                    const uint32_t o = (uint32_t)((it0 + j) * kF2T) + threadIdx.x;
-                    corr_eval(a, P, t, piece_w + o, st[j], shift, e_dot, [&]() {
-                        const int nn = (int)o + P.m - 1;
-                        const double2 c = final_out<1>(buf, R, nn >> 1);
-                        return ((nn & 1) ? c.y : c.x) * inv_l;
-                    }, up[j], lo[j], hit[j]);
+                    const int u = (it0 + (j >> 1)) * kF2T + (int)threadIdx.x;
+                    double2 c = make_double2(0.0, 0.0);
+                    if (inr[j] || inr[j + 1])
+                        c = final_out<1>(buf, R, (base >> 1) + u);
+                    corr_eval(a, P, t, jr[j], st[j], c.x * inv_l, up[j], lo[j], hit[j]);
+                    corr_eval(a, P, t, jr[j + 1], st[j + 1], c.y * inv_l, up[j + 1], lo[j + 1], hit[j + 1]);
                 }
                 if (P.mode == TM_MODE_KNN)
-                    bucket_minima<4>(a, t, lane, inr, jr, up, lo); // the group spans 3 x 512 + 32 windows
+                    bucket_minima<4>(a, t, lane, inr, jr, up, lo); // the group spans 512 x 2 + 64 windows
                 else
 #pragma unroll
                     for (int j = 0; j < 4; j++)
@@ -717,7 +748,7 @@ __global__ void __launch_bounds__(kF2T, 1) k_fft3_corr(const Fft2Args a)
     const int lane = threadIdx.x & 31;
     const double inv_l = 1.0 / (double)kF3L;
     constexpr int N = kF3N;
-    float4 *cache = a.stats + (size_t)blockIdx.x * kF3S; // this block's statistics cache
+    float4 *cache = a.stats + (size_t)blockIdx.x * kFftCache; // this block's statistics cache
     for (uint32_t pi = blockIdx.x; pi < a.p_count; pi += gridDim.x)
     {
         int cached_m = -1; // the length whose statistics of this piece the cache holds
@@ -742,6 +773,10 @@ __global__ void __launch_bounds__(kF2T, 1) k_fft3_corr(const Fft2Args a)
             const float e_dot = (float)(kF3Kappa * norm * sm_ * (2.0 * sm_ + sqrt((double)kF3L)) * 1.01);
             const int base = P.m - 1;
             const bool cached = P.m == cached_m; // (each thread reads back only what it wrote)
+            const float4 c0 = a.gmax[2 * t], c1 = a.gmax[2 * t + 1];
+            const int64_t rel = (int64_t)piece_w - (int64_t)a.w0;
+            const int o_lo = (int)(rel < 0 ? -rel : 0);
+            const int o_hi = (int)((int64_t)P.wcount - rel < (int64_t)kF3S ? (int64_t)P.wcount - rel : (int64_t)kF3S);
             for (int h = 0; h < 2; h++)
             {
                 __syncthreads(); // the previous half's epilogue has read buf
@@ -795,55 +830,57 @@ __global__ void __launch_bounds__(kF2T, 1) k_fft3_corr(const Fft2Args a)
                 }
                 __syncthreads();
                 fft8192_r16<1>(buf, R);
-                // windows of this half: v -> n0 = 4 ((v >> 1) + (base >> 2)) + 2 h + (v & 1), o = n0 - base
-                for (int it0 = 0; it0 < 17; it0 += 2)
+                // work item u = it * 512 + thread of this half takes output k = (base >> 2) + u of
+                // its transform, c[2 k + h] of the whole one, whose real and imaginary parts are
+                // the dot products of windows o = 4 u - (base & 3) + 2 h and o + 1 (those in
+                // [o_lo, o_hi)); u <= 4096 covers the piece's windows (o_hi <= 16384 keeps u, and
+                // so k <= 8191, in bounds wherever a window is in range).
+                for (int it = 0; it < 9; it++)
                 {
+                    if (it * kF2T + (int)(threadIdx.x & ~31u) >= kF3Items)
+                        continue; // no item of this warp (uniform across the warp)
+                    const int u = it * kF2T + (int)threadIdx.x;
+                    const int o0 = 4 * u - (base & 3) + 2 * h;
                     float4 st[2];
                     bool inr[2], hit[2];
                     uint32_t jr[2];
                     float up[2], lo[2];
-                    uint64_t gg[2];
-                    int nn[2], oo[2];
 #pragma unroll
                     for (int j = 0; j < 2; j++)
                     {
-                        const int v = (it0 + j) * kF2T + (int)threadIdx.x;
-                        nn[j] = 4 * ((v >> 1) + (base >> 2)) + 2 * h + (v & 1);
-                        const int o = nn[j] - base;
-                        const bool in_piece = it0 + j < 17 && o >= 0 && o < kF3S;
-                        oo[j] = in_piece ? o : -1;
-                        gg[j] = piece_w + (uint64_t)(in_piece ? o : 0);
-                        inr[j] = in_piece && gg[j] >= a.w0 && gg[j] - a.w0 < P.wcount;
-                        jr[j] = inr[j] ? (uint32_t)(gg[j] - a.w0) : 0u;
+                        inr[j] = u < kF3Items && o0 + j >= o_lo && o0 + j < o_hi;
+                        jr[j] = (uint32_t)rel + (uint32_t)(o0 + j);
                     }
+                    float4 *slot = cache + h * 2 * kF3Items + 2 * u;
                     if (cached)
                     {
 #pragma unroll
                         for (int j = 0; j < 2; j++)
-                            st[j] = oo[j] >= 0 ? cache[oo[j]] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                            st[j] = inr[j] ? slot[j] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                     }
                     else
                     {
                         WinIn w[2];
 #pragma unroll
                         for (int j = 0; j < 2; j++)
-                            w[j] = load_window(a, P.m, inr[j], gg[j]);
+                            w[j] = load_window(a, P.m, inr[j], (uint64_t)((int64_t)a.w0 + (int64_t)jr[j]));
 #pragma unroll
                         for (int j = 0; j < 2; j++)
                         {
-                            st[j] = window_stats4(a, P.m, P.inv_m, inr[j], gg[j], w[j]);
-                            if (oo[j] >= 0)
-                                cache[oo[j]] = st[j];
+                            st[j] = fold_window(window_stats4(a, P.m, P.inv_m, inr[j],
+                                                              (uint64_t)((int64_t)a.w0 + (int64_t)jr[j]), w[j]),
+                                                c0, c1, P.m, shift, e_dot);
+                            if (inr[j])
+                                slot[j] = st[j];
                         }
                     }
-#pragma unroll
-                    for (int j = 0; j < 2; j++)
-                        corr_eval(a, P, t, gg[j], st[j], shift, e_dot, [&]() {
-                            const double2 c = final_out<1>(buf, R, nn[j] >> 2);
-                            return ((nn[j] & 1) ? c.y : c.x) * inv_l;
-                        }, up[j], lo[j], hit[j]);
+                    double2 c = make_double2(0.0, 0.0);
+                    if (inr[0] || inr[1])
+                        c = final_out<1>(buf, R, (base >> 2) + u);
+                    corr_eval(a, P, t, jr[0], st[0], c.x * inv_l, up[0], lo[0], hit[0]);
+                    corr_eval(a, P, t, jr[1], st[1], c.y * inv_l, up[1], lo[1], hit[1]);
                     if (P.mode == TM_MODE_KNN)
-                        bucket_minima<2>(a, t, lane, inr, jr, up, lo); // the group spans 1024 + 64 windows
+                        bucket_minima<2>(a, t, lane, inr, jr, up, lo); // the warp spans 4 x 32 windows
                     else
 #pragma unroll
                         for (int j = 0; j < 2; j++)

@@ -2,6 +2,7 @@
 // resident prefix sums), the contraction kernel or the FFT branch with its bounded
 // epilogue, the kNN bound and FP32 re-pass, exact re-scoring, and the answers assembled on
 // the device and handed to the result in pinned memory.
+#include <unordered_map>
 #include "tm_core.h"
 
 namespace tmh {
@@ -574,8 +575,29 @@ static void fft_contract_rows(tm_ctx *ctx, Lane &L, const GroupPlan &g, const tm
     DevBuf &Y = long_pieces ? L.fft3_Y : L.fft2_Y;
     Y.reserve(sizeof(double2) * static_cast<size_t>(nr) * H);
     L.fft_rows.reserve(sizeof(int) * static_cast<size_t>(nr));
-    L.fft_stats.reserve(sizeof(float4) * static_cast<size_t>(ctx->sms) * tmb::kF3S);
+    L.fft_stats.reserve(sizeof(float4) * static_cast<size_t>(ctx->sms) * tmb::kFftCache);
     TM_CUDA(cudaMemcpyAsync(L.fft_rows.p, rows.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, s));
+    // per row, the largest bound coefficients of the rows of its length (the epilogue's
+    // folded window statistics serve every template of one length in a piece)
+    std::vector<float4> gmax(2 * static_cast<size_t>(g.T), make_float4(0.0f, 0.0f, 0.0f, 0.0f));
+    std::unordered_map<int, std::pair<float4, float4>> by_m;
+    for (int t : rows)
+    {
+        const TemplParam &q = g.htp[static_cast<size_t>(t)];
+        auto it = by_m.emplace(q.m, std::make_pair(make_float4(0.0f, 0.0f, 0.0f, 0.0f),
+                                                   make_float4(0.0f, 0.0f, 0.0f, 0.0f))).first;
+        float4 &c0 = it->second.first, &c1 = it->second.second;
+        c0 = make_float4(std::max(c0.x, q.a1_main), std::max(c0.y, q.a2), std::max(c0.z, q.a5), std::max(c0.w, q.a6));
+        c1 = make_float4(std::max(c1.x, q.qs), std::max(c1.y, std::fabs(q.s1)), 0.0f, 0.0f);
+    }
+    for (int t : rows)
+    {
+        const auto &c = by_m.at(g.htp[static_cast<size_t>(t)].m);
+        gmax[2 * static_cast<size_t>(t)] = c.first;
+        gmax[2 * static_cast<size_t>(t) + 1] = c.second;
+    }
+    L.fft_gmax.reserve(sizeof(float4) * gmax.size());
+    TM_CUDA(cudaMemcpyAsync(L.fft_gmax.p, gmax.data(), sizeof(float4) * gmax.size(), cudaMemcpyHostToDevice, s));
     if (long_pieces)
     {
         // the forward transform's scratch is the context's: one launch at a time
@@ -620,6 +642,7 @@ static void fft_contract_rows(tm_ctx *ctx, Lane &L, const GroupPlan &g, const tm
     f.dbg_d = a.dbg_d;
     f.dbg_e = a.dbg_e;
     f.stats = L.fft_stats.as<float4>();
+    f.gmax = L.fft_gmax.as<float4>();
     TM_CUDA(long_pieces ? tmb::launch_fft3_corr(f, ctx->sms, s) : tmb::launch_fft2_corr(f, ctx->sms, s));
     count_launch(L, 2);
 }
