@@ -234,7 +234,7 @@ int tm_autotune(tm_ctx *ctx, double *ms, int capacity)
             {
                 for (int t = 0; t < 128; t++)
                 {
-                    const int m = ks[ki] - (mixed && (t & 1) ? 16 : 0);
+                    const int m = ks[ki] - (mixed ? t : 0); // several lengths: 128 distinct ones
                     temps[t].resize(static_cast<size_t>(m));
                     for (int i = 0; i < m; i++)
                         temps[t][i] = std::sin(0.003f * static_cast<float>(i) * (1.0f + 0.01f * t) +
@@ -259,9 +259,10 @@ int tm_autotune(tm_ctx *ctx, double *ms, int capacity)
                     table[mixed][v][ki] = per * (33554432.0 / windows);
                 }
             }
-        // the FFT branch, 8 templates each (its time does not depend on the length within
-        // either kind): templates of up to 8192 samples (the fused kernels; 4096 here) and
-        // longer ones (16384)
+        // the FFT branch, 8 templates of distinct lengths each (its time does not depend on
+        // the length within either kind; distinct lengths share no window statistics, the
+        // case of batches of many lengths): templates of up to 8192 samples (4089-4096 here)
+        // and longer ones (16377-16384)
         tc->tiles = TM_TILES_FFT;
         double fft_per[2];
         for (int kind = 0; kind < 2; kind++)
@@ -270,7 +271,7 @@ int tm_autotune(tm_ctx *ctx, double *ms, int capacity)
             std::vector<tm_request> fr(8);
             for (int t = 0; t < 8; t++)
             {
-                const int m = kind == 0 ? 4096 : 16384;
+                const int m = (kind == 0 ? 4096 : 16384) - t;
                 ft[t].resize(static_cast<size_t>(m));
                 for (int i = 0; i < m; i++)
                     ft[t][i] = std::sin(0.003f * static_cast<float>(i) * (1.0f + 0.01f * t) +

@@ -49,6 +49,78 @@ __device__ __forceinline__ float stats_error(const WindowStats &w, int m, float 
     return 1.25f * ((4.0f * (float)m + 2.0f * qs) * w.rel_sd + 2.0f * fabsf(s1q) * w.e_mu * w.iv);
 }
 
+// A window's first and second sums relative to its start block's centre, with bounds on
+// their errors (the two cases of window_prefix_stats).
+struct PrefixSums
+{
+    double s1, s2;
+    float e_s1, e_s2;
+};
+
+// The window lies in one prefix block: na and nb are the block offsets of its start and
+// end, qa = (float) Qa.y.
+__device__ __forceinline__ PrefixSums prefix_sums_one_block(double2 Qa, double2 Qb, float na, float nb, float qa)
+{
+    const float fg = (float)kPrefixGamma * 1.01f;
+    const float qb = (float)Qb.y;
+    PrefixSums r;
+    r.s1 = Qb.x - Qa.x;
+    r.s2 = Qb.y - Qa.y;
+    r.e_s2 = fg * (qa + qb);
+    // sqrt(na qa) + sqrt(nb qb) <= sqrt(2 (na qa + nb qb)) (Cauchy-Schwarz)
+    r.e_s1 = 1.001f * fg * sqrt_up(2.0f * (na * qa + nb * qb));
+    return r;
+}
+
+// The window starts in block b1 and ends in block be = b1 + 1 (m <= kPrefixBlock).
+__device__ __forceinline__ PrefixSums prefix_sums_two_blocks(const PrefixView &pv, double2 Qa, double2 Qb, uint64_t j,
+                                                             int m)
+{
+    const uint64_t e = j + (uint64_t)m;
+    const uint64_t b1 = j >> kPrefixBlockLog, be = e >> kPrefixBlockLog;
+    const float fg = (float)kPrefixGamma * 1.01f, fe = (float)kEps64 * 1.01f;
+    const float na = (float)(j - (b1 << kPrefixBlockLog)), qa = (float)Qa.y, qb = (float)Qb.y;
+    const double2 t = pv.T[b1];
+    const double d = pv.C[be] - pv.C[b1];
+    const double n2 = (double)(e - (be << kPrefixBlockLog));
+    PrefixSums r;
+    r.s1 = (t.x - Qa.x) + (Qb.x + n2 * d);
+    r.s2 = (t.y - Qa.y) + (Qb.y + (2.0 * d * Qb.x + n2 * d * d));
+    const float tq = (float)t.y, fd = fabsf((float)d), fn2 = (float)n2, q1b = fabsf((float)Qb.x);
+    const float nt = (float)kPrefixBlock;
+    const float eq1b = 1.001f * fg * sqrt_up(fn2 * qb);
+    r.e_s2 = fg * (tq + qa + qb) + 2.0f * fd * eq1b + 8.0f * fe * (2.0f * fd * q1b + fn2 * fd * fd) +
+             4.0f * fe * fd * (q1b + fn2 * fd);
+    r.e_s1 = 1.001f * fg * sqrt_up(2.0f * (nt * tq + na * qa)) + eq1b + 4.0f * fe * fn2 * fd +
+             4.0f * fe * (fabsf((float)t.x) + fabsf((float)Qa.x) + q1b + fn2 * fd);
+    return r;
+}
+
+// The statistics from a window's sums (centre c of its start block): 0 when trustworthy,
+// 2 when cancellation may have destroyed them (w is then meaningless). Branch-free apart
+// from its result, so that callers can evaluate several windows side by side.
+__device__ __forceinline__ int prefix_stats_tail(PrefixSums ps, int m, double inv_m, double c, WindowStats &w)
+{
+    const float fe = (float)kEps64 * 1.01f;
+    const double mu_c = ps.s1 * inv_m;
+    const double var = fma(-mu_c, mu_c, ps.s2 * inv_m);
+    const float fvar = (float)var, fmu = (float)mu_c;
+    // 1 / m from the caller's FP64 inverse, rounded up (a factor for the bounds only)
+    const float fm = (float)m, fim = (float)inv_m * (1.0f + 1.1920929e-07f);
+    const float fs2 = fm * (fvar + fmu * fmu) * 1.0001f;
+    const float e_s2 = ps.e_s2 + 4.0f * fe * fs2;
+    const float e_s1 = ps.e_s1 + 4.0f * fe * fm * fabsf(fmu);
+    const float e_var = (e_s2 + 2.0f * fabsf(fmu) * e_s1 + 8.0f * fe * fs2) * fim * 1.0001f;
+    const float center_f = (float)c;
+    w.iv = rsqrtf(fvar);
+    w.mu = fmu + center_f;
+    w.rel_sd = 0.5f * e_var * w.iv * w.iv * 1.001f + 6.0e-7f;
+    w.e_mu = e_s1 * fim + 1.2e-7f * (fabsf(w.mu) + fabsf(center_f)) + 4.0f * fe * fabsf(w.mu) +
+             6.0e-8f * fabsf(center_f);
+    // var < 1e-22 (std < 1e-11): near the reference's 1e-12 cut, decided by the exact path
+    return (var > 1e-22 && var < 1e36 && e_var <= 1e-4f * fvar) ? 0 : 2;
+}
+
 // Statistics of window [j, j + m) (global sample index, m <= kPrefixBlock) from its
 // block-local prefix sums Qa = Q[j], Qb = Q[j + m]. Returns 0 when they are trustworthy, 2
 // when cancellation may have destroyed them (the window must then be re-scored exactly,
@@ -68,56 +140,13 @@ __device__ __forceinline__ int window_prefix_stats(const PrefixView &pv, double2
 {
     const uint64_t e = j + (uint64_t)m;
     const uint64_t b1 = j >> kPrefixBlockLog, be = e >> kPrefixBlockLog;
-    const float fg = (float)kPrefixGamma * 1.01f, fe = (float)kEps64 * 1.01f;
-    const float na = (float)(j - (b1 << kPrefixBlockLog)), qa = (float)Qa.y, qb = (float)Qb.y;
-    const double c = pv.C[b1];
-    double s1, s2;
-    float e_s1, e_s2;
+    PrefixSums ps;
     if (be == b1)
-    {
-        s1 = Qb.x - Qa.x;
-        s2 = Qb.y - Qa.y;
-        const float nb = (float)(e - (b1 << kPrefixBlockLog));
-        e_s2 = fg * (qa + qb);
-        // sqrt(na qa) + sqrt(nb qb) <= sqrt(2 (na qa + nb qb)) (Cauchy-Schwarz)
-        e_s1 = 1.001f * fg * sqrt_up(2.0f * (na * qa + nb * qb));
-    }
+        ps = prefix_sums_one_block(Qa, Qb, (float)(j - (b1 << kPrefixBlockLog)),
+                                   (float)(e - (b1 << kPrefixBlockLog)), (float)Qa.y);
     else
-    {
-        const double2 t = pv.T[b1];
-        const double d = pv.C[be] - c;
-        const double n2 = (double)(e - (be << kPrefixBlockLog));
-        s1 = (t.x - Qa.x) + (Qb.x + n2 * d);
-        s2 = (t.y - Qa.y) + (Qb.y + (2.0 * d * Qb.x + n2 * d * d));
-        const float tq = (float)t.y, fd = fabsf((float)d), fn2 = (float)n2, q1b = fabsf((float)Qb.x);
-        const float nt = (float)kPrefixBlock;
-        const float eq1b = 1.001f * fg * sqrt_up(fn2 * qb);
-        e_s2 = fg * (tq + qa + qb) + 2.0f * fd * eq1b + 8.0f * fe * (2.0f * fd * q1b + fn2 * fd * fd) +
-               4.0f * fe * fd * (q1b + fn2 * fd);
-        e_s1 = 1.001f * fg * sqrt_up(2.0f * (nt * tq + na * qa)) + eq1b + 4.0f * fe * fn2 * fd +
-               4.0f * fe * (fabsf((float)t.x) + fabsf((float)Qa.x) + q1b + fn2 * fd);
-    }
-    const double mu_c = s1 * inv_m;
-    const double var = fma(-mu_c, mu_c, s2 * inv_m);
-    // var < 1e-22 (std < 1e-11): near the reference's 1e-12 cut, decided by the exact path
-    if (!(var > 1e-22) || !(var < 1e36))
-        return 2;
-    const float fvar = (float)var, fmu = (float)mu_c;
-    // 1 / m from the caller's FP64 inverse, rounded up (a factor for the bounds only)
-    const float fm = (float)m, fim = (float)inv_m * (1.0f + 1.1920929e-07f);
-    const float fs2 = fm * (fvar + fmu * fmu) * 1.0001f;
-    e_s2 += 4.0f * fe * fs2;
-    e_s1 += 4.0f * fe * fm * fabsf(fmu);
-    const float e_var = (e_s2 + 2.0f * fabsf(fmu) * e_s1 + 8.0f * fe * fs2) * fim * 1.0001f;
-    if (!(e_var <= 1e-4f * fvar))
-        return 2;
-    const float center_f = (float)c;
-    w.iv = rsqrtf(fvar);
-    w.mu = fmu + center_f;
-    w.rel_sd = 0.5f * e_var * w.iv * w.iv * 1.001f + 6.0e-7f;
-    w.e_mu = e_s1 * fim + 1.2e-7f * (fabsf(w.mu) + fabsf(center_f)) + 4.0f * fe * fabsf(w.mu) +
-             6.0e-8f * fabsf(center_f);
-    return 0;
+        ps = prefix_sums_two_blocks(pv, Qa, Qb, j, m);
+    return prefix_stats_tail(ps, m, inv_m, pv.C[b1], w);
 }
 
 // fast_distance (tm_epilogue.cuh) for statistics from prefix sums: the a4 term of the

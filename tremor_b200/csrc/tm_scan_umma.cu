@@ -607,28 +607,78 @@ __global__ void __launch_bounds__(THREADS, 1)
                 const int G = 1 << glog;
                 for (int c0 = 128 * half; c0 < 128 * half + 128; c0 += G)
                 {
-                    for (int q = lane; q < (nd << glog); q += 32)
+                    // item q = lane + 32 it is window i = lane mod G of the group and distinct
+                    // length d = (lane >> glog) + it (32 >> glog): a lane's items share one
+                    // window, so its start (prefix sums, first sample, constant run, block) is
+                    // loaded once; its items go four at a time, the window ends loaded first,
+                    // then the single-block statistics of all four as independent straight-line
+                    // chains, then (rarely) the windows that end in the next prefix block
+                    const int i = lane & (G - 1), d0 = lane >> glog, dstep = 32 >> glog;
+                    const uint32_t j = j0 + (uint32_t)(c0 + i);
+                    const uint64_t g = a.w0 + j;
+                    const uint64_t b1 = g >> kPrefixBlockLog;
+                    double2 qa = make_double2(0.0, 0.0);
+                    float rv = kMissing;
+                    uint16_t rn = 0xffffu;
+                    double cen = 0.0;
+                    if (g < a.n)
                     {
-                        const int i = q & (G - 1), d = q >> glog;
-                        const uint32_t j = j0 + (uint32_t)(c0 + i);
-                        float4 r = make_float4(0.0f, 0.0f, nan_f(), 0.0f); // not searched
-                        const int len = sm.wl_len[ew][d];
-                        if (j < sm.wl_wc[ew][d]) // then w0 + j + len <= n: both prefix entries exist
+                        qa = a.P[g];
+                        rv = a.raw[g];
+                        rn = a.run[g];
+                        cen = a.PC[b1];
+                    }
+                    const float na = (float)(g - (b1 << kPrefixBlockLog)), qaf = (float)qa.y;
+#pragma unroll
+                    for (int it0 = 0; it0 < 8; it0 += 4)
+                    {
+                        if (d0 + dstep * it0 >= nd)
+                            break; // no length left for this lane (nothing in the loop is warp-collective)
+                        double2 qb[4];
+                        bool srch[4];
+#pragma unroll
+                        for (int k = 0; k < 4; k++)
                         {
-                            const uint64_t g = a.w0 + j;
-                            const double2 qa = a.P[g], qb = a.P[g + (uint64_t)len];
-                            const float rv = a.raw[g];
-                            const uint16_t rn = a.run[g];
-                            if (rv != kMissing && rn < len)
-                            {
-                                WindowStats ws;
-                                if (window_prefix_stats(pv, qa, qb, g, len, sm.wl_inv[ew][d], ws) == 0)
-                                    r = mixed_terms(ws, shift, sm.wl_c[ew][d], sm.wl_b[ew][d]);
-                                else
-                                    r.z = inf_f(); // statistics not trustworthy: d - e = -inf, exact re-scoring decides
-                            }
+                            const int d = d0 + dstep * (it0 + k); // < 32
+                            const int len = sm.wl_len[ew][d];
+                            srch[k] = d < nd && j < sm.wl_wc[ew][d] && rv != kMissing && rn < len;
+                            qb[k] = make_double2(0.0, 0.0);
+                            if (d < nd && j < sm.wl_wc[ew][d]) // then w0 + j + len <= n: both prefix entries exist
+                                qb[k] = a.P[g + (uint64_t)len];
                         }
-                        sm.wst[ew][(d << glog) + (i ^ (d & 7))] = r;
+                        float4 r[4];
+                        bool two[4];
+#pragma unroll
+                        for (int k = 0; k < 4; k++)
+                        {
+                            const int d = d0 + dstep * (it0 + k);
+                            const int len = sm.wl_len[ew][d];
+                            two[k] = ((g + (uint64_t)len) >> kPrefixBlockLog) != b1;
+                            WindowStats ws;
+                            const int st = prefix_stats_tail(prefix_sums_one_block(qa, qb[k], na, na + (float)len, qaf),
+                                                             len, sm.wl_inv[ew][d], cen, ws);
+                            r[k] = st == 0 ? mixed_terms(ws, shift, sm.wl_c[ew][d], sm.wl_b[ew][d])
+                                           : make_float4(0.0f, 0.0f, inf_f(), 0.0f);
+                        }
+#pragma unroll
+                        for (int k = 0; k < 4; k++)
+                        {
+                            const int d = d0 + dstep * (it0 + k);
+                            if (srch[k] && two[k])
+                            {
+                                const int len = sm.wl_len[ew][d];
+                                WindowStats ws;
+                                r[k] = window_prefix_stats(pv, qa, qb[k], g, len, sm.wl_inv[ew][d], ws) == 0
+                                           ? mixed_terms(ws, shift, sm.wl_c[ew][d], sm.wl_b[ew][d])
+                                           : make_float4(0.0f, 0.0f, inf_f(), 0.0f);
+                            }
+                            // not searched: NaN; statistics not trustworthy: E0 = +inf (d - e =
+                            // -inf, exact re-scoring decides)
+                            if (!srch[k])
+                                r[k] = make_float4(0.0f, 0.0f, nan_f(), 0.0f);
+                            if (d < nd)
+                                sm.wst[ew][(d << glog) + (i ^ (d & 7))] = r[k];
+                        }
                     }
                     __syncwarp();
                     uint32_t mask = 0;
@@ -1063,6 +1113,10 @@ __global__ void __launch_bounds__(THREADS, 1)
                 miss = winv == 0.0f;
             }
             const float a2 = (float)pj.y;
+            // mixed: the window's prefix block, its offset in it and the block's centre
+            const uint64_t jb = (a.w0 + j) >> kPrefixBlockLog;
+            const float jna = (float)(a.w0 + j - (jb << kPrefixBlockLog));
+            const double jcen = MIXED && in ? a.PC[jb] : 0.0;
             const float shift = wm_shift<MIXED>(a, j0);
             const size_t bucket = j0 / kBucket;
             if (!mbar_wait_warp(&sm.acc_full[buf], (tc >> 1) & 1, sm.abort, wa.err, 26))
@@ -1082,43 +1136,49 @@ __global__ void __launch_bounds__(THREADS, 1)
                 float v[8];
                 tmem_ld8(taddr + g, v);
 #pragma unroll
-                for (int i = 0; i < 8; i++)
+                for (int h4 = 0; h4 < 8; h4 += 4)
                 {
-                    const ColParam &c = sm.cp[buf][g + i];
-                    const uint32_t t = (uint32_t)(ct * NT + g + i);
-                    const bool ok = MIXED ? (!miss && j < c.wcount && runj < (uint32_t)c.m) : (!miss && c.wcount > 0);
-                    bool hit = false;
-                    float up = inf_f(), lo = inf_f();
-                    if (!MIXED && ok)
+                    // mixed: the statistics of the window for four columns' lengths, as four
+                    // independent single-block evaluations, then (rarely) the lengths whose window
+                    // ends in the next prefix block
+                    WindowStats wsv[4];
+                    int wst[4];
+                    if (MIXED)
                     {
-                        const float ms = wmean - shift;
-                        const float cross = (v[i] - ms * c.s1) * winv;
-                        const float dd = c.c_lin - 2.0f * cross;
-                        const float r = ms * winv, r0 = wmean * winv;
-                        const float e = c.a1 * sqrtf(1.0f + r * r) + c.a2 + c.a3 * fmaxf(dd, 0.0f) +
-                                        c.a4 * (1.0f + 2.0f * r0 * r0) + c.a5 * r0 * r0 +
-                                        c.a6 * (fabsf(wmean) + fabsf(shift)) * winv;
-                        if (a.dbg_d != nullptr)
+#pragma unroll
+                        for (int k = 0; k < 4; k++)
                         {
-                            a.dbg_d[(size_t)t * a.W + j] = dd;
-                            a.dbg_e[(size_t)t * a.W + j] = e;
+                            const ColParam &c = sm.cp[buf][g + h4 + k];
+                            wst[k] = prefix_stats_tail(prefix_sums_one_block(pj, pe[h4 + k], jna, jna + (float)c.m, a2),
+                                                       c.m, c.inv_m, jcen, wsv[k]);
                         }
-                        up = dd + e;
-                        lo = dd - e;
-                        hit = lo <= c.thr;
-                    }
-                    else if (ok)
-                    {
-                        WindowStats ws;
-                        if (window_prefix_stats(pv, pj, pe[i], a.w0 + j, c.m, c.inv_m, ws) == 0)
+#pragma unroll
+                        for (int k = 0; k < 4; k++)
                         {
-                            const float ms = ws.mu - shift;
-                            const float cross = (v[i] - ms * c.s1) * ws.iv;
+                            const ColParam &c = sm.cp[buf][g + h4 + k];
+                            const bool ok = !miss && j < c.wcount && runj < (uint32_t)c.m;
+                            if (ok && ((a.w0 + j + (uint64_t)c.m) >> kPrefixBlockLog) != jb)
+                                wst[k] = window_prefix_stats(pv, pj, pe[h4 + k], a.w0 + j, c.m, c.inv_m, wsv[k]);
+                        }
+                    }
+#pragma unroll
+                    for (int k = 0; k < 4; k++)
+                    {
+                        const int i = h4 + k;
+                        const ColParam &c = sm.cp[buf][g + i];
+                        const uint32_t t = (uint32_t)(ct * NT + g + i);
+                        const bool ok = MIXED ? (!miss && j < c.wcount && runj < (uint32_t)c.m) : (!miss && c.wcount > 0);
+                        bool hit = false;
+                        float up = inf_f(), lo = inf_f();
+                        if (!MIXED && ok)
+                        {
+                            const float ms = wmean - shift;
+                            const float cross = (v[i] - ms * c.s1) * winv;
                             const float dd = c.c_lin - 2.0f * cross;
-                            const float r = ms * ws.iv, r0 = ws.mu * ws.iv;
+                            const float r = ms * winv, r0 = wmean * winv;
                             const float e = c.a1 * sqrtf(1.0f + r * r) + c.a2 + c.a3 * fmaxf(dd, 0.0f) +
-                                            c.a5 * r0 * r0 + c.a6 * (fabsf(ws.mu) + fabsf(shift)) * ws.iv +
-                                            stats_error(ws, c.m, c.qs, c.s1);
+                                            c.a4 * (1.0f + 2.0f * r0 * r0) + c.a5 * r0 * r0 +
+                                            c.a6 * (fabsf(wmean) + fabsf(shift)) * winv;
                             if (a.dbg_d != nullptr)
                             {
                                 a.dbg_d[(size_t)t * a.W + j] = dd;
@@ -1128,24 +1188,46 @@ __global__ void __launch_bounds__(THREADS, 1)
                             lo = dd - e;
                             hit = lo <= c.thr;
                         }
+                        else if (ok)
+                        {
+                            const WindowStats &ws = wsv[k];
+                            if (wst[k] == 0)
+                            {
+                                const float ms = ws.mu - shift;
+                                const float cross = (v[i] - ms * c.s1) * ws.iv;
+                                const float dd = c.c_lin - 2.0f * cross;
+                                const float r = ms * ws.iv, r0 = ws.mu * ws.iv;
+                                const float e = c.a1 * sqrtf(1.0f + r * r) + c.a2 + c.a3 * fmaxf(dd, 0.0f) +
+                                                c.a5 * r0 * r0 + c.a6 * (fabsf(ws.mu) + fabsf(shift)) * ws.iv +
+                                                stats_error(ws, c.m, c.qs, c.s1);
+                                if (a.dbg_d != nullptr)
+                                {
+                                    a.dbg_d[(size_t)t * a.W + j] = dd;
+                                    a.dbg_e[(size_t)t * a.W + j] = e;
+                                }
+                                up = dd + e;
+                                lo = dd - e;
+                                hit = lo <= c.thr;
+                            }
+                            else
+                            {
+                                lo = -inf_f(); // statistics not trustworthy: exact re-scoring decides
+                                hit = true;
+                            }
+                        }
+                        if (c.mode == 1) // kNN: bucket minima over the warp's 32 windows
+                        {
+                            const uint32_t ku = __reduce_min_sync(0xffffffffu, float_key(up));
+                            const uint32_t kl = __reduce_min_sync(0xffffffffu, float_key(lo));
+                            if (lane == 0 && (ku != float_key(inf_f()) || kl != float_key(inf_f())))
+                            {
+                                atomicMin(&a.bmin_u[(size_t)t * a.nb + bucket], ku);
+                                atomicMin(&a.bmin_l[(size_t)t * a.nb + bucket], kl);
+                            }
+                        }
                         else
-                        {
-                            lo = -inf_f(); // statistics not trustworthy: exact re-scoring decides
-                            hit = true;
-                        }
+                            stage_emit_lane<64>(hit, lane, t, j, sm.stage[ew], staged, a.cand, a.cand_count, a.cand_cap);
                     }
-                    if (c.mode == 1) // kNN: bucket minima over the warp's 32 windows
-                    {
-                        const uint32_t ku = __reduce_min_sync(0xffffffffu, float_key(up));
-                        const uint32_t kl = __reduce_min_sync(0xffffffffu, float_key(lo));
-                        if (lane == 0 && (ku != float_key(inf_f()) || kl != float_key(inf_f())))
-                        {
-                            atomicMin(&a.bmin_u[(size_t)t * a.nb + bucket], ku);
-                            atomicMin(&a.bmin_l[(size_t)t * a.nb + bucket], kl);
-                        }
-                    }
-                    else
-                        stage_emit_lane<64>(hit, lane, t, j, sm.stage[ew], staged, a.cand, a.cand_count, a.cand_cap);
                 }
             }
             tc_fence_before();
