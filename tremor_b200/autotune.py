@@ -4,10 +4,11 @@
     python -m tremor_b200.autotune [--out model.json]
 
 The model is the kernel time in milliseconds of 128 templates against 2^25 windows, per
-group kind (one length, several lengths), tile shape (128-template row tiles; window-major
-column tiles of 128, 64 and 32 templates) and template length K; TILES_AUTO picks the
-shape (or the FFT branch, whose per-template time is measured too) of least modelled
-time from it."""
+group kind (one length; several lengths, measured with 128 distinct lengths K - 127 .. K,
+as batches of lengths drawn from a continuous range have), tile shape (128-template row
+tiles; window-major column tiles of 128, 64 and 32 templates) and template length K;
+TILES_AUTO picks the shape (or the FFT branch, whose per-template time is measured too,
+on templates of distinct lengths) of least modelled time from it."""
 from __future__ import annotations
 
 import argparse

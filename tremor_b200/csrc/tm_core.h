@@ -324,16 +324,17 @@ struct tm_ctx
     int kernel = TM_KERNEL_AUTO;
     int tiles = TM_TILES_AUTO;
     // tiling cost model: kernel milliseconds for 128 templates x 2^25 windows, per group kind
-    // (one length / several), shape (row tiles; column tiles of 128, 64, 32) and K (256,
-    // 1024, 4096, 16384). Defaults: a B200 measurement; tm_autotune re-measures.
-    double tile_ms[2][4][4] = {{{7.5, 17.2, 59.3, 259.0},
-                                {29.7, 31.5, 84.7, 331.8},
-                                {31.6, 42.9, 157.5, 581.6},
-                                {36.3, 83.4, 307.4, 1133.7}},
-                               {{11.1, 17.0, 59.3, 259.3},
-                                {82.1, 84.8, 100.2, 341.1},
-                                {84.7, 88.6, 160.7, 584.4},
-                                {90.0, 96.8, 306.7, 1126.6}}};
+    // (one length / several: 128 distinct lengths), shape (row tiles; column tiles of 128, 64,
+    // 32) and K (256, 1024, 4096, 16384). Defaults: a B200 measurement; tm_autotune
+    // re-measures.
+    double tile_ms[2][4][4] = {{{7.2, 16.6, 61.3, 262.5},
+                                {29.7, 31.5, 86.5, 337.2},
+                                {31.6, 43.2, 157.8, 583.8},
+                                {36.2, 83.2, 307.9, 1132.7}},
+                               {{61.5, 69.5, 104.4, 294.8},
+                                {67.1, 74.0, 94.7, 347.9},
+                                {68.8, 74.0, 159.5, 584.0},
+                                {74.5, 88.8, 308.4, 1140.0}}};
     std::map<int, std::unique_ptr<tmh::LengthStats>> lengths;
     uint64_t use_clock = 0;
     tmh::DevBuf suf; // window-statistics scratch (per-length statistics)
@@ -350,9 +351,10 @@ struct tm_ctx
     std::mutex fft_mu;
     int sms = 148;
     // model: the FFT branch's ms per template per 2^25 samples, for templates of up to 8192
-    // samples (the fused kernels) and longer ones (B200 defaults; tm_autotune measures both)
-    double fft_ms = 0.84;
-    double fft_long_ms = 1.22;
+    // samples (the fused kernels) and longer ones, templates of distinct lengths (B200 defaults;
+    // tm_autotune measures both)
+    double fft_ms = 0.71;
+    double fft_long_ms = 1.07;
     // the context's own memory pool for per-batch buffers (DevBuf::reserve_on); it keeps
     // up to 4 GiB of freed memory for the next batch
     cudaMemPool_t pool = nullptr;

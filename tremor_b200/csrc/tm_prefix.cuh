@@ -121,6 +121,48 @@ __device__ __forceinline__ int prefix_stats_tail(PrefixSums ps, int m, double in
     return (var > 1e-22 && var < 1e36 && e_var <= 1e-4f * fvar) ? 0 : 2;
 }
 
+// Fast path for windows that lie in one prefix block and are well conditioned (most of
+// them): bounds that hold for every single-block window of block b, from its block total of
+// squares T2 (the block-local prefix of squares only grows, so qa, qb <= T2 up to rounding,
+// and na, nb <= 2^16):
+//   e_s2 = fg (qa + qb)                        <= a = 2 fg T2
+//   e_s1 = 1.001 fg sqrt(2 (na qa + nb qb))    <= b = 1.001 fg 512 sqrt(T2)
+// (each with a 1e-5 margin). When, in addition, (a + 2 |mu_c| b) / m <= 0.9e-7 var and
+// mu_c^2 <= 1e6 var, prefix_stats_tail's e_var is at most 1.0004e-7 var, so the statistics
+// are trusted and its rel_sd is at most 0.5 x 1.0004e-7 (1 + 2^-21) 1.001 + 6e-7 < 6.6e-7
+// (kFastRelSd), and its e_mu is at most b / m + 1.3e-7 |mu| + 1.9e-7 |c|. mu and 1 / std are
+// computed exactly as there.
+struct BlockBounds
+{
+    float a, b;
+};
+
+constexpr float kFastRelSd = 6.6e-7f;
+
+__device__ __forceinline__ BlockBounds block_bounds(double t2)
+{
+    const float fg = (float)kPrefixGamma * 1.01f;
+    const float T = (float)t2 * 1.00001f;
+    return BlockBounds{2.0f * fg * T * 1.00001f, 1.001f * fg * 512.0f * sqrt_up(T) * 1.00001f};
+}
+
+// Returns true when the fast path applies (the window must lie in one block); then mu, iv
+// are the window's mean and 1 / std, e_mu a bound on the error of mu, and kFastRelSd one on
+// the relative error of the std. fim: (float) inv_m rounded up, cf: (float) c.
+__device__ __forceinline__ bool prefix_stats_fast(double2 Qa, double2 Qb, double inv_m, float fim, float cf,
+                                                  BlockBounds bb, float &mu, float &iv, float &e_mu)
+{
+    const double s1 = Qb.x - Qa.x, s2 = Qb.y - Qa.y;
+    const double mu_c = s1 * inv_m;
+    const double var = fma(-mu_c, mu_c, s2 * inv_m);
+    const float fvar = (float)var, fmu = (float)mu_c;
+    iv = rsqrtf(fvar);
+    mu = fmu + cf;
+    e_mu = bb.b * fim + 1.3e-7f * fabsf(mu) + 1.9e-7f * fabsf(cf);
+    return fvar > 2e-22f && fvar < 1e36f && fmu * fmu <= 1e6f * fvar &&
+           (bb.a + 2.0f * fabsf(fmu) * bb.b) * fim <= 0.9e-7f * fvar;
+}
+
 // Statistics of window [j, j + m) (global sample index, m <= kPrefixBlock) from its
 // block-local prefix sums Qa = Q[j], Qb = Q[j + m]. Returns 0 when they are trustworthy, 2
 // when cancellation may have destroyed them (the window must then be re-scored exactly,

@@ -73,6 +73,7 @@ template <bool MIXED> struct SmemT
     int wl_len[WL][32];        // the warp's distinct lengths
     uint32_t wl_wc[WL][32];    //   their window counts in the searched range
     double wl_inv[WL][32];     //   their inverses
+    float wl_fim[WL][32];      //   the same in float, rounded up
     float4 wl_c[WL][32];       //   maxima over their rows of a1, a5, a6 and 1.25 (4 m + 2 qs)
     float wl_b[WL][32];        //   and of 2.5 |s1|
     float4 win4[W2][TN];       // single-length tiles: window terms (win_terms), then (1/sigma, mu - shift, eb, Q)
@@ -295,6 +296,17 @@ __device__ __forceinline__ float4 mixed_terms(const WindowStats &ws, float shift
     const float e0 = c.x * sqrtf(1.0f + r * r) + c.y * (r0 * r0) + c.z * (fabsf(ws.mu) + fabsf(shift)) * ws.iv +
                      c.w * ws.rel_sd + cb * (ws.e_mu * ws.iv);
     return make_float4(ws.iv, ms, e0, 0.0f);
+}
+
+// mixed_terms for statistics from the fast path (prefix_stats_fast): the relative error of
+// the std is at most kFastRelSd, and sqrt(1 + r^2) <= 1 + |r|.
+__device__ __forceinline__ float4 mixed_terms_fast(float mu, float iv, float e_mu, float shift, float4 c, float cb)
+{
+    const float ms = mu - shift;
+    const float r = ms * iv, r0 = mu * iv;
+    const float e0 = c.x * (1.0f + fabsf(r)) + c.y * (r0 * r0) + c.z * (fabsf(mu) + fabsf(shift)) * iv +
+                     c.w * kFastRelSd + cb * (e_mu * iv);
+    return make_float4(iv, ms, e0, 0.0f);
 }
 
 // Maximum of a non-negative float over the lanes where `mine` holds (0 when none).
@@ -580,6 +592,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                         sm.wl_len[ew][nd] = len;
                         sm.wl_wc[ew][nd] = p.wcount; // a function of the length alone
                         sm.wl_inv[ew][nd] = p.inv_m;
+                        sm.wl_fim[ew][nd] = (float)p.inv_m * (1.0f + 1.1920929e-07f);
                         sm.wl_c[ew][nd] = make_float4(c1, c5, c6, cA);
                         sm.wl_b[ew][nd] = cB;
                     }
@@ -611,8 +624,9 @@ __global__ void __launch_bounds__(THREADS, 1)
                     // length d = (lane >> glog) + it (32 >> glog): a lane's items share one
                     // window, so its start (prefix sums, first sample, constant run, block) is
                     // loaded once; its items go four at a time, the window ends loaded first,
-                    // then the single-block statistics of all four as independent straight-line
-                    // chains, then (rarely) the windows that end in the next prefix block
+                    // then the fast-path statistics of all four (prefix_stats_fast) as
+                    // independent straight-line chains, then (rarely) the full bound for those
+                    // that end in the next prefix block or are ill-conditioned
                     const int i = lane & (G - 1), d0 = lane >> glog, dstep = 32 >> glog;
                     const uint32_t j = j0 + (uint32_t)(c0 + i);
                     const uint64_t g = a.w0 + j;
@@ -620,15 +634,17 @@ __global__ void __launch_bounds__(THREADS, 1)
                     double2 qa = make_double2(0.0, 0.0);
                     float rv = kMissing;
                     uint16_t rn = 0xffffu;
-                    double cen = 0.0;
+                    double cen = 0.0, t2 = 0.0;
                     if (g < a.n)
                     {
                         qa = a.P[g];
                         rv = a.raw[g];
                         rn = a.run[g];
                         cen = a.PC[b1];
+                        t2 = a.PT[b1].y;
                     }
-                    const float na = (float)(g - (b1 << kPrefixBlockLog)), qaf = (float)qa.y;
+                    const float cf = (float)cen;
+                    const BlockBounds bb = block_bounds(t2);
 #pragma unroll
                     for (int it0 = 0; it0 < 8; it0 += 4)
                     {
@@ -647,24 +663,23 @@ __global__ void __launch_bounds__(THREADS, 1)
                                 qb[k] = a.P[g + (uint64_t)len];
                         }
                         float4 r[4];
-                        bool two[4];
+                        bool fast[4];
 #pragma unroll
                         for (int k = 0; k < 4; k++)
                         {
                             const int d = d0 + dstep * (it0 + k);
                             const int len = sm.wl_len[ew][d];
-                            two[k] = ((g + (uint64_t)len) >> kPrefixBlockLog) != b1;
-                            WindowStats ws;
-                            const int st = prefix_stats_tail(prefix_sums_one_block(qa, qb[k], na, na + (float)len, qaf),
-                                                             len, sm.wl_inv[ew][d], cen, ws);
-                            r[k] = st == 0 ? mixed_terms(ws, shift, sm.wl_c[ew][d], sm.wl_b[ew][d])
-                                           : make_float4(0.0f, 0.0f, inf_f(), 0.0f);
+                            float mu, iv, emu;
+                            fast[k] = prefix_stats_fast(qa, qb[k], sm.wl_inv[ew][d], sm.wl_fim[ew][d], cf, bb, mu, iv,
+                                                        emu) &&
+                                      ((g + (uint64_t)len) >> kPrefixBlockLog) == b1;
+                            r[k] = mixed_terms_fast(mu, iv, emu, shift, sm.wl_c[ew][d], sm.wl_b[ew][d]);
                         }
 #pragma unroll
                         for (int k = 0; k < 4; k++)
                         {
                             const int d = d0 + dstep * (it0 + k);
-                            if (srch[k] && two[k])
+                            if (srch[k] && !fast[k]) // two prefix blocks, or ill-conditioned: the full bound
                             {
                                 const int len = sm.wl_len[ew][d];
                                 WindowStats ws;
@@ -1112,11 +1127,10 @@ __global__ void __launch_bounds__(THREADS, 1)
                 winv = a.inv[j];
                 miss = winv == 0.0f;
             }
-            const float a2 = (float)pj.y;
-            // mixed: the window's prefix block, its offset in it and the block's centre
+            // mixed: the window's prefix block, the block's centre and its fast-path error bounds
             const uint64_t jb = (a.w0 + j) >> kPrefixBlockLog;
-            const float jna = (float)(a.w0 + j - (jb << kPrefixBlockLog));
-            const double jcen = MIXED && in ? a.PC[jb] : 0.0;
+            const float jcf = MIXED && in ? (float)a.PC[jb] : 0.0f;
+            const BlockBounds jbb = block_bounds(MIXED && in ? a.PT[jb].y : 0.0);
             const float shift = wm_shift<MIXED>(a, j0);
             const size_t bucket = j0 / kBucket;
             if (!mbar_wait_warp(&sm.acc_full[buf], (tc >> 1) & 1, sm.abort, wa.err, 26))
@@ -1139,8 +1153,9 @@ __global__ void __launch_bounds__(THREADS, 1)
                 for (int h4 = 0; h4 < 8; h4 += 4)
                 {
                     // mixed: the statistics of the window for four columns' lengths, as four
-                    // independent single-block evaluations, then (rarely) the lengths whose window
-                    // ends in the next prefix block
+                    // independent fast-path evaluations (prefix_stats_fast), then (rarely) the
+                    // full bound for those whose window ends in the next prefix block or is
+                    // ill-conditioned
                     WindowStats wsv[4];
                     int wst[4];
                     if (MIXED)
@@ -1149,15 +1164,19 @@ __global__ void __launch_bounds__(THREADS, 1)
                         for (int k = 0; k < 4; k++)
                         {
                             const ColParam &c = sm.cp[buf][g + h4 + k];
-                            wst[k] = prefix_stats_tail(prefix_sums_one_block(pj, pe[h4 + k], jna, jna + (float)c.m, a2),
-                                                       c.m, c.inv_m, jcen, wsv[k]);
+                            const bool fast =
+                                prefix_stats_fast(pj, pe[h4 + k], c.inv_m, (float)c.inv_m * (1.0f + 1.1920929e-07f), jcf,
+                                                  jbb, wsv[k].mu, wsv[k].iv, wsv[k].e_mu) &&
+                                ((a.w0 + j + (uint64_t)c.m) >> kPrefixBlockLog) == jb;
+                            wsv[k].rel_sd = kFastRelSd;
+                            wst[k] = fast ? 0 : 1;
                         }
 #pragma unroll
                         for (int k = 0; k < 4; k++)
                         {
                             const ColParam &c = sm.cp[buf][g + h4 + k];
                             const bool ok = !miss && j < c.wcount && runj < (uint32_t)c.m;
-                            if (ok && ((a.w0 + j + (uint64_t)c.m) >> kPrefixBlockLog) != jb)
+                            if (ok && wst[k] != 0) // two prefix blocks, or ill-conditioned: the full bound
                                 wst[k] = window_prefix_stats(pv, pj, pe[h4 + k], a.w0 + j, c.m, c.inv_m, wsv[k]);
                         }
                     }
