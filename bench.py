@@ -764,9 +764,15 @@ def run_ours(args, w):
         roof['frac'] = achieved / roof['peak']
         if kname == 'k_scan_umma':
             sustained = peaks_sustained()
-            if sustained:
-                roof['peak_sustained'] = sustained / 3.0
-                roof['frac_sustained'] = achieved / (sustained / 3.0)
+            if sustained and k_avg_ms * args.steps >= 1000.0:
+                # the kernel runs back to back for seconds under the power cap: the measured
+                # sustained GEMM loop is its denominator; the burst figure stays beside it
+                roof['peak_burst'], roof['frac_burst'] = roof['peak'], roof['frac']
+                roof['peak'] = sustained / 3.0
+                roof['frac'] = achieved / roof['peak']
+                roof['peak_note'] = ('measured sustained bf16 dense / 3 (a seconds-long GEMM loop under the '
+                                     'power cap; three BF16 products per FP32 multiply-add); the burst figure '
+                                     'is in peak_burst')
         tb_bytes = traffic_for(kname, args.workload)
         roof['traffic'] = tb_bytes
         roof['kernel'] = kname

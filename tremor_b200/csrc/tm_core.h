@@ -327,14 +327,14 @@ struct tm_ctx
     // (one length / several: 128 distinct lengths), shape (row tiles; column tiles of 128, 64,
     // 32) and K (256, 1024, 4096, 16384). Defaults: a B200 measurement; tm_autotune
     // re-measures.
-    double tile_ms[2][4][4] = {{{7.2, 16.6, 61.3, 262.5},
-                                {29.7, 31.5, 86.5, 337.2},
-                                {31.6, 43.2, 157.8, 583.8},
-                                {36.2, 83.2, 307.9, 1132.7}},
-                               {{61.5, 69.5, 104.4, 294.8},
-                                {67.1, 74.0, 94.7, 347.9},
-                                {68.8, 74.0, 159.5, 584.0},
-                                {74.5, 88.8, 308.4, 1140.0}}};
+    double tile_ms[2][4][4] = {{{7.2, 16.4, 58.7, 259.0},
+                                {29.7, 31.5, 84.2, 334.1},
+                                {31.5, 42.8, 157.6, 588.2},
+                                {36.0, 83.2, 307.2, 1142.8}},
+                               {{47.4, 53.6, 85.9, 274.6},
+                                {70.8, 73.6, 89.2, 342.9},
+                                {72.7, 75.1, 155.0, 583.7},
+                                {78.3, 87.6, 310.9, 1163.1}}};
     std::map<int, std::unique_ptr<tmh::LengthStats>> lengths;
     uint64_t use_clock = 0;
     tmh::DevBuf suf; // window-statistics scratch (per-length statistics)

@@ -224,11 +224,21 @@ __device__ __forceinline__ WinIn load_window(const Fft2Args &a, int m, bool in_r
 // They do not depend on the template: the epilogues fold them (fold_window) and keep them in
 // the block's slice of a global scratch (L2-resident) for the next template of the same
 // length in the same piece.
+// Single-block, well-conditioned windows take the fast path (prefix_stats_fast), the others
+// the full bound.
 __device__ __forceinline__ float4 window_stats4(const Fft2Args &a, int m, double inv_m, bool in_range, uint64_t g,
                                                 const WinIn &w)
 {
     if (!(in_range && w.raw != kMissing && w.run < (uint32_t)min(m, 65535)))
         return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const uint64_t b1 = g >> kPrefixBlockLog;
+    if (((g + (uint64_t)m) >> kPrefixBlockLog) == b1)
+    {
+        float mu, iv, emu;
+        if (prefix_stats_fast(w.qa, w.qb, inv_m, (float)inv_m * (1.0f + 1.1920929e-07f), (float)a.pv.C[b1],
+                              block_bounds(a.pv.T[b1].y), mu, iv, emu))
+            return make_float4(mu, iv, kFastRelSd, emu);
+    }
     WindowStats ws;
     if (window_prefix_stats(a.pv, w.qa, w.qb, g, m, inv_m, ws) != 0)
         return make_float4(0.0f, -1.0f, 0.0f, 0.0f);
