@@ -14,7 +14,8 @@
 //
 // Tile: 256 windows x 64 templates per CTA, 8 warps; a warp owns 8 templates and a
 // lane 8 consecutive windows (64 FP32 accumulators). K advances in stages of 64
-// samples, double-buffered with cp.async. The stage's waveform slice is stored with 4
+// samples, three buffers deep with cp.async (one barrier per stage), the tile's shift
+// subtracted as the samples are read into registers. The stage's waveform slice is stored with 4
 // floats of padding after every 32 (xpos), so that the float4 loads of a quarter warp
 // (lanes 8 floats apart) fall in distinct shared-memory banks; a float4 never straddles
 // a pad because the loads start at multiples of 4 floats.
@@ -42,10 +43,17 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N> __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
+// Three operand buffers (dynamic shared memory): stage st + 2 is loaded into the buffer
+// that stage st - 1 used, so one barrier per stage both publishes stage st and retires
+// stage st - 1.
+constexpr int F_BUFS = 3;
+constexpr size_t F_SMEM = sizeof(float) * (size_t)F_BUFS * (F_XS_PAD + F_TPL * F_K);
+
 __global__ void __launch_bounds__(F_THREADS, 2) k_scan_fp32(ScanArgs a)
 {
-    __shared__ __align__(16) float xs[2][F_XS_PAD];
-    __shared__ __align__(16) float qs[2][F_TPL][F_K];
+    extern __shared__ __align__(16) float fsm[];
+    float(*xs)[F_XS_PAD] = reinterpret_cast<float(*)[F_XS_PAD]>(fsm);
+    float(*qs)[F_TPL][F_K] = reinterpret_cast<float(*)[F_TPL][F_K]>(fsm + F_BUFS * F_XS_PAD);
     __shared__ TemplParam tps[F_TPL];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -78,20 +86,18 @@ __global__ void __launch_bounds__(F_THREADS, 2) k_scan_fp32(ScanArgs a)
 
     const int stages = a.m_pad / F_K;
     load_stage(0, 0);
+    if (stages > 1)
+        load_stage(1, F_K);
     for (int st = 0; st < stages; st++)
     {
-        const int cur = st & 1;
+        const int cur = st % F_BUFS;
         if (st + 1 < stages)
-        {
-            load_stage(cur ^ 1, (st + 1) * F_K);
-            cp_wait<1>();
-        }
+            cp_wait<1>(); // this thread's copies of stage st have landed (st + 1 may be in flight)
         else
             cp_wait<0>();
-        __syncthreads();
-        for (int i = tid; i < F_XS; i += F_THREADS)
-            xs[cur][xpos(i)] -= shift;
-        __syncthreads();
+        __syncthreads(); // stage st visible to all; every warp is done with stage st - 1
+        if (st + 2 < stages)
+            load_stage((st + 2) % F_BUFS, (st + 2) * F_K);
         const float *xw = &xs[cur][0];
         const float *qw = &qs[cur][8 * warp][0];
 #pragma unroll 4
@@ -101,7 +107,11 @@ __global__ void __launch_bounds__(F_THREADS, 2) k_scan_fp32(ScanArgs a)
             const float4 xa = *reinterpret_cast<const float4 *>(xw + xpos(x0));
             const float4 xb = *reinterpret_cast<const float4 *>(xw + xpos(x0 + 4));
             const float4 xc = *reinterpret_cast<const float4 *>(xw + xpos(x0 + 8));
-            const float xr[12] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y, xb.z, xb.w, xc.x, xc.y, xc.z, xc.w};
+            // the tile's shift, subtracted in registers (the same float subtraction for every
+            // use of a sample)
+            const float xr[12] = {xa.x - shift, xa.y - shift, xa.z - shift, xa.w - shift,
+                                  xb.x - shift, xb.y - shift, xb.z - shift, xb.w - shift,
+                                  xc.x - shift, xc.y - shift, xc.z - shift, xc.w - shift};
 #pragma unroll
             for (int t = 0; t < 8; t++)
             {
@@ -116,7 +126,6 @@ __global__ void __launch_bounds__(F_THREADS, 2) k_scan_fp32(ScanArgs a)
                 }
             }
         }
-        __syncthreads();
     }
 
     // ---- fused epilogue ----
@@ -183,7 +192,8 @@ __global__ void __launch_bounds__(F_THREADS, 2) k_scan_fp32(ScanArgs a)
 cudaError_t launch_scan_fp32(const ScanArgs &a, cudaStream_t s)
 {
     dim3 grid((a.W + F_WIN - 1) / F_WIN, (a.T + F_TPL - 1) / F_TPL);
-    k_scan_fp32<<<grid, F_THREADS, 0, s>>>(a);
+    cudaFuncSetAttribute(k_scan_fp32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F_SMEM);
+    k_scan_fp32<<<grid, F_THREADS, F_SMEM, s>>>(a);
     return cudaGetLastError();
 }
 
