@@ -111,6 +111,20 @@ __device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity)
                  : "memory");
     return ok != 0;
 }
+// try_wait with a suspend-time hint (ns): a waiting warp sleeps until the phase completes
+// or the hint runs out, instead of re-polling and taking issue slots from the warps it
+// waits for.
+__device__ __forceinline__ bool mbar_try_sleep(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(saddr(bar)), "r"(parity), "r"(20000u)
+                 : "memory");
+    return ok != 0;
+}
 // Bounded wait: false on timeout or when another role aborted (the CTA then unwinds).
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int &abort_flag, int *err, int where)
 {
@@ -119,7 +133,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int &a
     const long long t0 = clock64();
     while (true)
     {
-        if (mbar_try(bar, parity))
+        if (mbar_try_sleep(bar, parity))
             return true;
         if (*(volatile int *)&abort_flag)
             return false;
