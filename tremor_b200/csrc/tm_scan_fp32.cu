@@ -24,9 +24,14 @@
 
 namespace tmb {
 
-constexpr int F_WIN = 256, F_TPL = 64, F_K = 64, F_THREADS = 256;
-constexpr int F_XS = F_WIN + F_K + 16;
-constexpr int F_XS_PAD = F_XS + ((F_XS + 31) >> 5) * 4; // F_XS floats with their padding
+constexpr int F_WIN = 256, F_TPL = 64, F_THREADS = 256;
+// per stage of K samples (64, or 128 when the padded length allows: half the barriers):
+// the waveform slice (F_XS floats, stored with their padding) and the templates' slices
+template <int K> struct FStage
+{
+    static constexpr int XS = F_WIN + K + 16;
+    static constexpr int XS_PAD = XS + ((XS + 31) >> 5) * 4;
+};
 
 __device__ __forceinline__ int xpos(int i) { return i + ((i >> 5) << 2); }
 
@@ -47,10 +52,15 @@ template <int N> __device__ __forceinline__ void cp_wait() { asm volatile("cp.as
 // that stage st - 1 used, so one barrier per stage both publishes stage st and retires
 // stage st - 1.
 constexpr int F_BUFS = 3;
-constexpr size_t F_SMEM = sizeof(float) * (size_t)F_BUFS * (F_XS_PAD + F_TPL * F_K);
+template <int K> constexpr size_t f_smem()
+{
+    return sizeof(float) * (size_t)F_BUFS * (FStage<K>::XS_PAD + F_TPL * K);
+}
 
+template <int F_K>
 __global__ void __launch_bounds__(F_THREADS, 2) k_scan_fp32(ScanArgs a)
 {
+    constexpr int F_XS = FStage<F_K>::XS, F_XS_PAD = FStage<F_K>::XS_PAD;
     extern __shared__ __align__(16) float fsm[];
     float(*xs)[F_XS_PAD] = reinterpret_cast<float(*)[F_XS_PAD]>(fsm);
     float(*qs)[F_TPL][F_K] = reinterpret_cast<float(*)[F_TPL][F_K]>(fsm + F_BUFS * F_XS_PAD);
@@ -192,8 +202,16 @@ __global__ void __launch_bounds__(F_THREADS, 2) k_scan_fp32(ScanArgs a)
 cudaError_t launch_scan_fp32(const ScanArgs &a, cudaStream_t s)
 {
     dim3 grid((a.W + F_WIN - 1) / F_WIN, (a.T + F_TPL - 1) / F_TPL);
-    cudaFuncSetAttribute(k_scan_fp32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F_SMEM);
-    k_scan_fp32<<<grid, F_THREADS, F_SMEM, s>>>(a);
+    if (a.m_pad % 128 == 0)
+    {
+        cudaFuncSetAttribute(k_scan_fp32<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f_smem<128>());
+        k_scan_fp32<128><<<grid, F_THREADS, f_smem<128>(), s>>>(a);
+    }
+    else
+    {
+        cudaFuncSetAttribute(k_scan_fp32<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f_smem<64>());
+        k_scan_fp32<64><<<grid, F_THREADS, f_smem<64>(), s>>>(a);
+    }
     return cudaGetLastError();
 }
 
