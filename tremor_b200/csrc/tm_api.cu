@@ -636,6 +636,12 @@ int tm_bound_diagnostics(tm_ctx *ctx, const float *queries, int count, int m, fl
         a.err = reinterpret_cast<int *>(ctx->main.counters.as<uint32_t>() + 2);
         a.dbg_d = dd.as<float>();
         a.dbg_e = de.as<float>();
+        if (!use_umma)
+        {
+            ctx->main.fp32_qt.reserve(sizeof(float) * static_cast<size_t>(g.T_pad) * g.m_pad);
+            a.qt = ctx->main.fp32_qt.as<float>();
+            count_launch(ctx->main); // the template-tile transposition
+        }
         TM_CUDA(use_umma ? tmb::launch_scan_umma(a, s) : tmb::launch_scan_fp32(a, s));
         count_launch(ctx->main);
         TM_CUDA(cudaMemcpyAsync(d, dd.p, pairs * sizeof(float), cudaMemcpyDeviceToHost, s));

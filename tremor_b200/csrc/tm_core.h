@@ -262,7 +262,7 @@ namespace tmh {
 struct Lane
 {
     cudaStream_t stream = nullptr;
-    DevBuf tkey, bmin_u, bmin_l, list, counters, cand, dist;
+    DevBuf tkey, bmin_u, bmin_l, list, counters, cand, dist, fp32_qt; // (fp32_qt: k_scan_fp32's template tiles)
     // answer assembly: sort keys and values (double buffers), sort scratch, runs
     DevBuf akeys, avals, avals64, sort_tmp, segs;
     std::vector<std::shared_ptr<PinnedBlock>> pool;
@@ -292,7 +292,7 @@ struct Lane
     {
         if (stream)
             cudaStreamSynchronize(stream);
-        for (DevBuf *b : {&tkey, &bmin_u, &bmin_l, &list, &counters, &cand, &dist, &akeys, &avals, &avals64, &sort_tmp,
+        for (DevBuf *b : {&tkey, &bmin_u, &bmin_l, &list, &counters, &cand, &dist, &fp32_qt, &akeys, &avals, &avals64, &sort_tmp,
                           &segs, &fft2_Y, &fft3_Y, &fft_rows, &fft_stats, &fft_gmax})
             b->release();
         for (HostBuf *b : {&h_split, &h_q, &h_order, &h_slots, &h_counters})

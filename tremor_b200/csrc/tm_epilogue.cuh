@@ -39,6 +39,8 @@ struct ScanArgs
     int k_stride;          // row stride of the template arrays
     uint64_t n;            // samples of the waveform (P has n + 1 entries)
     int col_tile;          // window-major kernel: templates per column tile (32, 64, 128); 0: row tiles
+    float *qt;             // FP32 kernel: scratch for the templates by 64-template tile, [tile][m_pad][64]
+                           //   (T_pad x m_pad floats; filled by launch_scan_fp32 from q)
 };
 
 // Distance d of one (template, window) pair from its shifted dot product

@@ -46,6 +46,22 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+// Two FP32 values in one 64-bit register pair, and the packed FMA of sm_100 on such pairs:
+// each half is an ordinary round-to-nearest fmaf, one instruction for two.
+__device__ __forceinline__ uint64_t f2pack(float lo, float hi)
+{
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void f2unpack(uint64_t v, float &lo, float &hi)
+{
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ void fma2(uint64_t &acc, uint64_t a, uint64_t b)
+{
+    asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc) : "l"(a), "l"(b));
+}
 template <int N> __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
 // Three operand buffers (dynamic shared memory): stage st + 2 is loaded into the buffer
@@ -63,7 +79,7 @@ __global__ void __launch_bounds__(F_THREADS, 2) k_scan_fp32(ScanArgs a)
     constexpr int F_XS = FStage<F_K>::XS, F_XS_PAD = FStage<F_K>::XS_PAD;
     extern __shared__ __align__(16) float fsm[];
     float(*xs)[F_XS_PAD] = reinterpret_cast<float(*)[F_XS_PAD]>(fsm);
-    float(*qs)[F_TPL][F_K] = reinterpret_cast<float(*)[F_TPL][F_K]>(fsm + F_BUFS * F_XS_PAD);
+    float(*qs)[F_K][F_TPL] = reinterpret_cast<float(*)[F_K][F_TPL]>(fsm + F_BUFS * F_XS_PAD);
     __shared__ TemplParam tps[F_TPL];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -74,25 +90,23 @@ __global__ void __launch_bounds__(F_THREADS, 2) k_scan_fp32(ScanArgs a)
     const uint32_t jmid = min(tile_j + F_WIN / 2, a.W - 1);
     const float shift = a.mean[jmid];
     const float *xg = a.x + a.w0 + tile_j;
-    const float *qg = a.q + (size_t)tile_t * a.m_pad;
+    const float *qg = a.qt + (size_t)tile_t * a.m_pad; // the tile's templates, [k][64]
 
     auto load_stage = [&](int buf, int k0) {
         for (int i = tid; i < F_XS; i += F_THREADS)
             cp_async4(&xs[buf][xpos(i)], xg + k0 + i);
         for (int i = tid; i < F_TPL * F_K / 4; i += F_THREADS)
-        {
-            const int t = i / (F_K / 4), c = i % (F_K / 4);
-            cp_async16(&qs[buf][t][c * 4], qg + (size_t)t * a.m_pad + k0 + c * 4);
-        }
+            cp_async16(&qs[buf][0][0] + i * 4, qg + (size_t)k0 * F_TPL + i * 4);
         cp_commit();
     };
 
-    float acc[8][8];
+    // acc2[w][p]: the products of window 8 lane + w with templates 8 warp + 2p and + 2p + 1
+    uint64_t acc2[8][4];
 #pragma unroll
     for (int w = 0; w < 8; w++)
 #pragma unroll
-        for (int t = 0; t < 8; t++)
-            acc[w][t] = 0.0f;
+        for (int p2 = 0; p2 < 4; p2++)
+            acc2[w][p2] = 0ull;
 
     const int stages = a.m_pad / F_K;
     load_stage(0, 0);
@@ -109,7 +123,7 @@ __global__ void __launch_bounds__(F_THREADS, 2) k_scan_fp32(ScanArgs a)
         if (st + 2 < stages)
             load_stage((st + 2) % F_BUFS, (st + 2) * F_K);
         const float *xw = &xs[cur][0];
-        const float *qw = &qs[cur][8 * warp][0];
+        const float *qw = &qs[cur][0][8 * warp];
 #pragma unroll 4
         for (int kk = 0; kk < F_K; kk += 4)
         {
@@ -122,21 +136,32 @@ __global__ void __launch_bounds__(F_THREADS, 2) k_scan_fp32(ScanArgs a)
             const float xr[12] = {xa.x - shift, xa.y - shift, xa.z - shift, xa.w - shift,
                                   xb.x - shift, xb.y - shift, xb.z - shift, xb.w - shift,
                                   xc.x - shift, xc.y - shift, xc.z - shift, xc.w - shift};
+            // sample kk + i of the warp's 8 templates (two broadcast float4 loads), as 4 pairs;
+            // each accumulator takes its products in k order, as one fmaf each
 #pragma unroll
-            for (int t = 0; t < 8; t++)
+            for (int i = 0; i < 4; i++)
             {
-                const float4 qv = *reinterpret_cast<const float4 *>(qw + t * F_K + kk);
+                const float4 qa = *reinterpret_cast<const float4 *>(qw + (kk + i) * F_TPL);
+                const float4 qb = *reinterpret_cast<const float4 *>(qw + (kk + i) * F_TPL + 4);
+                const uint64_t q2[4] = {f2pack(qa.x, qa.y), f2pack(qa.z, qa.w), f2pack(qb.x, qb.y),
+                                        f2pack(qb.z, qb.w)};
 #pragma unroll
                 for (int w = 0; w < 8; w++)
                 {
-                    acc[w][t] = fmaf(xr[w + 0], qv.x, acc[w][t]);
-                    acc[w][t] = fmaf(xr[w + 1], qv.y, acc[w][t]);
-                    acc[w][t] = fmaf(xr[w + 2], qv.z, acc[w][t]);
-                    acc[w][t] = fmaf(xr[w + 3], qv.w, acc[w][t]);
+                    const uint64_t x2 = f2pack(xr[w + i], xr[w + i]);
+#pragma unroll
+                    for (int p2 = 0; p2 < 4; p2++)
+                        fma2(acc2[w][p2], x2, q2[p2]);
                 }
             }
         }
     }
+    float acc[8][8];
+#pragma unroll
+    for (int w = 0; w < 8; w++)
+#pragma unroll
+        for (int p2 = 0; p2 < 4; p2++)
+            f2unpack(acc2[w][p2], acc[w][2 * p2], acc[w][2 * p2 + 1]);
 
     // ---- fused epilogue ----
     const uint32_t j0 = tile_j + 8 * lane;
@@ -199,9 +224,31 @@ __global__ void __launch_bounds__(F_THREADS, 2) k_scan_fp32(ScanArgs a)
     }
 }
 
+// The templates of each 64-template tile with the sample index outermost: qt[tile][k][t]
+// = q[tile 64 + t][k], so that a stage of K samples of a tile is one contiguous K x 64
+// block. One block per (tile, 32 samples), through shared memory.
+__global__ void k_template_tiles(const float *__restrict__ q, int m_pad, float *__restrict__ qt)
+{
+    __shared__ float sm[F_TPL][33];
+    const int tile = blockIdx.y, k0 = blockIdx.x * 32;
+    for (int i = threadIdx.x; i < F_TPL * 32; i += blockDim.x)
+    {
+        const int t = i >> 5, k = i & 31;
+        sm[t][k] = q[(size_t)(tile * F_TPL + t) * m_pad + k0 + k];
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < F_TPL * 32; i += blockDim.x)
+    {
+        const int k = i >> 6, t = i & 63;
+        qt[((size_t)tile * m_pad + k0 + k) * F_TPL + t] = sm[t][k];
+    }
+}
+
 cudaError_t launch_scan_fp32(const ScanArgs &a, cudaStream_t s)
 {
     dim3 grid((a.W + F_WIN - 1) / F_WIN, (a.T + F_TPL - 1) / F_TPL);
+    // m_pad is a multiple of 64, so of 32
+    k_template_tiles<<<dim3((unsigned)(a.m_pad / 32), grid.y), 256, 0, s>>>(a.q, a.m_pad, a.qt);
     if (a.m_pad % 128 == 0)
     {
         cudaFuncSetAttribute(k_scan_fp32<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f_smem<128>());

@@ -429,7 +429,12 @@ void execute_group(tm_ctx *ctx, Lane &L, GroupPlan &g, tm_result &res)
         if (use_umma)
             TM_CUDA(g.col_tile > 0 ? tmb::launch_scan_wm(a, s) : tmb::launch_scan_umma(a, s));
         else
+        {
+            L.fp32_qt.reserve(sizeof(float) * static_cast<size_t>(g.T_pad) * g.m_pad);
+            a.qt = L.fp32_qt.as<float>();
             TM_CUDA(tmb::launch_scan_fp32(a, s));
+            count_launch(L); // the template-tile transposition
+        }
         count_launch(L);
         if (L.profile)
         {
