@@ -80,6 +80,19 @@ def test_random_knn_matches_oracle(kernel, m):
             _assert_knn_equal(x, q, m, k, merge, I, D)
 
 
+@pytest.mark.parametrize('m', [150, 300, 384, 520])
+def test_fp32_stage_depths(m):
+    """The FP32 kernel's two stage depths: padded lengths 192 and 320 (stages of 64
+    samples, several of them) and 384 and 576 (stages of 128 when the padded length is a
+    multiple of 128, else 64), against the oracle bit for bit."""
+    x = _waveform(1 << 16, 31 + m)
+    q = _templates(x, m, np.random.default_rng(m + 3), 4)
+    with _ctx(x, tb.KERNEL_FP32) as ctx:
+        for k, merge in [(1, 0), (6, m // 2)]:
+            I, D = ctx.search_knn(q, k, merge)
+            _assert_knn_equal(x, q, m, k, merge, I, D)
+
+
 @pytest.mark.parametrize('kernel', KERNELS)
 @pytest.mark.parametrize('m', [48, 256, 1000])
 def test_random_threshold_matches_oracle(kernel, m):
