@@ -529,6 +529,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         constexpr uint32_t STAGE = Sm::STAGE;
         const PrefixView pv{a.P, a.PT, a.PC};
         uint32_t tc = 0, staged = 0;
+        int tab_tt = -1, my_d = 0, nd = 0; // mixed: the template tile of the warp's length tables
         for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x, tc++)
         {
             const int buf = tc & 1;
@@ -581,10 +582,13 @@ __global__ void __launch_bounds__(THREADS, 1)
                     goto done;
             }
             // mixed: the distinct lengths of this warp's rows (at most 32), found while the
-            // tile's MMAs run; my_d is the lane's entry
-            int my_d = 0, nd = 0;
-            if (MIXED)
+            // tile's MMAs run; my_d is the lane's entry. The tables depend only on the
+            // template tile, so a warp keeps them while its next tiles have the same one.
+            if (MIXED && tt != tab_tt)
             {
+                tab_tt = tt;
+                my_d = 0;
+                nd = 0;
                 __syncwarp(); // the previous tile's readers of the tables are done
                 uint32_t pending = __ballot_sync(0xffffffffu, valid);
                 while (pending != 0u)
