@@ -629,8 +629,8 @@ __global__ void __launch_bounds__(THREADS, 1)
                 // This warp's 128 windows of the tile (128 half .. + 127) in groups of G
                 // windows, G x nd <= 256 table entries (G = 32 for up to 8 lengths):
                 // phase A: statistics of each (window, distinct length of the warp) from the
-                //   prefix sums at the window's start and end (G lanes per length read G
-                //   consecutive windows; the four loads of an item are independent);
+                //   prefix sums at the window's start and end (the G lanes of a length read G
+                //   consecutive windows; a lane's lengths share its window);
                 // phase B: each lane's distances from its length's statistics, 8 windows
                 //   per TMEM load, one candidate emission per group.
                 const LaneTerms lt = lane_terms(p, valid);
